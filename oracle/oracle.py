@@ -1,0 +1,97 @@
+"""Python access to the CPU oracle (test infrastructure only).
+
+``liboracle()`` loads the restated oracle (oracle/pbsam_oracle.cpp, built into
+oracle/libpbsam_oracle.so by ``build()``); ``run_spec`` writes a spec file in
+the force-harness format and runs it; ``parse`` reads the harness/oracle output
+format (KAPPA / FRAME / FORCE / TORQUE / ENERGY / per-sphere dumps).
+Only tests, the smoke check and the bench's CPU-baseline leg use this module.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libpbsam_oracle.so")
+_lib = None
+
+DEFAULT_TOL = (1e-2, 1e-8, 100, 1000)   # MAX_POLAR_DEV, SOLVE_TOL, SOLVE_MAX_CT, MAX_POL_ROUNDS
+TIGHT_TOL = (1e-7, 1e-26, 400, 1000)
+
+
+def build(force=False):
+    """Compile the restated oracle (g++, no GPU needed)."""
+    src = os.path.join(HERE, "pbsam_oracle.cpp")
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+        subprocess.check_call(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-o", LIB, src])
+    return LIB
+
+
+def liboracle():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(LIB)
+        _lib.pbsam_oracle_run.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        _lib.pbsam_oracle_run.restype = ctypes.c_int
+    return _lib
+
+
+def write_spec(path, moltypes, frames, salt=0.05, idiel=4.0, poles=10, tol=DEFAULT_TOL, dump=0, energy=1):
+    """moltypes: list of (pqr, imatdir, expdir, expname); frames: list of lists
+    of (type, pos[3], quat[4])."""
+    with open(path, "w") as fh:
+        fh.write("salt %r\nidiel %r\npoles %d\ndump %d\nenergy %d\n" % (salt, idiel, poles, dump, energy))
+        fh.write("tol %r %r %d %d\n" % tuple(tol))
+        for mt in moltypes:
+            fh.write("moltype %s %s %s %s\n" % tuple(mt))
+        for fr in frames:
+            fh.write("frame\n")
+            for (t, pos, q) in fr:
+                fh.write("mol %d %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n" % tuple([t] + list(pos) + list(q)))
+
+
+def run_spec(spec, out):
+    rc = liboracle().pbsam_oracle_run(spec.encode(), out.encode())
+    if rc != 0:
+        raise RuntimeError("oracle failed with status %d" % rc)
+    return parse(out)
+
+
+def parse(path):
+    """Returns a list of frames: dict(ok, force[n,3], torque[n,3], energy, dump{tag:{(i,k):array}})."""
+    frames = []
+    cur = None
+    with open(path) as fh:
+        for ln in fh:
+            t = ln.split()
+            if not t:
+                continue
+            if t[0] == "FRAME":
+                cur = dict(ok=int(t[2]) == 1, force={}, torque={}, energy=None, dump={}, info=t[3:])
+                frames.append(cur)
+            elif t[0] == "FORCE":
+                cur["force"][int(t[1])] = [float(x) for x in t[2:5]]
+            elif t[0] == "TORQUE":
+                cur["torque"][int(t[1])] = [float(x) for x in t[2:5]]
+            elif t[0] == "ENERGY":
+                cur["energy"] = float(t[1])
+            elif t[0] == "KAPPA":
+                pass
+            elif cur is not None:
+                cur["dump"].setdefault(t[0], {})[(int(t[1]), int(t[2]))] = np.array([float(x) for x in t[4:]])
+    for fr in frames:
+        n = len(fr["force"])
+        fr["force"] = np.array([fr["force"][i] for i in range(n)]).reshape(-1, 3)
+        fr["torque"] = np.array([fr["torque"][i] for i in range(n)]).reshape(-1, 3)
+    return frames
+
+
+def golden_moltypes(case_dir):
+    return [(os.path.join(case_dir, "mol%s.pqr" % t), os.path.join(case_dir, "im" + t),
+             os.path.join(case_dir, "exp" + t), "mol%s.0" % t) for t in ("A", "B")]
+
+
+def golden_frames(poses_entry):
+    return [[(m["type"], m["pos"], m["quat"]) for m in poses_entry]]
