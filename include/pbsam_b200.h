@@ -1,0 +1,126 @@
+/* C ABI of the B200 drop-in for PB-SAM's mutual-polarization solve and its
+ * force/torque evaluation.
+ *
+ * The reference exposes this path as a C++ class API called by its drivers
+ * (pbsam / bdnam / bdm); each entry point below replaces the reference call
+ * named in its comment (paths relative to the PB-SAM source tree).  Plain
+ * pointers and sizes only; every call returns an int status (PBSAM_OK = 0,
+ * negative = call error).  Per-system outcomes of a force evaluation are
+ * reported in a status array (PBSAM_SYS_*), never by exiting the process.
+ *
+ * Units and layouts follow the reference: lengths in Angstrom, charges in e,
+ * expansions in the packed real layout of src/expansion.h:509-553 (p*p doubles
+ * per expansion), IMats p^2 x p^2 column-major doubles, quaternions (w,x,y,z).
+ * Forces and torques are returned exactly as CMolecule::computeForces returns
+ * them (molecule-frame sums rotated by the conjugate orientation,
+ * src/moldynamics.cpp:524-550).
+ */
+#ifndef PBSAM_B200_H
+#define PBSAM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PBSAM_OK 0
+#define PBSAM_E_BADARG (-1)
+#define PBSAM_E_IO (-2)
+#define PBSAM_E_CUDA (-3)
+#define PBSAM_E_NOMEM (-4)
+#define PBSAM_E_STATE (-5)
+
+/* per-system status of a force evaluation */
+#define PBSAM_SYS_OK 0
+#define PBSAM_SYS_OVERLAP 1   /* two spheres of different molecules overlap
+                                 (computeForces returns false, src/molecule.cpp:1090-1097) */
+
+typedef struct pbsam_params {
+  int poles;              /* pole order p (the reference's N_POLES, src/expansion.h:5-9) */
+  double salt;            /* ionic strength in mol/L; kappa as src/BDnam_main.cpp:53-55 */
+  double idiel;           /* interior dielectric (4) */
+  double sdiel;           /* solvent dielectric (78) */
+  double temperature;     /* K (298.15) */
+  double max_polar_dev;   /* MAX_POLAR_DEV, src/molecule.cpp:6 (1e-2) */
+  double solve_tol;       /* SOLVE_TOL, src/expcenter.cpp:17 (1e-8) */
+  int solve_max_ct;       /* SOLVE_MAX_CT, src/expcenter.cpp:18 (100) */
+  int max_pol_rounds;     /* MAX_POL_ROUNDS, src/molecule.cpp:10 (1000) */
+  double inter_cutoff;    /* inter-molecular polarization cutoff, src/BDnam.cpp:138 (10) */
+  double interact_cutoff; /* interaction cutoff, src/BDnam.cpp:139 (100) */
+  double intra_cutoff;    /* intra near-list cutoff, src/BDnam.cpp:82 (30) */
+  double min_sep_numeric; /* MINSEPDIST, src/molecule.h:22 (5) */
+  int num_points_x;       /* NUM_POINTS_X cap on surface points, src/molecule.cpp:64 (10000) */
+} pbsam_params;
+
+typedef struct pbsam_context pbsam_context;
+typedef struct pbsam_system pbsam_system;
+
+/* Defaults equal to the reference built with __ACCURATE__ at N_POLES = 10. */
+void pbsam_params_default(pbsam_params *prm);
+
+/* Replaces CSystem::initConstants(kappa, sdiel, temp) (src/system.h:19-20,
+ * src/system.cpp:15-25) and the constant tables it triggers
+ * (CMolecule::initConstants, src/molecule.cpp:41-70).  One context per device. */
+int pbsam_context_create(const pbsam_params *prm, int device, pbsam_context **ctx);
+int pbsam_context_destroy(pbsam_context *ctx);
+/* inverse Debye length used by the context (CSystem::KAPPA) */
+int pbsam_context_kappa(const pbsam_context *ctx, double *kappa);
+
+/* Replaces the per-species part of CBDnam::CBDnam (src/BDnam.cpp:59-119):
+ * readpqr, readMats (imat.sp<k>.out.bin), readExpansionsP (<name>.<k>.{F,H}.exp),
+ * generateMolSPX, generateMolExposedChargesFH, generateMolTypeIntraPolLists and
+ * computeMolTypeValues.  All types must be added before the first system. */
+int pbsam_moltype_load(pbsam_context *ctx, const char *pqr_path, const char *imat_dir,
+                       const char *exp_dir, const char *exp_name, int *type_id);
+/* Same from memory: centres[n_sph*3], radii[n_sph], chg_pos[n_chg*3], chg[n_chg],
+ * imats[n_sph*p^4], fself/hself[n_sph*p^2], hself_scale[n_sph] (the scale value stored
+ * with each H expansion). */
+int pbsam_moltype_create(pbsam_context *ctx, int n_sph, const double *centres, const double *radii,
+                         int n_chg, const double *chg_pos, const double *chg, const double *imats,
+                         const double *fself, const double *hself, const double *hself_scale, int *type_id);
+/* number of spheres / exposed surface points of a type */
+int pbsam_moltype_info(const pbsam_context *ctx, int type_id, int *n_sph, int *n_points);
+
+/* Replaces constructing the CMolecule objects of a run (src/molecule.h:67-77)
+ * followed by CMolecule::initMutualConstants(mols, inter, interact, true)
+ * (src/molecule.cpp:77-95), for n_systems independent copies of the same
+ * molecule list (mol_types[n_mol]).  Each system keeps its own solver state
+ * between calls, as the reference's molecules do. */
+int pbsam_system_create(pbsam_context *ctx, int n_systems, int n_mol, const int *mol_types,
+                        pbsam_system **sys);
+int pbsam_system_destroy(pbsam_system *sys);
+/* Return every system to the freshly constructed state. */
+int pbsam_system_reset(pbsam_system *sys);
+
+/* Replaces CMolecule::setPos / setOrient (src/molecule.h:325-326):
+ * pos[n_systems*n_mol*3], quat[n_systems*n_mol*4]; on_device != 0 means the
+ * pointers are device pointers. */
+int pbsam_system_set_poses(pbsam_system *sys, const double *pos, const double *quat, int on_device);
+
+/* Replaces CMolecule::computeForces(mols, force, torque) (src/molecule.h:179,
+ * src/moldynamics.cpp:553-587) for every system: force/torque[n_systems*n_mol*3],
+ * status[n_systems] (PBSAM_SYS_*).  Any output pointer may be NULL. */
+int pbsam_system_compute_forces(pbsam_system *sys, double *force, double *torque, int *status, int on_device);
+
+/* Replaces CMolecule::computeTotalIntEnergy (src/molecule.h:180,
+ * src/moldynamics.cpp:358-386) on the state left by the last force evaluation. */
+int pbsam_system_compute_energy(pbsam_system *sys, double *energy, int on_device);
+
+/* Counters of the last force evaluation, 8 ints per system: [0] sweeps,
+ * [1] inner F/H iterations, [2] inner solves, [3] gradient solves,
+ * [4] 1 if the polarization sweeps hit max_pol_rounds. */
+int pbsam_system_stats(const pbsam_system *sys, int *stats);
+
+/* CUDA stream the system's work is queued on (cudaStream_t as void*); the
+ * calls above synchronise it before returning host results. */
+int pbsam_system_set_stream(pbsam_system *sys, void *stream);
+
+/* Device time in milliseconds of the last force-kernel launch (CUDA events). */
+int pbsam_system_last_kernel_ms(const pbsam_system *sys, double *ms);
+
+/* Text of the last error on the calling thread. */
+const char *pbsam_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

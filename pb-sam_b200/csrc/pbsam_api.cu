@@ -1,0 +1,656 @@
+// Host side of the C ABI (include/pbsam_b200.h): constant tables, input file
+// readers, exposed-surface-point generation, device storage of molecule types
+// and systems, and kernel launches.  Single translation unit with the kernels.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "pbsam_b200.h"
+#include "pbsam_kernels.cu"
+
+using namespace pbsam;
+
+static thread_local std::string g_err;
+static int fail(int code, const std::string &msg) { g_err = msg; return code; }
+#define CK(x)                                                                                  \
+  do {                                                                                         \
+    cudaError_t e_ = (x);                                                                      \
+    if (e_ != cudaSuccess) return fail(PBSAM_E_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+extern "C" const char *pbsam_last_error(void) { return g_err.c_str(); }
+
+// ------------------------------------------------------------------ host tables
+// The formulas of src/expansion.cpp:39-96, src/rotcoeff.cpp:15-33, 949-983,
+// src/transcoeff.cpp:15-38, src/expcenter.cpp:186-210; zeta has 2NP columns
+// (the reference's table writes one column past its declared width).
+struct HostTab {
+  int NP;
+  double kappa;
+  std::vector<double> buf;
+  size_t oC1, oC2, oC3, oC4, oC6, oZ, oE, oA, oB, oG, oD, oQ, oK2, oK3;
+  void build(int np, double kap)
+  {
+    NP = np; kappa = kap;
+    const int N2 = 2 * NP;
+    size_t off = 0;
+    auto take = [&](size_t n) { size_t o = off; off += n; return o; };
+    oC1 = take(N2 * N2); oC2 = take(N2 * N2); oC3 = take(N2 * N2); oC4 = take(N2); oC6 = take(N2);
+    oZ = take(N2 * N2); oE = take(N2 * (4 * NP - 1)); oA = take(N2 * NP); oB = take(N2 * NP);
+    oG = take(N2 * (2 * NP - 1)); oD = take(N2 * (2 * NP - 1)); oQ = take((2 * NP - 1) * NP * 2);
+    oK2 = take(NP); oK3 = take(NP);
+    buf.assign(off, 0.0);
+    double *C1 = &buf[oC1], *C2 = &buf[oC2], *C3 = &buf[oC3], *C4 = &buf[oC4], *C6 = &buf[oC6];
+    std::vector<double> temp(4 * NP);
+    temp[0] = 1.0;
+    for (int i = 1; i < 4 * NP; i++) temp[i] = temp[i - 1] * sqrt((double)i);
+    for (int n = 0; n < N2; n++)
+      for (int m = 0; m <= n; m++) {
+        C1[n * N2 + m] = (2 * n - 1) / (double)(n - m);
+        C2[n * N2 + m] = (n + m - 1) / (double)(n - m);
+        C3[n * N2 + m] = temp[n - m] / temp[n + m];
+      }
+    C6[0] = 1.0; C6[1] = 1.0;
+    for (int n = 2; n < N2; n++) C6[n] = C6[n - 1] * (2 * n - 1);
+    for (int n = 0; n < N2; n++) C4[n] = 1.0 / ((2 * n - 1) * (2 * n - 3));
+    auto ZETA = [&](int n, int m) -> double & { return buf[oZ + n * N2 + m]; };
+    auto ETA = [&](int n, int m) -> double & { return buf[oE + n * (4 * NP - 1) + 2 * NP - 1 + m]; };
+    for (int n = 0; n < N2; n++)
+      for (int m = 0; m <= n; m++) ZETA(n, m) = sqrt((double)(n + m + 1) * (n - m + 1) / ((2 * n + 1) * (2 * n + 3)));
+    for (int n = 0; n < N2; n++)
+      for (int m = 0; m <= n; m++) {
+        ETA(n, m) = sqrt((double)(n - m - 1) * (n - m) / ((2 * n + 1) * (2 * n - 1)));
+        if (m != 0) ETA(n, -m) = -sqrt((double)(n + m - 1) * (n + m) / ((2 * n + 1) * (2 * n - 1)));
+      }
+    // singular-rotation derivative coefficients from the degenerate harmonics at theta = 0
+    {
+      const int nn = 2 * NP - 1;
+      std::vector<double> SH(nn, 0.0);
+      if (nn > 1) SH[1] = -1;
+      if (nn > 2) SH[2] = -1.0 * 3;
+      for (int l = 3; l < nn; l++) SH[l] = (1.0 * (2 * l - 1) * SH[l - 1] - l * SH[l - 2]) / (l - 1);
+      for (int l = 1; l < nn; l++) SH[l] *= (-C3[l * N2 + 1]);
+      auto Q = [&](int n, int m, int k) -> double & { return buf[oQ + (n * NP + m) * 2 + k]; };
+      for (int n = 1; n < nn; n++) { Q(n, 0, 0) = 0.0; Q(n, 0, 1) = SH[n]; }
+      for (int n = 2; n < nn; n++) {
+        Q(n - 1, 1, 0) = (ETA(n, -1) * Q(n, 0, 1) + ZETA(n - 1, 0)) / ETA(n, 0);
+        Q(n - 1, 1, 1) = (n > 2) ? (ETA(n, 1) / ETA(n, 0)) * Q(n, 0, 1) : 0.0;
+      }
+      for (int m = 1; m < NP - 1; m++)
+        for (int n = m + 2; n < 2 * NP - m - 1; n++) {
+          Q(n - 1, m + 1, 0) = (ETA(n, m - 1) * Q(n, m, 0) + ZETA(n - 1, m)) / ETA(n, m);
+          Q(n - 1, m + 1, 1) = (n > m + 2) ? (ETA(n, m + 1) / ETA(n, m)) * Q(n, m, 1) : 0.0;
+        }
+    }
+    const double kapsqr = (kappa == 0 ? 0 : 1.0);
+    for (int n = 0; n < N2; n++)
+      for (int m = 0; m < NP; m++) {
+        double &A = buf[oA + n * NP + m], &B = buf[oB + n * NP + m];
+        double &G = buf[oG + n * (2 * NP - 1) + NP - 1 + m], &D = buf[oD + n * (2 * NP - 1) + NP - 1 + m];
+        A = sqrt((double)(n + m + 1) * (n - m + 1));
+        B = kapsqr * A / ((2 * n + 1) * (2 * n + 3));
+        G = sqrt((double)(n - m - 1) * (n - m));
+        D = kapsqr * G / ((2 * n + 1) * (2 * n - 1));
+        if (m != 0) {
+          double &Gm = buf[oG + n * (2 * NP - 1) + NP - 1 - m], &Dm = buf[oD + n * (2 * NP - 1) + NP - 1 - m];
+          Gm = -sqrt((double)(n + m - 1) * (n + m));
+          Dm = kapsqr * Gm / ((2 * n + 1) * (2 * n - 1));
+        }
+      }
+    for (int l = 0; l < NP; l++) { buf[oK2 + l] = (2 * l + 1) / (4.0 * M_PI); buf[oK3 + l] = 1 / (double)(2 * l + 1); }
+  }
+  Tab view(const double *d) const
+  {
+    Tab t;
+    t.NP = NP; t.kappa = kappa;
+    t.C1 = d + oC1; t.C2 = d + oC2; t.C3 = d + oC3; t.C4 = d + oC4; t.C6 = d + oC6;
+    t.zeta = d + oZ; t.eta = d + oE; t.alpha = d + oA; t.beta = d + oB; t.gam = d + oG; t.del = d + oD;
+    t.Q = d + oQ; t.CONST2 = d + oK2; t.CONST3 = d + oK3;
+    return t;
+  }
+};
+
+// ------------------------------------------------------------------ molecule types (host copy)
+struct HostType {
+  int ns = 0;
+  double maxR = 0;
+  std::vector<double> cen, rad;       // molecule frame (sphere centres minus their mean)
+  std::vector<double> spx;            // exposed points, per sphere, relative to its centre
+  std::vector<int> spx_cnt, nspx;
+  std::vector<std::vector<int> > near;
+  std::vector<double> fself, hself, hscale, imat;
+  std::vector<double> chg_pos, chg;   // relative to the molecule centre
+};
+
+struct pbsam_context {
+  pbsam_params prm;
+  int device = 0;
+  HostTab ht;
+  double *dtab = nullptr;
+  Tab T;
+  std::vector<HostType> types;
+  bool finalized = false;
+  TypeView tv;
+  std::vector<void *> tbufs;
+  int live_systems = 0;
+};
+
+struct pbsam_system {
+  pbsam_context *ctx = nullptr;
+  Ctx c;
+  int B = 0, nmol = 0;
+  std::vector<void *> bufs;
+  cudaStream_t stream = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+};
+
+extern "C" void pbsam_params_default(pbsam_params *p)
+{
+  p->poles = 10; p->salt = 0.05; p->idiel = 4.0; p->sdiel = 78.0; p->temperature = 298.15;
+  p->max_polar_dev = 1e-2; p->solve_tol = 1e-8; p->solve_max_ct = 100; p->max_pol_rounds = 1000;
+  p->inter_cutoff = 10; p->interact_cutoff = 100; p->intra_cutoff = 30; p->min_sep_numeric = 5;
+  p->num_points_x = 10000;
+}
+
+static double kappa_of(const pbsam_params &p)
+{
+  const double AVO = 6.0221415e23, ECHG = 1.60217646e-19, EPS0 = 8.854187817e-12;
+  const double KBOLTZ = 1.3806503e-23, ANG = 1e-10, LIT = 1e-3;
+  return ANG * sqrt((2 * p.salt * AVO / LIT * ECHG * ECHG) / (p.sdiel * EPS0 * KBOLTZ * p.temperature));
+}
+
+extern "C" int pbsam_context_create(const pbsam_params *prm, int device, pbsam_context **out)
+{
+  if (!prm || !out) return fail(PBSAM_E_BADARG, "null argument");
+  if (prm->poles < 1 || prm->poles > 32) return fail(PBSAM_E_BADARG, "poles must be in [1, 32]");
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(PBSAM_E_BADARG, "no such CUDA device");
+  CK(cudaSetDevice(device));
+  CK(cudaDeviceSetLimit(cudaLimitStackSize, 8192));
+  pbsam_context *c = new pbsam_context();
+  c->prm = *prm;
+  c->device = device;
+  c->ht.build(prm->poles, kappa_of(*prm));
+  cudaError_t e = cudaMalloc(&c->dtab, c->ht.buf.size() * sizeof(double));
+  if (e != cudaSuccess) { delete c; return fail(PBSAM_E_CUDA, cudaGetErrorString(e)); }
+  e = cudaMemcpy(c->dtab, c->ht.buf.data(), c->ht.buf.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { cudaFree(c->dtab); delete c; return fail(PBSAM_E_CUDA, cudaGetErrorString(e)); }
+  c->T = c->ht.view(c->dtab);
+  *out = c;
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_context_kappa(const pbsam_context *c, double *kappa)
+{
+  if (!c || !kappa) return fail(PBSAM_E_BADARG, "null argument");
+  *kappa = c->ht.kappa;
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_context_destroy(pbsam_context *c)
+{
+  if (!c) return PBSAM_OK;
+  if (c->live_systems > 0) return fail(PBSAM_E_STATE, "systems still alive");
+  cudaSetDevice(c->device);
+  for (void *p : c->tbufs) cudaFree(p);
+  cudaFree(c->dtab);
+  delete c;
+  return PBSAM_OK;
+}
+
+// ------------------------------------------------------------------ input files
+// PQR as read by src/readutil.cpp:285-355 (CEN at byte 18, x y z q r from byte 31)
+static bool read_pqr(const char *fname, std::vector<double> &pos, std::vector<double> &ch, std::vector<double> &rad,
+                     std::vector<double> &cen)
+{
+  FILE *f = fopen(fname, "r");
+  if (!f) return false;
+  char buf[512];
+  while (fgets(buf, sizeof buf, f)) {
+    if (strncmp(buf, "ATOM", 4) != 0 || strlen(buf) < 32) continue;
+    double x, y, z, c, r;
+    if (sscanf(buf + 31, "%lf %lf %lf %lf %lf", &x, &y, &z, &c, &r) != 5) continue;
+    if (strncmp(buf + 18, "CEN", 3) == 0) { rad.push_back(r); cen.push_back(x); cen.push_back(y); cen.push_back(z); }
+    else { pos.push_back(x); pos.push_back(y); pos.push_back(z); ch.push_back(c); }
+  }
+  fclose(f);
+  return true;
+}
+// IMat binary: int p, then p^4 doubles; a larger p is truncated as src/readutil.cpp:399-435
+static bool read_imat(const char *fname, int NP, double *mat)
+{
+  FILE *f = fopen(fname, "rb");
+  if (!f) return false;
+  int p = 0;
+  if (fread(&p, sizeof(int), 1, f) != 1 || p < NP) { fclose(f); return false; }
+  const long psq = (long)NP * NP;
+  bool ok = true;
+  if (p == NP) ok = fread(mat, sizeof(double), psq * psq, f) == (size_t)(psq * psq);
+  else {
+    const long matlen = (long)p * p;
+    for (long j = 0; j < psq && ok; j++) {
+      ok = fread(mat + j * psq, sizeof(double), psq, f) == (size_t)psq;
+      fseek(f, (matlen - psq) * (long)sizeof(double), SEEK_CUR);
+    }
+  }
+  fclose(f);
+  return ok;
+}
+// expansion text file: p, scale, rcut, coefficients (src/readutil.cpp:564-598)
+static bool read_exp(const char *fname, int NP, double *V, double &scale)
+{
+  std::ifstream fin(fname);
+  if (!fin) return false;
+  int pr = 0;
+  double rcut = 0;
+  fin >> pr >> scale >> rcut;
+  if (!fin) return false;
+  for (int k = 0; k < NP * NP; k++) V[k] = 0.0;
+  const int n = (pr < NP) ? pr * pr : NP * NP;
+  for (int k = 0; k < n; k++) fin >> V[k];
+  return (bool)fin;
+}
+
+// exposed surface points (src/molecule.cpp:756-780, 877-894, 948-994, 2272-2294)
+static void make_surface_points(const pbsam_params &prm, HostType &t, const std::vector<double> &cen_abs)
+{
+  const int ns = t.ns;
+  t.spx.clear(); t.spx_cnt.assign(ns, 0); t.nspx.assign(ns, 0);
+  for (int k = 0; k < ns; k++) {
+    std::vector<int> neigh;
+    for (int j = 0; j < ns; j++) {
+      if (j == k) continue;
+      const double sr = t.rad[k] + t.rad[j];
+      const double dx = cen_abs[3 * k] - cen_abs[3 * j], dy = cen_abs[3 * k + 1] - cen_abs[3 * j + 1],
+                   dz = cen_abs[3 * k + 2] - cen_abs[3 * j + 2];
+      if (dx * dx + dy * dy + dz * dz < sr * sr) neigh.push_back(j);
+    }
+    const int Nin = prm.num_points_x;
+    const double cutoff = 1.5, maxrad = 10, gradient = Nin / ((maxrad - cutoff) * (maxrad - cutoff));
+    int N;
+    if (t.rad[k] < cutoff) N = 200;
+    else { N = int(200 + gradient * (t.rad[k] - cutoff) * (t.rad[k] - cutoff)); if (N > Nin) N = Nin; }
+    std::vector<double> th(N), ph(N);
+    for (int i = 1; i <= N; i++) {
+      const double h = -1.0 + 2.0 * (i - 1.0) / (N - 1.0);
+      th[i - 1] = acos(h);
+      if (i == 1 || i == N) ph[i - 1] = 0;
+      else ph[i - 1] = (ph[i - 2] + 3.6 / sqrt(N * (1.0 - h * h)));
+      while (ph[i - 1] > 2 * M_PI) ph[i - 1] -= 2 * M_PI;
+      while (ph[i - 1] < -2 * M_PI) ph[i - 1] += 2 * M_PI;
+    }
+    for (int n = 0; n < N; n++) {
+      const double px = t.rad[k] * (1 * sin(th[n]) * cos(ph[n])), py = t.rad[k] * (1 * sin(th[n]) * sin(ph[n])),
+                   pz = t.rad[k] * (1 * cos(th[n]));
+      bool inside = false;
+      for (int j : neigh) {
+        const double dx = px + cen_abs[3 * k] - cen_abs[3 * j], dy = py + cen_abs[3 * k + 1] - cen_abs[3 * j + 1],
+                     dz = pz + cen_abs[3 * k + 2] - cen_abs[3 * j + 2];
+        if (dx * dx + dy * dy + dz * dz < t.rad[j] * t.rad[j]) { inside = true; break; }
+      }
+      if (!inside) { t.spx.push_back(px); t.spx.push_back(py); t.spx.push_back(pz); t.spx_cnt[k]++; }
+    }
+    t.nspx[k] = N;
+  }
+}
+
+static int add_type(pbsam_context *c, HostType &&t0, const std::vector<double> &cen_abs)
+{
+  HostType t = std::move(t0);
+  const int ns = t.ns;
+  // molecule centre = mean sphere centre (src/BDnam.cpp:68-70)
+  double rc[3] = {0, 0, 0};
+  for (int k = 0; k < ns; k++) for (int d = 0; d < 3; d++) rc[d] += cen_abs[3 * k + d];
+  for (int d = 0; d < 3; d++) rc[d] /= ns;
+  t.cen.resize(3 * ns);
+  t.maxR = 0;
+  for (int k = 0; k < ns; k++) {
+    for (int d = 0; d < 3; d++) t.cen[3 * k + d] = cen_abs[3 * k + d] - rc[d];
+    const double r = sqrt(t.cen[3 * k] * t.cen[3 * k] + t.cen[3 * k + 1] * t.cen[3 * k + 1] + t.cen[3 * k + 2] * t.cen[3 * k + 2]) + t.rad[k];
+    if (r > t.maxR) t.maxR = r;
+  }
+  for (size_t q = 0; q < t.chg.size(); q++) for (int d = 0; d < 3; d++) t.chg_pos[3 * q + d] -= rc[d];
+  make_surface_points(c->prm, t, cen_abs);
+  // intra near lists (src/molecule.cpp:500-535)
+  t.near.assign(ns, std::vector<int>());
+  for (int kj = 0; kj < ns; kj++)
+    for (int ki = 0; ki < kj; ki++) {
+      const double dx = t.cen[3 * ki] - t.cen[3 * kj], dy = t.cen[3 * ki + 1] - t.cen[3 * kj + 1], dz = t.cen[3 * ki + 2] - t.cen[3 * kj + 2];
+      const double rho = sqrt(dx * dx + dy * dy + dz * dz);
+      if (rho < (t.rad[ki] + t.rad[kj] + c->prm.intra_cutoff)) { t.near[ki].push_back(kj); t.near[kj].push_back(ki); }
+    }
+  c->types.push_back(std::move(t));
+  return (int)c->types.size() - 1;
+}
+
+extern "C" int pbsam_moltype_load(pbsam_context *c, const char *pqr, const char *imat_dir, const char *exp_dir,
+                                  const char *exp_name, int *type_id)
+{
+  if (!c || !pqr || !imat_dir || !exp_dir || !exp_name || !type_id) return fail(PBSAM_E_BADARG, "null argument");
+  if (c->finalized) return fail(PBSAM_E_STATE, "molecule types are frozen once a system exists");
+  const int NP = c->prm.poles;
+  HostType t;
+  std::vector<double> cen_abs;
+  if (!read_pqr(pqr, t.chg_pos, t.chg, t.rad, cen_abs)) return fail(PBSAM_E_IO, std::string("cannot read ") + pqr);
+  t.ns = (int)t.rad.size();
+  if (t.ns == 0) return fail(PBSAM_E_IO, std::string("no CEN spheres in ") + pqr);
+  const long NP2 = (long)NP * NP;
+  t.imat.resize((size_t)t.ns * NP2 * NP2);
+  t.fself.resize((size_t)t.ns * NP2);
+  t.hself.resize((size_t)t.ns * NP2);
+  t.hscale.resize(t.ns);
+  char fn[4096];
+  for (int k = 0; k < t.ns; k++) {
+    snprintf(fn, sizeof fn, "%s/imat.sp%d.out.bin", imat_dir, k);
+    if (!read_imat(fn, NP, t.imat.data() + (size_t)k * NP2 * NP2)) return fail(PBSAM_E_IO, std::string("cannot read ") + fn);
+    double sc;
+    snprintf(fn, sizeof fn, "%s/%s.%d.F.exp", exp_dir, exp_name, k);
+    if (!read_exp(fn, NP, t.fself.data() + (size_t)k * NP2, sc)) return fail(PBSAM_E_IO, std::string("cannot read ") + fn);
+    snprintf(fn, sizeof fn, "%s/%s.%d.H.exp", exp_dir, exp_name, k);
+    if (!read_exp(fn, NP, t.hself.data() + (size_t)k * NP2, t.hscale[k])) return fail(PBSAM_E_IO, std::string("cannot read ") + fn);
+  }
+  *type_id = add_type(c, std::move(t), cen_abs);
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_moltype_create(pbsam_context *c, int n_sph, const double *centres, const double *radii, int n_chg,
+                                    const double *chg_pos, const double *chg, const double *imats, const double *fself,
+                                    const double *hself, const double *hself_scale, int *type_id)
+{
+  if (!c || n_sph <= 0 || n_chg < 0 || !centres || !radii || !imats || !fself || !hself || !hself_scale || !type_id ||
+      (n_chg > 0 && (!chg_pos || !chg)))
+    return fail(PBSAM_E_BADARG, "bad argument");
+  if (c->finalized) return fail(PBSAM_E_STATE, "molecule types are frozen once a system exists");
+  const long NP2 = (long)c->prm.poles * c->prm.poles;
+  HostType t;
+  t.ns = n_sph;
+  t.rad.assign(radii, radii + n_sph);
+  t.chg_pos.assign(chg_pos, chg_pos + 3 * n_chg);
+  t.chg.assign(chg, chg + n_chg);
+  t.imat.assign(imats, imats + (size_t)n_sph * NP2 * NP2);
+  t.fself.assign(fself, fself + (size_t)n_sph * NP2);
+  t.hself.assign(hself, hself + (size_t)n_sph * NP2);
+  t.hscale.assign(hself_scale, hself_scale + n_sph);
+  std::vector<double> cen_abs(centres, centres + 3 * n_sph);
+  *type_id = add_type(c, std::move(t), cen_abs);
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_moltype_info(const pbsam_context *c, int id, int *n_sph, int *n_points)
+{
+  if (!c || id < 0 || id >= (int)c->types.size()) return fail(PBSAM_E_BADARG, "bad type id");
+  if (n_sph) *n_sph = c->types[id].ns;
+  if (n_points) *n_points = (int)(c->types[id].spx.size() / 3);
+  return PBSAM_OK;
+}
+
+template <class T>
+static int dalloc(std::vector<void *> &bufs, T **p, size_t n)
+{
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess) return fail(PBSAM_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  bufs.push_back((void *)*p);
+  e = cudaMemset(*p, 0, n * sizeof(T));
+  if (e != cudaSuccess) return fail(PBSAM_E_CUDA, cudaGetErrorString(e));
+  return PBSAM_OK;
+}
+template <class T>
+static int dput(std::vector<void *> &bufs, const T **p, const std::vector<T> &h)
+{
+  T *d;
+  int r = dalloc(bufs, &d, h.size());
+  if (r) return r;
+  if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *p = d;
+  return PBSAM_OK;
+}
+#define TRY(x) do { int r_ = (x); if (r_) return r_; } while (0)
+
+// upload all molecule types and run the per-type setup kernels
+static int finalize_types(pbsam_context *c)
+{
+  if (c->finalized) return PBSAM_OK;
+  if (c->types.empty()) return fail(PBSAM_E_STATE, "no molecule types");
+  CK(cudaSetDevice(c->device));
+  const int NP = c->prm.poles;
+  const long NP2 = (long)NP * NP;
+  std::vector<int> type_off(1, 0), spx_off(1, 0), nspx, near_off(1, 0), near, chg_off(1, 0);
+  std::vector<double> maxR, cen, rad, spx, Fs, Hs, hsc, imat, chg_pos, chg;
+  int maxq = 0, maxns = 0;
+  for (auto &t : c->types) {
+    type_off.push_back(type_off.back() + t.ns);
+    maxR.push_back(t.maxR);
+    cen.insert(cen.end(), t.cen.begin(), t.cen.end());
+    rad.insert(rad.end(), t.rad.begin(), t.rad.end());
+    for (int k = 0; k < t.ns; k++) {
+      spx_off.push_back(spx_off.back() + t.spx_cnt[k]);
+      nspx.push_back(t.nspx[k]);
+      near_off.push_back(near_off.back() + (int)t.near[k].size());
+      near.insert(near.end(), t.near[k].begin(), t.near[k].end());
+    }
+    spx.insert(spx.end(), t.spx.begin(), t.spx.end());
+    Fs.insert(Fs.end(), t.fself.begin(), t.fself.end());
+    Hs.insert(Hs.end(), t.hself.begin(), t.hself.end());
+    hsc.insert(hsc.end(), t.hscale.begin(), t.hscale.end());
+    imat.insert(imat.end(), t.imat.begin(), t.imat.end());
+    chg_off.push_back(chg_off.back() + (int)t.chg.size());
+    chg_pos.insert(chg_pos.end(), t.chg_pos.begin(), t.chg_pos.end());
+    chg.insert(chg.end(), t.chg.begin(), t.chg.end());
+    if ((int)t.chg.size() > maxq) maxq = (int)t.chg.size();
+    if (t.ns > maxns) maxns = t.ns;
+  }
+  TypeView &tv = c->tv;
+  auto &B = c->tbufs;
+  tv.ntypes = (int)c->types.size();
+  tv.TS = type_off.back();
+  const int TS = tv.TS, TP = spx_off.back();
+  TRY(dput(B, &tv.type_off, type_off)); TRY(dput(B, &tv.maxR, maxR)); TRY(dput(B, &tv.cen, cen));
+  TRY(dput(B, &tv.rad, rad)); TRY(dput(B, &tv.spx_off, spx_off)); TRY(dput(B, &tv.spx, spx));
+  TRY(dput(B, &tv.nspx, nspx)); TRY(dput(B, &tv.Fself, Fs)); TRY(dput(B, &tv.Hself, Hs));
+  TRY(dput(B, &tv.hself_scale, hsc)); TRY(dput(B, &tv.near_off, near_off)); TRY(dput(B, &tv.near, near));
+  TRY(dput(B, &tv.imat, imat)); TRY(dput(B, &tv.chg_off, chg_off)); TRY(dput(B, &tv.chg_pos, chg_pos));
+  TRY(dput(B, &tv.chg, chg));
+  TRY(dalloc(B, &tv.qFself, TP)); TRY(dalloc(B, &tv.qHself, TP));
+  TRY(dalloc(B, &tv.tFself, TS)); TRY(dalloc(B, &tv.tHself, TS));
+  TRY(dalloc(B, &tv.LFintra, TS * NP2)); TRY(dalloc(B, &tv.LHintra, TS * NP2));
+  TRY(dalloc(B, &tv.LFfar, TS * NP2)); TRY(dalloc(B, &tv.LHfar, TS * NP2));
+  TRY(dalloc(B, &tv.Dfix, TS * NP2)); TRY(dalloc(B, &tv.Vfix, TS * NP2));
+  TRY(dalloc(B, &tv.cst, (size_t)TS * CST_N * NP));
+  // setup scratch: one team per type sphere; misc must hold 2 weights per charge
+  long long Sm = maxns;
+  while (4096 + Sm * Sm < 2LL * maxq) Sm++;
+  const long long stride = scr_doubles(NP, Sm);
+  double *scr;
+  if (cudaMalloc(&scr, (size_t)stride * TS * sizeof(double)) != cudaSuccess)
+    return fail(PBSAM_E_NOMEM, "setup scratch");
+  Ctx cx;
+  memset(&cx, 0, sizeof cx);
+  cx.T = c->T;
+  cx.tv = tv;
+  cx.prm.idiel = c->prm.idiel; cx.prm.sdiel = c->prm.sdiel;
+  cx.prm.min_sep_numeric = c->prm.min_sep_numeric;
+  pbsam_setup1_kernel<<<TS, PBSAM_TEAM>>>(cx, scr, stride);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) { pbsam_setup2_kernel<<<TS, PBSAM_TEAM>>>(cx, scr, stride); e = cudaGetLastError(); }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(scr);
+  if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("setup kernels: ") + cudaGetErrorString(e));
+  c->finalized = true;
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, const int *mol_types, pbsam_system **out)
+{
+  if (!c || n_systems <= 0 || n_mol <= 0 || n_mol > 32 || !mol_types || !out) return fail(PBSAM_E_BADARG, "bad argument");
+  for (int i = 0; i < n_mol; i++)
+    if (mol_types[i] < 0 || mol_types[i] >= (int)c->types.size()) return fail(PBSAM_E_BADARG, "bad molecule type");
+  TRY(finalize_types(c));
+  CK(cudaSetDevice(c->device));
+  const int NP = c->prm.poles;
+  const long NP2 = (long)NP * NP;
+  pbsam_system *s = new pbsam_system();
+  s->ctx = c;
+  s->B = n_systems; s->nmol = n_mol;
+  std::vector<int> mol_off(1, 0), sph_ts, sph_mol, pt_off(1, 0), toff(1, 0);
+  for (auto &t : c->types) toff.push_back(toff.back() + t.ns);
+  for (int i = 0; i < n_mol; i++) {
+    const HostType &t = c->types[mol_types[i]];
+    for (int k = 0; k < t.ns; k++) {
+      sph_ts.push_back(toff[mol_types[i]] + k);
+      sph_mol.push_back(i);
+      pt_off.push_back(pt_off.back() + t.spx_cnt[k]);
+    }
+    mol_off.push_back(mol_off.back() + t.ns);
+  }
+  const int S = mol_off.back(), SP = pt_off.back();
+  const long long B = n_systems;
+  BatchView &bv = s->c.bv;
+  auto &Bf = s->bufs;
+  bv.B = n_systems; bv.nmol = n_mol; bv.S = S; bv.SP = SP;
+  std::vector<int> mt(mol_types, mol_types + n_mol);
+  int r = 0;
+  auto chk = [&](int rr) { if (rr && !r) r = rr; };
+  chk(dput(Bf, &bv.mol_type, mt)); chk(dput(Bf, &bv.mol_off, mol_off)); chk(dput(Bf, &bv.sph_ts, sph_ts));
+  chk(dput(Bf, &bv.sph_mol, sph_mol)); chk(dput(Bf, &bv.pt_off, pt_off));
+  double *pos, *quat;
+  chk(dalloc(Bf, &pos, B * n_mol * 3)); chk(dalloc(Bf, &quat, B * n_mol * 4));
+  bv.pos = pos; bv.quat = quat;
+  chk(dalloc(Bf, &bv.F, B * S * NP2)); chk(dalloc(Bf, &bv.H, B * S * NP2)); chk(dalloc(Bf, &bv.Hrot, B * S * NP2));
+  chk(dalloc(Bf, &bv.HselfRot, B * S * NP2)); chk(dalloc(Bf, &bv.LS, B * S * NP2));
+  chk(dalloc(Bf, &bv.LFS, B * S * NP2)); chk(dalloc(Bf, &bv.LHS, B * S * NP2));
+  chk(dalloc(Bf, &bv.hscale, B * S)); chk(dalloc(Bf, &bv.tF, B * S)); chk(dalloc(Bf, &bv.tH, B * S));
+  chk(dalloc(Bf, &bv.maxgF, B * S)); chk(dalloc(Bf, &bv.maxgH, B * S)); chk(dalloc(Bf, &bv.dev, B * S));
+  chk(dalloc(Bf, &bv.qF, B * SP)); chk(dalloc(Bf, &bv.qH, B * SP));
+  chk(dalloc(Bf, &bv.gFp, B * SP * 3)); chk(dalloc(Bf, &bv.gHp, B * SP * 3));
+  chk(dalloc(Bf, &bv.gLHN, B * S * 3 * NP2)); chk(dalloc(Bf, &bv.gH, B * S * 3 * NP2));
+  chk(dalloc(Bf, &bv.cenRot, B * S * 3));
+  chk(dalloc(Bf, &bv.ipol, B * S * S)); chk(dalloc(Bf, &bv.ipol_n, B * S));
+  chk(dalloc(Bf, &bv.iact, B * S * S)); chk(dalloc(Bf, &bv.iact_n, B * S));
+  chk(dalloc(Bf, &bv.interMol, B * n_mol * S)); chk(dalloc(Bf, &bv.interMol_n, B * n_mol));
+  chk(dalloc(Bf, &bv.intraPol, B * n_mol * S)); chk(dalloc(Bf, &bv.intraPol_n, B * n_mol));
+  chk(dalloc(Bf, &bv.intraAct, B * n_mol * S)); chk(dalloc(Bf, &bv.intraAct_n, B * n_mol));
+  chk(dalloc(Bf, &bv.interX, B * n_mol));
+  chk(dalloc(Bf, &bv.gFw, B * S * 3 * NP2)); chk(dalloc(Bf, &bv.gHw, B * S * 3 * NP2));
+  chk(dalloc(Bf, &bv.gHrotw, B * S * 3 * NP2)); chk(dalloc(Bf, &bv.tGw, B * S * 3 * NP2));
+  chk(dalloc(Bf, &bv.gkey, B * S)); chk(dalloc(Bf, &bv.dgrad, B * S));
+  chk(dalloc(Bf, &bv.molR, (size_t)B * n_mol * rot_off(2 * NP - 1)));
+  chk(dalloc(Bf, &bv.molRS, B * n_mol * 16));
+  chk(dalloc(Bf, &bv.sep, B * S * S));
+  bv.scr_stride = scr_doubles(NP, S);
+  chk(dalloc(Bf, &bv.scr, (size_t)B * bv.scr_stride));
+  chk(dalloc(Bf, &bv.force, B * n_mol * 3)); chk(dalloc(Bf, &bv.torque, B * n_mol * 3));
+  chk(dalloc(Bf, &bv.energy, B)); chk(dalloc(Bf, &bv.status, B)); chk(dalloc(Bf, &bv.stats, B * 8));
+  if (r) {
+    for (void *p : Bf) cudaFree(p);
+    delete s;
+    return r;
+  }
+  s->c.T = c->T;
+  s->c.tv = c->tv;
+  SolveParams &p = s->c.prm;
+  p.max_polar_dev = c->prm.max_polar_dev; p.solve_tol = c->prm.solve_tol; p.solve_max_ct = c->prm.solve_max_ct;
+  p.max_pol_rounds = c->prm.max_pol_rounds; p.inter_cut = c->prm.inter_cutoff; p.interact_cut = c->prm.interact_cutoff;
+  p.min_sep_numeric = c->prm.min_sep_numeric; p.idiel = c->prm.idiel; p.sdiel = c->prm.sdiel;
+  cudaEventCreate(&s->ev0);
+  cudaEventCreate(&s->ev1);
+  c->live_systems++;
+  *out = s;
+  return pbsam_system_reset(s);
+}
+
+extern "C" int pbsam_system_reset(pbsam_system *s)
+{
+  if (!s) return fail(PBSAM_E_BADARG, "null system");
+  CK(cudaSetDevice(s->ctx->device));
+  pbsam_init_kernel<<<s->B, PBSAM_TEAM, 0, s->stream>>>(s->c);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s->stream));
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_system_destroy(pbsam_system *s)
+{
+  if (!s) return PBSAM_OK;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->stream);
+  for (void *p : s->bufs) cudaFree(p);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  s->ctx->live_systems--;
+  delete s;
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_system_set_stream(pbsam_system *s, void *stream)
+{
+  if (!s) return fail(PBSAM_E_BADARG, "null system");
+  s->stream = (cudaStream_t)stream;
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_system_set_poses(pbsam_system *s, const double *pos, const double *quat, int on_device)
+{
+  if (!s || !pos || !quat) return fail(PBSAM_E_BADARG, "null argument");
+  CK(cudaSetDevice(s->ctx->device));
+  const size_t n = (size_t)s->B * s->nmol;
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CK(cudaMemcpyAsync((void *)s->c.bv.pos, pos, n * 3 * sizeof(double), k, s->stream));
+  CK(cudaMemcpyAsync((void *)s->c.bv.quat, quat, n * 4 * sizeof(double), k, s->stream));
+  if (!on_device) CK(cudaStreamSynchronize(s->stream));
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_system_compute_forces(pbsam_system *s, double *force, double *torque, int *status, int on_device)
+{
+  if (!s) return fail(PBSAM_E_BADARG, "null system");
+  CK(cudaSetDevice(s->ctx->device));
+  CK(cudaEventRecord(s->ev0, s->stream));
+  pbsam_forces_kernel<<<s->B, PBSAM_TEAM, 0, s->stream>>>(s->c);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(s->ev1, s->stream));
+  const size_t n = (size_t)s->B * s->nmol * 3;
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (force) CK(cudaMemcpyAsync(force, s->c.bv.force, n * sizeof(double), k, s->stream));
+  if (torque) CK(cudaMemcpyAsync(torque, s->c.bv.torque, n * sizeof(double), k, s->stream));
+  if (status) CK(cudaMemcpyAsync(status, s->c.bv.status, s->B * sizeof(int), k, s->stream));
+  if (!on_device) {
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaEventElapsedTime(&s->last_ms, s->ev0, s->ev1));
+  }
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_system_compute_energy(pbsam_system *s, double *energy, int on_device)
+{
+  if (!s || !energy) return fail(PBSAM_E_BADARG, "null argument");
+  CK(cudaSetDevice(s->ctx->device));
+  pbsam_energy_kernel<<<s->B, PBSAM_TEAM, 0, s->stream>>>(s->c);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(energy, s->c.bv.energy, s->B * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s->stream));
+  if (!on_device) CK(cudaStreamSynchronize(s->stream));
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_system_stats(const pbsam_system *s, int *stats)
+{
+  if (!s || !stats) return fail(PBSAM_E_BADARG, "null argument");
+  CK(cudaSetDevice(s->ctx->device));
+  CK(cudaMemcpy(stats, s->c.bv.stats, (size_t)s->B * 8 * sizeof(int), cudaMemcpyDeviceToHost));
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_system_last_kernel_ms(const pbsam_system *s, double *ms)
+{
+  if (!s || !ms) return fail(PBSAM_E_BADARG, "null argument");
+  *ms = s->last_ms;
+  return PBSAM_OK;
+}

@@ -1,0 +1,1309 @@
+// CUDA kernels of the PB-SAM mutual-polarization drop-in (sm_100a, FP64).
+//
+// One team (a CTA of PBSAM_TEAM threads) owns one independent system and runs
+// the whole CMolecule::computeForces sequence for it in a single launch:
+// pair lists, the first round from self-polarized values, the selective
+// Gauss-Seidel sweeps, the per-molecule gradient solves and the force/torque
+// reduction, in exactly the order and with the stopping rules of the
+// reference (src/moldynamics.cpp:553-587, src/molecule.cpp:1988-2263).  Every
+// loop is bounded by the reference's own iteration caps; no thread ever waits
+// on another team.
+#include <cstdio>
+#include "pbsam_types.cuh"
+
+namespace pbsam {
+
+#define PBSAM_TEAM 256
+#define PBSAM_NCH 64            // max point chunks in a numeric expansion
+
+// ------------------------------------------------------------------ scratch
+struct Scr {
+  int NP2;
+  double *sh;            // (2NP)^2
+  double2 *R, *dR;       // rotation coefficients
+  double *TH, *dTH, *TF; // translation coefficients
+  double *kbuf, *fact;   // 2NP+2, NP
+  double *e;             // 16 * NP2
+  double *g;             // 8 * 3 * NP2
+  double *part;          // PBSAM_NCH * 3 * NP2
+  double *sol;           // 6 * 3 * NP2 (solver work)
+  double *misc;          // 4096
+  __device__ double *E(int i) const { return e + (size_t)i * NP2; }
+  __device__ double *G(int i) const { return g + (size_t)i * 3 * NP2; }
+};
+
+__host__ __device__ inline long long scr_doubles(int NP, long long S)
+{
+  const long long NP2 = (long long)NP * NP;
+  const int NN = 2 * NP - 1;
+  const long long rotE = rot_off(NN), trE = tr_off(NN);
+  long long n = 0;
+  n += 4LL * NP * NP;           // sh
+  n += 2 * 2 * rotE;            // R, dR (double2)
+  n += 3 * trE;                 // TH, dTH, TF
+  n += 2 * NP + 2 + NP + 8;     // kbuf, fact
+  n += 16 * NP2;                // e
+  n += 8 * 3 * NP2;             // g
+  n += (long long)PBSAM_NCH * 3 * NP2;   // part
+  n += 6 * 3 * NP2;             // sol
+  n += 4096 + S * S;            // misc + list building workspace
+  return n;
+}
+
+__device__ Scr make_scr(double *base, int NP)
+{
+  Scr s;
+  const int NP2 = NP * NP;
+  const int NN = 2 * NP - 1;
+  const long long rotE = rot_off(NN), trE = tr_off(NN);
+  s.NP2 = NP2;
+  double *p = base;
+  s.sh = p; p += 4 * NP * NP;
+  s.R = (double2 *)p; p += 2 * rotE;
+  s.dR = (double2 *)p; p += 2 * rotE;
+  s.TH = p; p += trE;
+  s.dTH = p; p += trE;
+  s.TF = p; p += trE;
+  s.kbuf = p; p += 2 * NP + 2;
+  s.fact = p; p += NP + 8;
+  s.e = p; p += 16 * NP2;
+  s.g = p; p += 8 * 3 * NP2;
+  s.part = p; p += (long long)PBSAM_NCH * 3 * NP2;
+  s.sol = p; p += 6 * 3 * NP2;
+  s.misc = p;
+  return s;
+}
+
+// ------------------------------------------------------------------ team helpers
+__device__ __forceinline__ void tcopy(const Team &tm, double *dst, const double *src, int n)
+{ for (int i = tm.rank; i < n; i += tm.size) dst[i] = src[i]; }
+__device__ __forceinline__ void tzero(const Team &tm, double *dst, int n)
+{ for (int i = tm.rank; i < n; i += tm.size) dst[i] = 0.0; }
+__device__ __forceinline__ void tadd(const Team &tm, double *dst, const double *src, int n)
+{ for (int i = tm.rank; i < n; i += tm.size) dst[i] += src[i]; }
+
+// deterministic tree sum (team size is a power of two)
+__device__ double team_sum(const Team &tm, double v, double *red)
+{
+  red[tm.rank] = v;
+  tm.sync();
+  for (int s = tm.size / 2; s > 0; s >>= 1) {
+    if (tm.rank < s) red[tm.rank] += red[tm.rank + s];
+    tm.sync();
+  }
+  double r = red[0];
+  tm.sync();
+  return r;
+}
+
+// per-pair truncation order (src/xforms.cpp:401-414), MAX_ERROR 1e-6
+__device__ __forceinline__ int compute_order(int NP, double rho, double TQ, double scale)
+{
+  if (TQ < 1e-10) return 1;
+  double c = rho / scale - 1;
+  if (c <= 1) return NP;
+  int p = int(log(TQ / (1e-6 * scale * (c - 1))) / log(c) - 1 + 0.5);
+  if (p < 1) p = 1;
+  if (p > NP) p = NP;
+  return p;
+}
+
+// ------------------------------------------------------------------ pair transforms
+// Prepared analytic re-expansion between two sphere centres
+// (CXFormA / CXFormAIntra, src/xforms.cpp:11-270).
+struct PairXf {
+  RotState rs;
+  TransState th, tf;
+  int pH, pF;
+  double Rm[9];
+};
+
+// Coefficients for re-expanding a source centred at c_src into a target centred
+// at c_tgt, P = c_tgt - c_src.  pF > 0 also prepares the unscreened (F) translation.
+__device__ void prep_pair(const Team &tm, const Tab &T, const Scr &sc, const double *P, int pH, int pF,
+                          double sS, double sT, bool grad, PairXf &X)
+{
+  const Sph S = cart2sph(P[0], P[1], P[2]);
+  const int prot = pF > pH ? pF : pH;
+  X.pH = pH; X.pF = pF;
+  rot_compute(tm, T, S.theta, S.phi, PB_PI, prot, grad, X.rs, sc.R, sc.dR, sc.sh);
+  trans_compute(tm, T, S.rho, T.kappa, pH, sS, sT, grad, X.th, sc.TH, sc.dTH, sc.kbuf);
+  if (pF > 0) trans_compute(tm, T, S.rho, 0.0, pF, sS, sT, false, X.tf, sc.TF, nullptr, sc.kbuf);
+  if (tm.rank == 0) {
+    sc.fact[0] = 1.0;
+    for (int n = 1; n < T.NP; n++) sc.fact[n] = sc.fact[n - 1] * (sT / sS);
+  }
+  // spherical-to-Cartesian gradient matrix (src/xforms.cpp:59-76)
+  const double ir = 1.0 / S.rho;
+  if (X.rs.sing) {
+    const double c = X.rs.cost;
+    double m[9] = {0.0, ir * c, 0.0, 0.0, 0.0, ir, c, 0.0, 0.0};
+    for (int i = 0; i < 9; i++) X.Rm[i] = m[i];
+  } else {
+    const double st = X.rs.sint, ct = X.rs.cost, sp = X.rs.exphi.y, cp = X.rs.exphi.x;
+    const double irst = ir / st, irct = ir * ct;
+    double m[9] = {st * cp, irct * cp, -irst * sp, st * sp, irct * sp, irst * cp, ct, -ir * st, 0.0};
+    for (int i = 0; i < 9; i++) X.Rm[i] = m[i];
+  }
+  tm.sync();
+}
+
+// rotate -> translate -> rotate back (src/xforms.cpp:122-132, 260-270); Mout zero-padded to NP
+__device__ void pair_apply(const Team &tm, const Tab &T, const Scr &sc, const PairXf &X, bool useF, const double *Min,
+                           double *Mout)
+{
+  const int p = useF ? X.pF : X.pH;
+  const TransState &ts = useF ? X.tf : X.th;
+  double *tM = sc.E(0), *tL = sc.E(1);
+  rot_apply(tm, X.rs, Min, tM, p, true, p);
+  tm.sync();
+  trans_apply(tm, ts, sc.fact, tM, tL, false, p);
+  tm.sync();
+  rot_apply(tm, X.rs, tL, Mout, p, false, T.NP);
+  tm.sync();
+}
+
+// gradient of the re-expansion w.r.t. the target position (src/xforms.cpp:85-115, 164-192);
+// G holds 3 expansions (x, y, z), each zero-padded to NP.
+__device__ void pair_apply_grad(const Team &tm, const Tab &T, const Scr &sc, const PairXf &X, const double *Min,
+                                double *G)
+{
+  const int p = X.pH, NP2 = T.NP * T.NP;
+  double *tM = sc.E(0), *tL = sc.E(1), *tmp = sc.E(2);
+  double *G0 = G, *G1 = G + NP2, *G2 = G + 2 * NP2;
+  rot_apply(tm, X.rs, Min, tM, p, true, p);
+  tm.sync();
+  trans_apply(tm, X.th, sc.fact, tM, tL, true, p);
+  tm.sync();
+  rot_apply(tm, X.rs, tL, G0, p, false, T.NP);
+  tm.sync();
+  trans_apply(tm, X.th, sc.fact, tM, tL, false, p);
+  tm.sync();
+  drot_apply(tm, T, X.rs, tL, G1, p, false, 0, T.NP);
+  drot_apply(tm, T, X.rs, tL, G2, p, false, 1, T.NP);
+  tm.sync();
+  drot_apply(tm, T, X.rs, Min, tM, p, true, 0, p);
+  tm.sync();
+  trans_apply(tm, X.th, sc.fact, tM, tL, false, p);
+  tm.sync();
+  rot_apply(tm, X.rs, tL, tmp, p, false, p);
+  tm.sync();
+  tadd(tm, G1, tmp, p * p);
+  tm.sync();
+  drot_apply(tm, T, X.rs, Min, tM, p, true, 1, p);
+  tm.sync();
+  trans_apply(tm, X.th, sc.fact, tM, tL, false, p);
+  tm.sync();
+  rot_apply(tm, X.rs, tL, tmp, p, false, p);
+  tm.sync();
+  tadd(tm, G2, tmp, p * p);
+  tm.sync();
+  for (int i = tm.rank; i < p * p; i += tm.size) {
+    const double a0 = G0[i], a1 = G1[i], a2 = G2[i];
+    G0[i] = X.Rm[0] * a0 + X.Rm[1] * a1 + X.Rm[2] * a2;
+    G1[i] = X.Rm[3] * a0 + X.Rm[4] * a1 + X.Rm[5] * a2;
+    G2[i] = X.Rm[6] * a0 + X.Rm[7] * a1 + X.Rm[8] * a2;
+  }
+  tm.sync();
+}
+
+// ------------------------------------------------------------------ numeric expansions
+// Expansion about the target centre of point charges located at pts[h] - shift
+// (CLocalExpan / CMulExpan / CGradExpan over charge sets, src/expansion.cpp:203-264,
+// src/triexpan.cpp:127-153).  NC = 1: weights w[h] (points with w == 0 skipped),
+// NC = 3: weights w[3h..3h+2] (points with |w|^2 < 1e-15 skipped, unit charge).
+// local: true = local expansion (k-hat radial part, e^{-kappa rho}/rho (a/rho)^n),
+// false = multipole ((rho/a)^n, unscreened).  out: NC expansions of NP2, P degrees
+// written, zero-padded to NP.
+template <int NC>
+__device__ void numeric_expand(const Team &tm, const Tab &T, const Scr &sc, const double *pts, int N,
+                               const double *shift, const double *w, bool local, bool kappa, int P, double scale,
+                               double *out)
+{
+  const int NP2 = T.NP * T.NP;
+  const int npair = (P + 1) / 2;
+  int C = tm.size / npair;
+  if (C > PBSAM_NCH) C = PBSAM_NCH;
+  if (C < 1) C = 1;
+  const int cp = tm.rank % npair, c = tm.rank / npair;
+  if (c < C) {
+    const int m1 = cp, m2 = P - 1 - cp;
+    const int n1 = P - m1;                      // degrees in column m1
+    double acc[NC][2 * 33 + 2];
+    for (int k = 0; k < NC; k++)
+      for (int i = 0; i < 2 * P + 2; i++) acc[k][i] = 0.0;
+    double rad[33];
+    for (int h = c; h < N; h += C) {
+      double wv[NC];
+      if (NC == 1) {
+        wv[0] = w[h];
+        if (wv[0] == 0.0) continue;
+      } else {
+        wv[0] = w[3 * h]; wv[1] = w[3 * h + 1]; wv[2] = w[3 * h + 2];
+        if (wv[0] * wv[0] + wv[1] * wv[1] + wv[2] * wv[2] < 1e-15) continue;
+      }
+      const double dx = pts[3 * h] - shift[0], dy = pts[3 * h + 1] - shift[1], dz = pts[3 * h + 2] - shift[2];
+      const Sph s = cart2sph(dx, dy, dz);
+      const double ch = (NC == 1) ? wv[0] : 1.0;
+      if (local) {
+        const double val = kappa ? s.rho * T.kappa : 0.0;
+        bessel_k(T, rad, P + 1, val);
+        double r = 1.0 / s.rho;
+        double k = ch * (r * (kappa ? exp(-val) : 1.0));
+        r *= scale;
+        for (int n = 0; n < P; n++) { rad[n] = rad[n] * k; k *= r; }
+      } else {
+        double k = ch;
+        const double r = s.rho * (1.0 / scale);
+        for (int n = 0; n < P; n++) { rad[n] = 1.0 * k; k *= r; }
+      }
+      double st, ct;
+      sincos(s.theta, &st, &ct);
+      auto body = [&](int base, int m0) {
+        return [&, base, m0](int n, double re, double im) {
+          const double rr = rad[n];
+          const int ix = base + 2 * (n - m0);
+          if (NC == 1) {
+            acc[0][ix] += re * rr;
+            acc[0][ix + 1] += im * rr;
+          } else {
+            const double vr = re * rr, vi = im * rr;
+            for (int k = 0; k < NC; k++) { acc[k][ix] += wv[k] * vr; acc[k][ix + 1] += wv[k] * vi; }
+          }
+        };
+      };
+      sh_column(T, ct, st, s.phi, m1, P, body(0, m1));
+      if (m2 != m1) sh_column(T, ct, st, s.phi, m2, P, body(2 * n1, m2));
+    }
+    // write this chunk's partials for the thread's columns
+    for (int k = 0; k < NC; k++) {
+      double *pp = sc.part + ((size_t)c * NC + k) * NP2;
+      for (int n = m1; n < P; n++) {
+        const int ix = 2 * (n - m1);
+        if (m1 == 0) pp[IDX(n)] = acc[k][ix];
+        else { pp[IDX(n) + 2 * m1 - 1] = acc[k][ix]; pp[IDX(n) + 2 * m1] = acc[k][ix + 1]; }
+      }
+      if (m2 != m1)
+        for (int n = m2; n < P; n++) {
+          const int ix = 2 * n1 + 2 * (n - m2);
+          if (m2 == 0) pp[IDX(n)] = acc[k][ix];
+          else { pp[IDX(n) + 2 * m2 - 1] = acc[k][ix]; pp[IDX(n) + 2 * m2] = acc[k][ix + 1]; }
+        }
+    }
+  }
+  tm.sync();
+  for (int i = tm.rank; i < NC * NP2; i += tm.size) {
+    const int k = i / NP2, j = i % NP2;
+    double v = 0.0;
+    if (j < P * P)
+      for (int cc = 0; cc < C; cc++) v += sc.part[((size_t)cc * NC + k) * NP2 + j];
+    out[(size_t)k * NP2 + j] = v;
+  }
+  tm.sync();
+}
+
+// ------------------------------------------------------------------ surface charges
+// q[h] = dA * sum_n (2 sum_{m>0} E(n,m) Y(n,m) c_n + E(n,0) Y(n,0) c_n) at each
+// exposed point (computeExposedSurfaceChargesFH, src/expcenter.cpp:1419-1440);
+// returns sum |q| over the points.  NC expansions E (stride NP2) share the
+// points and the per-degree factors c; q is written as q[NC*h + k].
+template <int NC>
+__device__ void surface_q(const Team &tm, const Tab &T, const double *pts, int N, double dA, const double *E,
+                          const double *cdeg, double *q, double *tot, double *red)
+{
+  const int NP = T.NP, NP2 = NP * NP;
+  double ta[NC];
+  for (int k = 0; k < NC; k++) ta[k] = 0.0;
+  for (int h = tm.rank; h < N; h += tm.size) {
+    const Sph s = cart2sph(pts[3 * h], pts[3 * h + 1], pts[3 * h + 2]);
+    double st, ct;
+    sincos(s.theta, &st, &ct);
+    double sn[NC][32], t0[NC][32];
+    for (int k = 0; k < NC; k++)
+      for (int n = 0; n < NP; n++) { sn[k][n] = 0.0; t0[k][n] = 0.0; }
+    for (int m = 0; m < NP; m++) {
+      sh_column(T, ct, st, s.phi, m, NP, [&](int n, double re, double im) {
+        const double c = cdeg[n];
+        for (int k = 0; k < NC; k++) {
+          const double *Ek = E + (size_t)k * NP2 + IDX(n);
+          if (m == 0) t0[k][n] = Ek[0] * (re * c);
+          else {
+            sn[k][n] += Ek[2 * m - 1] * (re * c);
+            sn[k][n] += Ek[2 * m] * (im * c);
+          }
+        }
+      });
+    }
+    for (int k = 0; k < NC; k++) {
+      double sum = 0.0;
+      for (int n = 0; n < NP; n++) {
+        double v = sn[k][n] * 2.0;
+        v += t0[k][n];
+        sum += v;
+      }
+      const double qq = sum * dA;
+      q[NC * h + k] = qq;
+      ta[k] += fabs(qq);
+    }
+  }
+  for (int k = 0; k < NC; k++) tot[k] = team_sum(tm, ta[k], red);
+}
+
+// ------------------------------------------------------------------ F/H inner solve
+// Fixed-point solve of one sphere's surface-charge expansions
+// (CSolExpCenter::solveFH, src/expcenter.cpp:1079-1370) for D = 1 (F, H) or
+// D = 3 (x, y, z gradients).  F and H (D*NP2) are updated in place; returns the
+// deviation of H from its value on entry (computeDev2).
+__device__ double solve_fh(const Team &tm, const Tab &T, const TypeView &tv, const SolveParams &prm, const Scr &sc,
+                           int ts, int D, double *F, double *H, const double *LF, const double *LH, double *red,
+                           int *stats)
+{
+  const int NP = T.NP, NP2 = NP * NP, len = D * NP2;
+  const double *cst = tv.cst + (size_t)ts * CST_N * NP;
+  const double *Dfix = tv.Dfix + (size_t)ts * NP2, *Vfix = tv.Vfix + (size_t)ts * NP2;
+  const double *IM = tv.imat + (size_t)ts * NP2 * NP2;
+  double *fbase = sc.sol, *hbase = sc.sol + len, *fx = sc.sol + 2 * len, *hx = sc.sol + 3 * len;
+  double *oldH = sc.sol + 4 * len, *outH = sc.sol + 5 * len;
+  for (int k = tm.rank; k < len; k += tm.size) {
+    const int kk = k % NP2;
+    int n = (int)sqrt((double)kk);
+    while (n * n > kk) n--;
+    while ((n + 1) * (n + 1) <= kk) n++;
+    if (D == 1) {
+      fbase[k] = Vfix[kk] + cst[CST_LH1 * NP + n] * LH[k] + cst[CST_LF1 * NP + n] * LF[k];
+      hbase[k] = Dfix[kk] + cst[CST_LH2 * NP + n] * LH[k] + cst[CST_LF2 * NP + n] * LF[k];
+    } else {
+      fbase[k] = cst[CST_LH1 * NP + n] * LH[k] + cst[CST_LF1 * NP + n] * LF[k];
+      hbase[k] = cst[CST_LH2 * NP + n] * LH[k] + cst[CST_LF2 * NP + n] * LF[k];
+    }
+    oldH[k] = H[k];
+    outH[k] = H[k];
+  }
+  tm.sync();
+  int ct = 0;
+  double dev = 0.0;
+  for (;;) {
+    for (int k = tm.rank; k < len; k += tm.size) {
+      const int kk = k % NP2;
+      int n = (int)sqrt((double)kk);
+      while (n * n > kk) n--;
+      while ((n + 1) * (n + 1) <= kk) n++;
+      fx[k] = fbase[k] + cst[CST_H1 * NP + n] * H[k] + cst[CST_F1 * NP + n] * F[k];
+    }
+    tm.sync();
+    for (int k = tm.rank; k < len; k += tm.size) {
+      const int d = k / NP2, i = k % NP2;
+      int n = (int)sqrt((double)i);
+      while (n * n > i) n--;
+      while ((n + 1) * (n + 1) <= i) n++;
+      const double *x = fx + d * NP2;
+      double s = 0.0;
+      for (int kk = 0; kk < NP2; kk++) s += IM[(size_t)kk * NP2 + i] * x[kk];
+      F[k] = s * T.CONST3[n];
+    }
+    tm.sync();
+    for (int k = tm.rank; k < len; k += tm.size) {
+      const int kk = k % NP2;
+      int n = (int)sqrt((double)kk);
+      while (n * n > kk) n--;
+      while ((n + 1) * (n + 1) <= kk) n++;
+      hx[k] = hbase[k] + cst[CST_H2 * NP + n] * H[k] + cst[CST_F2 * NP + n] * F[k];
+    }
+    tm.sync();
+    for (int k = tm.rank; k < len; k += tm.size) {
+      const int d = k / NP2, i = k % NP2;
+      int n = (int)sqrt((double)i);
+      while (n * n > i) n--;
+      while ((n + 1) * (n + 1) <= i) n++;
+      const double *x = hx + d * NP2;
+      double s = 0.0;
+      for (int kk = 0; kk < NP2; kk++) s += IM[(size_t)kk * NP2 + i] * x[kk];
+      H[k] = s * cst[CST_INVH * NP + n];
+    }
+    tm.sync();
+    // computeDev over complex entries (d, n, m)
+    double part = 0.0;
+    const int ncx = D * NP * (NP + 1) / 2;
+    for (int u = tm.rank; u < ncx; u += tm.size) {
+      const int d = u / (NP * (NP + 1) / 2), r = u % (NP * (NP + 1) / 2);
+      int n = (int)((sqrt(8.0 * r + 1.0) - 1.0) * 0.5);
+      while (n * (n + 1) / 2 > r) n--;
+      while ((n + 1) * (n + 2) / 2 <= r) n++;
+      const int m = r - n * (n + 1) / 2;
+      const int base = d * NP2 + IDX(n);
+      double ar, ai = 0.0, br, bi = 0.0;
+      if (m == 0) { ar = oldH[base]; br = H[base]; }
+      else { ar = oldH[base + 2 * m - 1]; ai = oldH[base + 2 * m]; br = H[base + 2 * m - 1]; bi = H[base + 2 * m]; }
+      const double PL = 1e-30;
+      double s;
+      if (fabs(ar) < PL && fabs(ai) < PL) {
+        if (fabs(br) < PL && fabs(bi) < PL) continue;
+        s = 1.0;
+      } else if (fabs(br) < PL && fabs(bi) < PL) s = 1.0;
+      else {
+        const double dr = ar - br, di = ai - bi;
+        const double top = dr * dr + di * di;
+        const double bot = ar * ar + ai * ai + br * br + bi * bi;
+        s = (m != 0) ? 2 * top / bot : top / bot;
+      }
+      part += s;
+    }
+    dev = team_sum(tm, part, red) / (4 * NP * NP);
+    for (int k = tm.rank; k < len; k += tm.size) oldH[k] = H[k];
+    tm.sync();
+    ct++;
+    if (!(dev > prm.solve_tol && ct < prm.solve_max_ct)) break;
+  }
+  if (tm.rank == 0 && stats) { stats[1] += ct; stats[2] += 1; }
+  // computeDev2 (outer deviation)
+  double pd = 0.0, ps = 0.0;
+  for (int u = tm.rank; u < len; u += tm.size) {
+    const int i = u % NP2;
+    int n = (int)sqrt((double)i);
+    while (n * n > i) n--;
+    const int mm = i - n * n;
+    const double a = outH[u], b = H[u], df = a - b;
+    const double w = (mm == 0) ? 1.0 : 2.0;
+    pd += w * (df * df);
+    ps += w * (a * a + b * b);
+  }
+  const double td = team_sum(tm, pd, red), tsm = team_sum(tm, ps, red);
+  return td / (4 * tsm) / double(D);
+}
+
+// ------------------------------------------------------------------ system state access
+struct Sys {
+  const Ctx *c;
+  int b, NP, NP2, S;
+  Scr sc;
+  double *red;
+  __device__ int ts(int s) const { return c->bv.sph_ts[s]; }
+  __device__ int mol(int s) const { return c->bv.sph_mol[s]; }
+  __device__ double rad(int s) const { return c->tv.rad[ts(s)]; }
+  __device__ size_t vs(int s) const { return ((size_t)b * S + s) * NP2; }
+  __device__ size_t gs(int s) const { return ((size_t)b * S + s) * 3 * NP2; }
+  __device__ size_t sc1(int s) const { return (size_t)b * S + s; }
+  __device__ double *F(int s) const { return c->bv.F + vs(s); }
+  __device__ double *H(int s) const { return c->bv.H + vs(s); }
+  __device__ double *Hrot(int s) const { return c->bv.Hrot + vs(s); }
+  __device__ double *HselfRot(int s) const { return c->bv.HselfRot + vs(s); }
+  __device__ double *LS(int s) const { return c->bv.LS + vs(s); }
+  __device__ double *LFS(int s) const { return c->bv.LFS + vs(s); }
+  __device__ double *LHS(int s) const { return c->bv.LHS + vs(s); }
+  __device__ double *gLHN(int s) const { return c->bv.gLHN + gs(s); }
+  __device__ double *gH(int s) const { return c->bv.gH + gs(s); }
+  __device__ int npts(int s) const { return c->bv.pt_off[s + 1] - c->bv.pt_off[s]; }
+  __device__ double *qF(int s) const { return c->bv.qF + (size_t)b * c->bv.SP + c->bv.pt_off[s]; }
+  __device__ double *qH(int s) const { return c->bv.qH + (size_t)b * c->bv.SP + c->bv.pt_off[s]; }
+  __device__ double *gFp(int s) const { return c->bv.gFp + ((size_t)b * c->bv.SP + c->bv.pt_off[s]) * 3; }
+  __device__ double *gHp(int s) const { return c->bv.gHp + ((size_t)b * c->bv.SP + c->bv.pt_off[s]) * 3; }
+  __device__ const double *spx(int s) const { return c->tv.spx + 3 * (size_t)c->tv.spx_off[ts(s)]; }
+  __device__ const double *cen(int s) const { return c->tv.cen + 3 * ts(s); }
+  __device__ double *cenRot(int s) const { return c->bv.cenRot + 3 * sc1(s); }
+  __device__ void cen_lab(int s, double *o) const
+  {
+    const int i = mol(s);
+    const double *p = c->bv.pos + 3 * ((size_t)b * c->bv.nmol + i);
+    const double *r = cenRot(s);
+    o[0] = p[0] + r[0]; o[1] = p[1] + r[1]; o[2] = p[2] + r[2];
+  }
+  __device__ int *ipol(int s) const { return c->bv.ipol + ((size_t)b * S + s) * S; }
+  __device__ int nipol(int s) const { return c->bv.ipol_n[sc1(s)]; }
+  __device__ int *iact(int s) const { return c->bv.iact + ((size_t)b * S + s) * S; }
+  __device__ int niact(int s) const { return c->bv.iact_n[sc1(s)]; }
+  __device__ double *gw(double *base, int k) const { return base + ((size_t)b * S + k) * 3 * NP2; }
+  __device__ int *stats() const { return c->bv.stats + (size_t)b * 8; }
+  // molecule rotation state (coefficients computed once per call)
+  __device__ RotState molrot(int i) const
+  {
+    RotState rs;
+    const double *v = c->bv.molRS + ((size_t)b * c->bv.nmol + i) * 16;
+    rs.p = NP;
+    rs.sing = v[0] != 0.0;
+    rs.cost = v[1]; rs.sint = v[2]; rs.cott = v[3]; rs.xi = v[4];
+    rs.exphi = make_double2(v[5], v[6]);
+    rs.exiphi = cconj(rs.exphi);
+    rs.exxi = make_double2(v[7], v[8]);
+    rs.R = c->bv.molR + ((size_t)b * c->bv.nmol + i) * rot_off(2 * NP - 1);
+    rs.dR = nullptr;
+    return rs;
+  }
+};
+
+__device__ void add_vec_into(const Team &tm, double *dst, const double *src, int n)
+{
+  for (int i = tm.rank; i < n; i += tm.size) dst[i] += src[i];
+  tm.sync();
+}
+
+// LS from the inter-molecular polarization neighbours (src/molecule.cpp:1265-1358)
+__device__ void reexpand_LS(const Team &tm, const Sys &y, int s, bool fromSelf)
+{
+  const Tab &T = y.c->T;
+  double *LSrot = y.sc.E(6), *tL = y.sc.E(7);
+  tzero(tm, LSrot, y.NP2);
+  tm.sync();
+  const int *lst = y.ipol(s);
+  const int nl = y.nipol(s);
+  double ci[3];
+  y.cen_lab(s, ci);
+  for (int e = 0; e < nl; e++) {
+    const int s2 = lst[e];
+    double cj[3];
+    y.cen_lab(s2, cj);
+    const double P[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+    const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+    const double TQ = fromSelf ? y.c->tv.tHself[y.ts(s2)] : y.c->bv.tH[y.sc1(s2)];
+    const int p = compute_order(y.NP, rho, TQ, y.rad(s2));
+    PairXf X;
+    prep_pair(tm, T, y.sc, P, p, 0, y.rad(s2), y.rad(s), false, X);
+    pair_apply(tm, T, y.sc, X, false, fromSelf ? y.HselfRot(s2) : y.Hrot(s2), tL);
+    add_vec_into(tm, LSrot, tL, y.NP2);
+  }
+  const RotState mr = y.molrot(y.mol(s));
+  rot_apply_xi(tm, mr, LSrot, y.LS(s), y.NP, false, y.NP);
+  tm.sync();
+}
+
+// F/H solve + surface charges of one sphere (src/expcenter.cpp:594-629)
+__device__ double solve_surface(const Team &tm, const Sys &y, int s, bool rotH)
+{
+  const Tab &T = y.c->T;
+  const int ts = y.ts(s);
+  double dv = solve_fh(tm, T, y.c->tv, y.c->prm, y.sc, ts, 1, y.F(s), y.H(s), y.LFS(s), y.LHS(s), y.red, y.stats());
+  if (rotH) {
+    const RotState mr = y.molrot(y.mol(s));
+    rot_apply_xi(tm, mr, y.H(s), y.Hrot(s), y.NP, true, y.NP);
+  }
+  const double *cst = y.c->tv.cst + (size_t)ts * CST_N * y.NP;
+  const double dA = 4 * PB_PI / double(y.c->tv.nspx[ts]);
+  double tot[1];
+  surface_q<1>(tm, T, y.spx(s), y.npts(s), dA, y.F(s), T.CONST2, y.qF(s), tot, y.red);
+  double tF = tot[0];
+  surface_q<1>(tm, T, y.spx(s), y.npts(s), dA, y.H(s), cst + CST_CHGH * y.NP, y.qH(s), tot, y.red);
+  if (tm.rank == 0) {
+    y.c->bv.tF[y.sc1(s)] = tF;
+    y.c->bv.tH[y.sc1(s)] = tot[0];
+    y.c->bv.hscale[y.sc1(s)] = 1.0 / y.rad(s);
+    y.c->bv.dev[y.sc1(s)] = dv;
+  }
+  tm.sync();
+  return dv;
+}
+
+__device__ double recompute_from_self(const Team &tm, const Sys &y, int s)   // src/molecule.cpp:1136-1160
+{
+  const int ts = y.ts(s);
+  reexpand_LS(tm, y, s, true);
+  const double *LHi = y.c->tv.LHintra + (size_t)ts * y.NP2, *LFi = y.c->tv.LFintra + (size_t)ts * y.NP2;
+  const double *Fs = y.c->tv.Fself + (size_t)ts * y.NP2, *Hs = y.c->tv.Hself + (size_t)ts * y.NP2;
+  for (int i = tm.rank; i < y.NP2; i += tm.size) {
+    y.LHS(s)[i] = y.LS(s)[i] + LHi[i];
+    y.LFS(s)[i] = LFi[i];
+    y.F(s)[i] = Fs[i];
+    y.H(s)[i] = Hs[i];
+  }
+  tm.sync();
+  return solve_surface(tm, y, s, true);
+}
+
+// intra near re-expansion with the latest values (src/molecule.cpp:1413-1473)
+__device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s)
+{
+  const Tab &T = y.c->T;
+  const int ts = y.ts(s), i = y.mol(s);
+  const int mo = y.c->bv.mol_off[i];
+  const int to = y.c->tv.type_off[y.c->bv.mol_type[i]];
+  double *a = y.sc.E(7), *bq = y.sc.E(8);
+  tzero(tm, y.LFS(s), y.NP2);
+  tcopy(tm, y.LHS(s), y.LS(s), y.NP2);
+  tm.sync();
+  const double *ci = y.cen(s);
+  for (int e = y.c->tv.near_off[ts]; e < y.c->tv.near_off[ts + 1]; e++) {
+    const int kj = y.c->tv.near[e];
+    const int s2 = mo + kj;
+    const double *cj = y.c->tv.cen + 3 * (to + kj);
+    const double P[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+    const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+    const double rj = y.rad(s2);
+    const double sep = rho - y.rad(s) - rj;
+    const int pF = compute_order(y.NP, rho, y.c->bv.tF[y.sc1(s2)], rj);
+    const int pH = compute_order(y.NP, rho, y.c->bv.tH[y.sc1(s2)], rj);
+    if (sep > 0 && !(sep < y.c->prm.min_sep_numeric)) {
+      PairXf X;
+      prep_pair(tm, T, y.sc, P, pH, pF, rj, y.rad(s), false, X);
+      pair_apply(tm, T, y.sc, X, true, y.F(s2), a);
+      pair_apply(tm, T, y.sc, X, false, y.H(s2), bq);
+    } else {
+      numeric_expand<1>(tm, T, y.sc, y.spx(s2), y.npts(s2), P, y.qF(s2), true, false, pF, y.rad(s), a);
+      numeric_expand<1>(tm, T, y.sc, y.spx(s2), y.npts(s2), P, y.qH(s2), true, true, pH, y.rad(s), bq);
+    }
+    for (int t = tm.rank; t < y.NP2; t += tm.size) { y.LFS(s)[t] += a[t]; y.LHS(s)[t] += bq[t]; }
+    tm.sync();
+  }
+}
+
+__device__ double recompute(const Team &tm, const Sys &y, int s)             // src/molecule.cpp:1168-1229
+{
+  const int ts = y.ts(s);
+  reexpand_LS(tm, y, s, false);
+  reexpand_intra_near(tm, y, s);
+  const double *LHf = y.c->tv.LHfar + (size_t)ts * y.NP2, *LFf = y.c->tv.LFfar + (size_t)ts * y.NP2;
+  for (int i = tm.rank; i < y.NP2; i += tm.size) { y.LHS(s)[i] += LHf[i]; y.LFS(s)[i] += LFf[i]; }
+  tm.sync();
+  return solve_surface(tm, y, s, false);
+}
+
+// gradient re-expansion of neighbour m's rotated H into sphere s, accumulated in acc (3*NP2)
+__device__ void grad_xform_from(const Team &tm, const Sys &y, int s, int sm, bool self, double *acc)
+{
+  const Tab &T = y.c->T;
+  double ci[3], cm[3];
+  y.cen_lab(s, ci);
+  y.cen_lab(sm, cm);
+  const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+  const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+  const double TQ = self ? y.c->tv.tHself[y.ts(sm)] : y.c->bv.tH[y.sc1(sm)];
+  const int p = compute_order(y.NP, rho, TQ, y.rad(sm));
+  PairXf X;
+  prep_pair(tm, T, y.sc, P, p, 0, y.rad(sm), y.rad(s), true, X);
+  double *G = y.sc.G(0);
+  pair_apply_grad(tm, T, y.sc, X, self ? y.HselfRot(sm) : y.Hrot(sm), G);
+  add_vec_into(tm, acc, G, 3 * y.NP2);
+}
+
+__device__ void prepare_dta_iself(const Team &tm, const Sys &y, int s)     // src/molecule.cpp:1584-1628
+{
+  double *acc = y.gLHN(s);
+  tzero(tm, acc, 3 * y.NP2);
+  tm.sync();
+  for (int e = 0; e < y.nipol(s); e++) grad_xform_from(tm, y, s, y.ipol(s)[e], true, acc);
+  for (int e = 0; e < y.niact(s); e++) grad_xform_from(tm, y, s, y.iact(s)[e], true, acc);
+}
+
+// one gradient recompute of sphere s w.r.t. molecule j (src/molecule.cpp:1680-1843)
+__device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int key)
+{
+  const Tab &T = y.c->T;
+  const BatchView &bv = y.c->bv;
+  const int NP2 = y.NP2, i = y.mol(s), ts = y.ts(s);
+  double *tGrot = y.sc.G(1), *LGH = y.sc.G(2), *LGF = y.sc.G(3), *LGH2 = y.sc.G(4), *tmpG = y.sc.G(5);
+  double *tL = y.sc.E(7);
+  tcopy(tm, tGrot, y.gw(bv.tGw, key), 3 * NP2);
+  tm.sync();
+  double ci[3];
+  y.cen_lab(s, ci);
+  for (int e = 0; e < y.nipol(s); e++) {
+    const int sm = y.ipol(s)[e];
+    if (i != j && y.mol(sm) != j) continue;
+    double cm[3];
+    y.cen_lab(sm, cm);
+    const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+    const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+    const int p = compute_order(y.NP, rho, bv.maxgH[y.sc1(sm)], y.rad(sm));
+    PairXf X;
+    prep_pair(tm, T, y.sc, P, p, 0, y.rad(sm), y.rad(s), false, X);
+    const double *src = y.gw(bv.gHrotw, bv.gkey[y.sc1(sm)]);
+    for (int cc = 0; cc < 3; cc++) {
+      pair_apply(tm, T, y.sc, X, false, src + cc * NP2, tL);
+      add_vec_into(tm, tGrot + cc * NP2, tL, NP2);
+    }
+  }
+  const RotState mr = y.molrot(i);
+  for (int cc = 0; cc < 3; cc++) rot_apply_xi(tm, mr, tGrot + cc * NP2, LGH + cc * NP2, y.NP, false, y.NP);
+  tm.sync();
+  if (j == i) { tcopy(tm, y.gLHN(s), LGH, 3 * NP2); tm.sync(); }
+  tzero(tm, LGF, 3 * NP2);
+  tzero(tm, LGH2, 3 * NP2);
+  tm.sync();
+  // intra list of the gradient: molecule j's polarized spheres (i == j) or
+  // i's spheres polarized by j (i != j)
+  const int nlist = (i == j) ? bv.intraPol_n[(size_t)y.b * bv.nmol + j] : bv.interMol_n[(size_t)y.b * bv.nmol + j];
+  const int *lst = (i == j) ? bv.intraPol + ((size_t)y.b * bv.nmol + j) * y.S : bv.interMol + ((size_t)y.b * bv.nmol + j) * y.S;
+  const double *cis = y.cen(s);
+  for (int e = 0; e < nlist; e++) {
+    const int sm = lst[e];
+    if (i != j && y.mol(sm) != i) continue;
+    if (sm == s) continue;
+    const double *cms = y.cen(sm);
+    const double P[3] = {cis[0] - cms[0], cis[1] - cms[1], cis[2] - cms[2]};
+    const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+    const double rm = y.rad(sm);
+    const double sep = rho - y.rad(s) - rm;
+    const int pF = compute_order(y.NP, rho, bv.maxgF[y.sc1(sm)], rm);
+    const int pH = compute_order(y.NP, rho, bv.maxgH[y.sc1(sm)], rm);
+    if (sep > 0 && !(sep < y.c->prm.min_sep_numeric)) {
+      PairXf X;
+      prep_pair(tm, T, y.sc, P, pH, pF, rm, y.rad(s), false, X);
+      const int km = bv.gkey[y.sc1(sm)];
+      for (int cc = 0; cc < 3; cc++) {
+        pair_apply(tm, T, y.sc, X, true, y.gw(bv.gFw, km) + cc * NP2, tL);
+        add_vec_into(tm, LGF + cc * NP2, tL, NP2);
+        pair_apply(tm, T, y.sc, X, false, y.gw(bv.gHw, km) + cc * NP2, tL);
+        add_vec_into(tm, LGH2 + cc * NP2, tL, NP2);
+      }
+    } else {
+      numeric_expand<3>(tm, T, y.sc, y.spx(sm), y.npts(sm), P, y.gFp(sm), true, false, pF, y.rad(s), tmpG);
+      add_vec_into(tm, LGF, tmpG, 3 * NP2);
+      numeric_expand<3>(tm, T, y.sc, y.spx(sm), y.npts(sm), P, y.gHp(sm), true, true, pH, y.rad(s), tmpG);
+      add_vec_into(tm, LGH2, tmpG, 3 * NP2);
+    }
+  }
+  add_vec_into(tm, LGH, LGH2, 3 * NP2);
+  double *gF = y.gw(bv.gFw, key), *gHk = y.gw(bv.gHw, key);
+  const double dv = solve_fh(tm, T, y.c->tv, y.c->prm, y.sc, ts, 3, gF, gHk, LGF, LGH, y.red, y.stats());
+  for (int cc = 0; cc < 3; cc++) rot_apply_xi(tm, mr, gHk + cc * NP2, y.gw(bv.gHrotw, key) + cc * NP2, y.NP, true, y.NP);
+  tm.sync();
+  // exposed gradient charges (src/expcenter.cpp:1377-1412)
+  const double *cst = y.c->tv.cst + (size_t)ts * CST_N * y.NP;
+  const double dA = 4 * PB_PI / double(y.c->tv.nspx[ts]);
+  double totF[3], totH[3];
+  surface_q<3>(tm, T, y.spx(s), y.npts(s), dA, gF, T.CONST2, y.gFp(s), totF, y.red);
+  surface_q<3>(tm, T, y.spx(s), y.npts(s), dA, gHk, cst + CST_CHGH * y.NP, y.gHp(s), totH, y.red);
+  if (tm.rank == 0) {
+    double mf = totF[0] > totF[1] ? totF[0] : totF[1];
+    if (totF[2] > mf) mf = totF[2];
+    double mh = totH[0] > totH[1] ? totH[0] : totH[1];
+    if (totH[2] > mh) mh = totH[2];
+    bv.maxgF[y.sc1(s)] = mf;
+    bv.maxgH[y.sc1(s)] = mh;
+    bv.dev[y.sc1(s)] = dv;
+    y.stats()[3] += 1;
+  }
+  tm.sync();
+  return dv;
+}
+
+// multipole-local inner product with scale bookkeeping (src/expansion.h:705-741)
+__device__ double inprod_ml(const double *M, double mscale, const double *L, double lscale, int NP)
+{
+  double sum = 0.0, fact = 1 / (mscale * lscale), scale = 1.0;
+  for (int n = 0; n < NP; n++) {
+    double s = 0.0;
+    for (int mm = 1; mm < 2 * n + 1; mm++) s += M[IDX(n) + mm] * L[IDX(n) + mm];
+    s *= 2.0;
+    s += M[IDX(n)] * L[IDX(n)];
+    sum += scale * s;
+    scale *= fact;
+  }
+  return sum;
+}
+
+// ------------------------------------------------------------------ the force kernel
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
+{
+  __shared__ double red[PBSAM_TEAM];
+  __shared__ double shv[16];
+  const Team tm{(int)threadIdx.x, (int)blockDim.x};
+  const BatchView &bv = c.bv;
+  const int b = blockIdx.x;
+  if (b >= bv.B) return;
+  Sys y;
+  y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = bv.S;
+  y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP);
+  y.red = red;
+  const int S = bv.S, nmol = bv.nmol, NP2 = y.NP2;
+  int *st = y.stats();
+  if (tm.rank == 0) {
+    for (int k = 0; k < 8; k++) st[k] = 0;
+    bv.status[b] = PBSAM_STATUS_OK;
+  }
+  for (int t = tm.rank; t < nmol * 3; t += tm.size) {
+    bv.force[(size_t)b * nmol * 3 + t] = 0.0;
+    bv.torque[(size_t)b * nmol * 3 + t] = 0.0;
+  }
+  // sphere centres for this pose (CMolecule::rotate / rotateCenters)
+  for (int s = tm.rank; s < S; s += tm.size) {
+    const double *q = bv.quat + 4 * ((size_t)b * nmol + y.mol(s));
+    double qn[4];
+    const double in = 1.0 / sqrt((q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) + q[0] * q[0]);
+    qn[0] = q[0] * in; qn[1] = q[1] * in; qn[2] = q[2] * in; qn[3] = q[3] * in;
+    qrot(qn, y.cen(s), y.cenRot(s));
+  }
+  tm.sync();
+  if (nmol == 1) return;
+  // ---- pair lists (src/molecule.cpp:1035-1126, 122-166)
+  double *sep = bv.sep + (size_t)b * S * S;
+  for (int u = tm.rank; u < S * S; u += tm.size) {
+    const int s1 = u / S, s2 = u % S;
+    double a[3], d[3];
+    y.cen_lab(s1, a);
+    y.cen_lab(s2, d);
+    const double dx = a[0] - d[0], dy = a[1] - d[1], dz = a[2] - d[2];
+    sep[u] = sqrt(dx * dx + dy * dy + dz * dz) - y.rad(s1) - y.rad(s2);
+  }
+  tm.sync();
+  if (tm.rank == 0) {
+    int ok = 1;
+    for (int s = 0; s < S; s++) { bv.ipol_n[y.sc1(s)] = 0; bv.iact_n[y.sc1(s)] = 0; }
+    for (int i = 0; i < nmol; i++) bv.interX[(size_t)b * nmol + i] = 0;
+    for (int j = 1; j < nmol && ok; j++) {
+      int neigh[64];
+      int nn = 0;
+      for (int i = 0; i < j; i++) {
+        const double *pi = bv.pos + 3 * ((size_t)b * nmol + i), *pj = bv.pos + 3 * ((size_t)b * nmol + j);
+        const double dx = pi[0] - pj[0], dy = pi[1] - pj[1], dz = pi[2] - pj[2];
+        const double c2c = sqrt(dx * dx + dy * dy + dz * dz);
+        const double ms = c2c - c.tv.maxR[bv.mol_type[i]] - c.tv.maxR[bv.mol_type[j]];
+        if (ms < c.prm.interact_cut && nn < 64) neigh[nn++] = i;
+      }
+      for (int kj = bv.mol_off[j]; kj < bv.mol_off[j + 1] && ok; kj++)
+        for (int ii = 0; ii < nn && ok; ii++) {
+          const int i = neigh[ii];
+          for (int ki = bv.mol_off[i]; ki < bv.mol_off[i + 1]; ki++) {
+            const double g = sep[(size_t)ki * S + kj];
+            if (g <= 0) { ok = 0; break; }
+            if (g < c.prm.interact_cut) {
+              if (g > c.prm.inter_cut) {
+                y.iact(ki)[bv.iact_n[y.sc1(ki)]++] = kj;
+                y.iact(kj)[bv.iact_n[y.sc1(kj)]++] = ki;
+              } else {
+                y.ipol(ki)[bv.ipol_n[y.sc1(ki)]++] = kj;
+                y.ipol(kj)[bv.ipol_n[y.sc1(kj)]++] = ki;
+              }
+              bv.interX[(size_t)b * nmol + i] = 1;
+              bv.interX[(size_t)b * nmol + j] = 1;
+            }
+          }
+        }
+    }
+    if (!ok) bv.status[b] = PBSAM_STATUS_OVERLAP;
+    else {
+      for (int i = 0; i < nmol; i++) bv.interMol_n[(size_t)b * nmol + i] = 0;
+      for (int s = 0; s < S; s++) {
+        int added = 0;   // molecules already credited (bit mask; nmol <= 32 here)
+        for (int e = 0; e < y.nipol(s); e++) {
+          const int j = y.mol(y.ipol(s)[e]);
+          if (added & (1 << j)) continue;
+          int &n = bv.interMol_n[(size_t)b * nmol + j];
+          bv.interMol[((size_t)b * nmol + j) * S + n++] = s;
+          added |= (1 << j);
+        }
+      }
+      for (int j = 0; j < nmol; j++) {
+        int &np = bv.intraPol_n[(size_t)b * nmol + j], &na = bv.intraAct_n[(size_t)b * nmol + j];
+        np = 0; na = 0;
+        for (int s = bv.mol_off[j]; s < bv.mol_off[j + 1]; s++) {
+          if (y.nipol(s) > 0) bv.intraPol[((size_t)b * nmol + j) * S + np++] = s;
+          else if (y.niact(s) > 0) bv.intraAct[((size_t)b * nmol + j) * S + na++] = s;
+        }
+      }
+    }
+  }
+  tm.sync();
+  if (bv.status[b] != PBSAM_STATUS_OK) return;
+  const Tab &T = c.T;
+  // ---- polarize_mutual: molecule rotations, rotated self H (src/molecule.cpp:2002-2015)
+  for (int i = 0; i < nmol; i++) {
+    if (!bv.interX[(size_t)b * nmol + i]) continue;
+    const double *q = bv.quat + 4 * ((size_t)b * nmol + i);
+    double qn[4];
+    const double in = 1.0 / sqrt((q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) + q[0] * q[0]);
+    qn[0] = q[0] * in; qn[1] = q[1] * in; qn[2] = q[2] * in; qn[3] = q[3] * in;
+    double th, ph, xi;
+    quat_angles(qn, th, ph, xi);
+    RotState rs;
+    double2 *Rm = bv.molR + ((size_t)b * nmol + i) * rot_off(2 * y.NP - 1);
+    rot_compute(tm, T, th, ph, xi, y.NP, false, rs, Rm, nullptr, y.sc.sh);
+    if (tm.rank == 0) {
+      double *v = bv.molRS + ((size_t)b * nmol + i) * 16;
+      v[0] = rs.sing ? 1.0 : 0.0; v[1] = rs.cost; v[2] = rs.sint; v[3] = rs.cott; v[4] = rs.xi;
+      v[5] = rs.exphi.x; v[6] = rs.exphi.y; v[7] = rs.exxi.x; v[8] = rs.exxi.y;
+    }
+    tm.sync();
+    const RotState mr = y.molrot(i);
+    for (int s = bv.mol_off[i]; s < bv.mol_off[i + 1]; s++) {
+      if (y.nipol(s) == 0 && y.niact(s) == 0) continue;
+      rot_apply_xi(tm, mr, c.tv.Hself + (size_t)y.ts(s) * NP2, y.HselfRot(s), y.NP, true, y.NP);
+      tm.sync();
+      tcopy(tm, y.Hrot(s), y.HselfRot(s), NP2);
+      tm.sync();
+    }
+  }
+  // ---- first round from self values
+  double dev = 0.0, MAXDEV = 0.0;
+  int mtotal = 0;
+  {
+    double maxdevs[32];
+    for (int i = 0; i < nmol && i < 32; i++) maxdevs[i] = 0.0;
+    for (int i = 0; i < nmol; i++) {
+      double dmol = 0.0;
+      if (bv.interX[(size_t)b * nmol + i])
+        for (int s = bv.mol_off[i]; s < bv.mol_off[i + 1]; s++) {
+          if (y.nipol(s) == 0) continue;
+          const double d = recompute_from_self(tm, y, s);
+          dmol += d;
+          if (maxdevs[i] < d) maxdevs[i] = d;
+          mtotal++;
+        }
+      dev += dmol;
+    }
+    for (int i = 0; i < nmol; i++) if (maxdevs[i] > MAXDEV) MAXDEV = maxdevs[i];
+  }
+  int ct = 1;
+  const double itot = (mtotal > 0 ? 1.0 / mtotal : 0);
+  const double tol2 = c.prm.max_polar_dev * c.prm.max_polar_dev;
+  while (dev * itot > tol2 && ct < c.prm.max_pol_rounds) {
+    dev = 0.0;
+    double maxdevs[32];
+    for (int i = 0; i < nmol && i < 32; i++) maxdevs[i] = 0.0;
+    for (int i = 0; i < nmol; i++) {
+      double dmol = 0.0;
+      if (bv.interX[(size_t)b * nmol + i])
+        for (int s = bv.mol_off[i]; s < bv.mol_off[i + 1]; s++) {
+          if (y.nipol(s) == 0) continue;
+          double d = bv.dev[y.sc1(s)];
+          if (d > 0.1 * MAXDEV) d = recompute(tm, y, s);
+          if (maxdevs[i] < d) maxdevs[i] = d;
+          dmol += d;
+        }
+      dev += dmol;
+    }
+    MAXDEV = 0.0;
+    for (int i = 0; i < nmol; i++) if (maxdevs[i] > MAXDEV) MAXDEV = maxdevs[i];
+    ct++;
+  }
+  if (tm.rank == 0) {
+    st[0] = ct;
+    if (dev * itot > tol2) st[4] = 1;   // polarization hit the sweep cap
+  }
+  // ---- gradient phase (src/molecule.cpp:2081-2228)
+  for (int j = 0; j < nmol; j++) {
+    const int ni = bv.interMol_n[(size_t)b * nmol + j];
+    if (ni == 0) {
+      if (bv.interX[(size_t)b * nmol + j])
+        for (int s = bv.mol_off[j]; s < bv.mol_off[j + 1]; s++)
+          if (y.nipol(s) > 0 || y.niact(s) > 0) prepare_dta_iself(tm, y, s);
+      continue;
+    }
+    const int na = bv.intraPol_n[(size_t)b * nmol + j];
+    const int jsize = ni + na;
+    const double itj = 1.0 / double(jsize);
+    const int *inter = bv.interMol + ((size_t)b * nmol + j) * S;
+    const int *intra = bv.intraPol + ((size_t)b * nmol + j) * S;
+    for (int s = tm.rank; s < S; s += tm.size) bv.gkey[y.sc1(s)] = -1;
+    tm.sync();
+    for (int k = tm.rank; k < jsize; k += tm.size) bv.gkey[y.sc1(k < ni ? inter[k] : intra[k - ni])] = k;
+    for (int k = 0; k < jsize; k++) {
+      tzero(tm, y.gw(bv.gFw, k), 3 * NP2);
+      tzero(tm, y.gw(bv.gHw, k), 3 * NP2);
+      tzero(tm, y.gw(bv.gHrotw, k), 3 * NP2);
+      tzero(tm, y.gw(bv.tGw, k), 3 * NP2);
+    }
+    tm.sync();
+    // prepareDTA (src/molecule.cpp:1483-1571)
+    for (int k = 0; k < jsize; k++) {
+      const int s = k < ni ? inter[k] : intra[k - ni];
+      double *acc = y.gw(bv.tGw, k);
+      if (k < ni) {
+        for (int e = 0; e < y.nipol(s); e++) {
+          const int sm = y.ipol(s)[e];
+          if (y.mol(sm) != j) continue;
+          grad_xform_from(tm, y, s, sm, false, acc);
+        }
+      } else {
+        for (int e = 0; e < y.nipol(s); e++) grad_xform_from(tm, y, s, y.ipol(s)[e], false, acc);
+        for (int e = 0; e < y.niact(s); e++) grad_xform_from(tm, y, s, y.iact(s)[e], false, acc);
+      }
+    }
+    double *dg = bv.dgrad + (size_t)b * S;
+    double dv = 0.0;
+    for (int k = 0; k < jsize; k++) {
+      const int s = k < ni ? inter[k] : intra[k - ni];
+      const double d = recompute_grad(tm, y, s, j, k);
+      if (tm.rank == 0) dg[k] = d;
+      dv += d;
+    }
+    tm.sync();
+    int gct = 1, k = 0;
+    while (dv * itj > tol2 && gct < c.prm.max_pol_rounds) {
+      dv -= dg[k];
+      const int s = k < ni ? inter[k] : intra[k - ni];
+      const double d = recompute_grad(tm, y, s, j, k);
+      tm.sync();
+      if (tm.rank == 0) dg[k] = d;
+      tm.sync();
+      dv += d;
+      k++;
+      if (k == jsize) { k = 0; gct++; }
+    }
+    for (int h = 0; h < na; h++) {
+      const int s = intra[h];
+      tcopy(tm, y.gH(s), y.gw(bv.gHw, bv.gkey[y.sc1(s)]), 3 * NP2);
+    }
+    tm.sync();
+    const int nact = bv.intraAct_n[(size_t)b * nmol + j];
+    for (int h = 0; h < nact; h++) prepare_dta_iself(tm, y, bv.intraAct[((size_t)b * nmol + j) * S + h]);
+  }
+  tm.sync();
+  // ---- forces and torques (src/moldynamics.cpp:524-550, src/expcenter.cpp:123-149)
+  double *fk = y.sc.misc;   // [S][3]
+  for (int s = tm.rank; s < S; s += tm.size) {
+    double f[3] = {0.0, 0.0, 0.0};
+    const int i = y.mol(s);
+    if (bv.interX[(size_t)b * nmol + i] && (y.nipol(s) > 0 || y.niact(s) > 0)) {
+      const double r = y.rad(s);
+      for (int cc = 0; cc < 3; cc++) {
+        if (y.nipol(s) > 0) {
+          f[cc] -= inprod_ml(y.H(s), 1.0 / r, y.gLHN(s) + cc * NP2, r, y.NP);
+          f[cc] -= inprod_ml(y.gH(s) + cc * NP2, 1.0 / r, y.LS(s), r, y.NP);
+        } else {
+          f[cc] -= inprod_ml(c.tv.Hself + (size_t)y.ts(s) * NP2, c.tv.hself_scale[y.ts(s)], y.gLHN(s) + cc * NP2, r, y.NP);
+        }
+      }
+    }
+    fk[3 * s] = f[0]; fk[3 * s + 1] = f[1]; fk[3 * s + 2] = f[2];
+  }
+  tm.sync();
+  if (tm.rank < nmol) {
+    const int i = tm.rank;
+    double F[3] = {0, 0, 0}, Tq[3] = {0, 0, 0};
+    if (bv.interX[(size_t)b * nmol + i])
+      for (int s = bv.mol_off[i]; s < bv.mol_off[i + 1]; s++) {
+        if (y.nipol(s) == 0 && y.niact(s) == 0) continue;
+        const double *f = fk + 3 * s, *cn = y.cen(s);
+        F[0] += f[0]; F[1] += f[1]; F[2] += f[2];
+        Tq[0] += cn[1] * f[2] - cn[2] * f[1];
+        Tq[1] += cn[2] * f[0] - cn[0] * f[2];
+        Tq[2] += cn[0] * f[1] - cn[1] * f[0];
+      }
+    const double *q = bv.quat + 4 * ((size_t)b * nmol + i);
+    double qn[4];
+    double in = 1.0 / sqrt((q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) + q[0] * q[0]);
+    qn[0] = q[0] * in; qn[1] = -(q[1] * in); qn[2] = -(q[2] * in); qn[3] = -(q[3] * in);
+    in = 1.0 / sqrt((qn[1] * qn[1] + qn[2] * qn[2] + qn[3] * qn[3]) + qn[0] * qn[0]);
+    qn[0] *= in; qn[1] *= in; qn[2] *= in; qn[3] *= in;
+    qrot(qn, F, bv.force + ((size_t)b * nmol + i) * 3);
+    qrot(qn, Tq, bv.torque + ((size_t)b * nmol + i) * 3);
+  }
+  tm.sync();
+  (void)shv;
+}
+
+// interaction energy with the reference's convention (unrotated centres and
+// molecule-frame H, src/moldynamics.cpp:358-386, src/molecule.cpp:1850-1890)
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c)
+{
+  __shared__ double red[PBSAM_TEAM];
+  const Team tm{(int)threadIdx.x, (int)blockDim.x};
+  const BatchView &bv = c.bv;
+  const int b = blockIdx.x;
+  if (b >= bv.B) return;
+  Sys y;
+  y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = bv.S;
+  y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP);
+  y.red = red;
+  const Tab &T = c.T;
+  double pot = 0.0;
+  if (bv.status[b] == PBSAM_STATUS_OK) {
+    for (int i = 0; i < bv.nmol; i++)
+      for (int j = i + 1; j < bv.nmol; j++) {
+        double e = 0.0;
+        const double *pi = bv.pos + 3 * ((size_t)b * bv.nmol + i), *pj = bv.pos + 3 * ((size_t)b * bv.nmol + j);
+        for (int si = bv.mol_off[i]; si < bv.mol_off[i + 1]; si++) {
+          double *Lki = y.sc.E(9), *tL = y.sc.E(10);
+          tzero(tm, Lki, y.NP2);
+          tm.sync();
+          const double *ci = y.cen(si);
+          for (int sj = bv.mol_off[j]; sj < bv.mol_off[j + 1]; sj++) {
+            const double *cj = y.cen(sj);
+            const double P[3] = {(pi[0] + ci[0]) - (pj[0] + cj[0]), (pi[1] + ci[1]) - (pj[1] + cj[1]),
+                                 (pi[2] + ci[2]) - (pj[2] + cj[2])};
+            const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+            const int pi2j = compute_order(y.NP, rho, bv.tH[y.sc1(si)], y.rad(si));
+            const int pj2i = compute_order(y.NP, rho, bv.tH[y.sc1(sj)], y.rad(sj));
+            const int minp = pi2j < pj2i ? pi2j : pj2i;
+            PairXf X;
+            prep_pair(tm, T, y.sc, P, minp, 0, y.rad(sj), y.rad(si), false, X);
+            pair_apply(tm, T, y.sc, X, false, y.H(sj), tL);
+            add_vec_into(tm, Lki, tL, y.NP2);
+          }
+          e += inprod_ml(y.H(si), bv.hscale[y.sc1(si)], Lki, y.rad(si), y.NP);
+          tm.sync();
+        }
+        pot += e;
+      }
+  }
+  if (tm.rank == 0) bv.energy[b] = pot;
+}
+
+// state of every system reset to the self-polarized values (CSolExpCenter BD constructor,
+// src/expcenter.cpp:398-425, and initGradient, src/expcenter.cpp:559-569)
+__global__ void pbsam_init_kernel(Ctx c)
+{
+  const BatchView &bv = c.bv;
+  const int b = blockIdx.x;
+  const int NP2 = c.T.NP * c.T.NP;
+  for (int s = 0; s < bv.S; s++) {
+    const int ts = bv.sph_ts[s];
+    const size_t o = ((size_t)b * bv.S + s) * NP2;
+    for (int i = threadIdx.x; i < NP2; i += blockDim.x) {
+      bv.F[o + i] = c.tv.Fself[(size_t)ts * NP2 + i];
+      bv.H[o + i] = c.tv.Hself[(size_t)ts * NP2 + i];
+      bv.Hrot[o + i] = c.tv.Hself[(size_t)ts * NP2 + i];
+      bv.HselfRot[o + i] = 0.0;
+      bv.LS[o + i] = 0.0; bv.LFS[o + i] = 0.0; bv.LHS[o + i] = 0.0;
+    }
+    for (int i = threadIdx.x; i < 3 * NP2; i += blockDim.x) {
+      bv.gLHN[((size_t)b * bv.S + s) * 3 * NP2 + i] = 0.0;
+      bv.gH[((size_t)b * bv.S + s) * 3 * NP2 + i] = 0.0;
+    }
+    const int p0 = bv.pt_off[s], np = bv.pt_off[s + 1] - p0, tp0 = c.tv.spx_off[ts];
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+      bv.qF[(size_t)b * bv.SP + p0 + i] = c.tv.qFself[tp0 + i];
+      bv.qH[(size_t)b * bv.SP + p0 + i] = c.tv.qHself[tp0 + i];
+    }
+    for (int i = threadIdx.x; i < 3 * np; i += blockDim.x) {
+      bv.gFp[((size_t)b * bv.SP + p0) * 3 + i] = 0.0;
+      bv.gHp[((size_t)b * bv.SP + p0) * 3 + i] = 0.0;
+    }
+    if (threadIdx.x == 0) {
+      const size_t k = (size_t)b * bv.S + s;
+      bv.hscale[k] = c.tv.hself_scale[ts];
+      bv.tF[k] = c.tv.tFself[ts];
+      bv.tH[k] = c.tv.tHself[ts];
+      bv.maxgF[k] = 0.0; bv.maxgH[k] = 0.0; bv.dev[k] = 0.0;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ molecule-type setup
+// per type sphere: constants (initMyConstants, src/expcenter.cpp:469-505), self
+// surface charges (src/molecule.cpp:787-810), fixed-charge expansions and their
+// Dirichlet/Neumann terms (src/expcenter.cpp:513-552, 1041-1060)
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup1_kernel(Ctx c, double *scr, long long scr_stride)
+{
+  __shared__ double red[PBSAM_TEAM];
+  const Team tm{(int)threadIdx.x, (int)blockDim.x};
+  const Tab &T = c.T;
+  const TypeView &tv = c.tv;
+  const int ts = blockIdx.x;
+  const int NP = T.NP, NP2 = NP * NP;
+  Scr sc = make_scr(scr + (size_t)ts * scr_stride, NP);
+  int t = 0;
+  while (tv.type_off[t + 1] <= ts) t++;
+  const double rad = tv.rad[ts];
+  double *cst = tv.cst + (size_t)ts * CST_N * NP;
+  if (tm.rank == 0) {
+    double bK[34], bI[34];
+    const double val = T.kappa * rad, valsqr = val * val, exp_val = exp(-1.0 * val);
+    const double eps = c.prm.idiel / c.prm.sdiel;
+    bessel_k(T, bK, NP + 1, val);
+    bessel_i(bI, NP + 1, val);
+    for (int n = 0; n < NP; n++) {
+      const double DH = -exp_val * bK[n], DF = 1.0;
+      const double VH = exp_val * (n * bK[n] - (2 * n + 1) * bK[n + 1]), VF = -eps * n;
+      cst[CST_H1 * NP + n] = VH;
+      cst[CST_F1 * NP + n] = VF + (2 * n + 1);
+      cst[CST_LF1 * NP + n] = -rad * eps * n;
+      cst[CST_LH1 * NP + n] = rad * (n * bI[n] + valsqr * bI[n + 1] / double(2 * n + 3));
+      cst[CST_H2 * NP + n] = DH + (2 * n + 1) / bI[n];
+      cst[CST_F2 * NP + n] = DF;
+      cst[CST_LF2 * NP + n] = rad;
+      cst[CST_LH2 * NP + n] = -rad * bI[n];
+      cst[CST_INVH * NP + n] = bI[n] * (T.CONST3[n]);
+      cst[CST_CHGH * NP + n] = T.CONST2[n] / bI[n];
+    }
+  }
+  tm.sync();
+  const double *pts = tv.spx + 3 * (size_t)tv.spx_off[ts];
+  const int npt = tv.spx_off[ts + 1] - tv.spx_off[ts];
+  const double dA = 4.0 * PB_PI / double(tv.nspx[ts]);
+  double tot[1];
+  surface_q<1>(tm, T, pts, npt, dA, tv.Fself + (size_t)ts * NP2, T.CONST2, tv.qFself + tv.spx_off[ts], tot, red);
+  const double tF = tot[0];
+  surface_q<1>(tm, T, pts, npt, dA, tv.Hself + (size_t)ts * NP2, cst + CST_CHGH * NP, tv.qHself + tv.spx_off[ts], tot, red);
+  if (tm.rank == 0) { tv.tFself[ts] = tF; tv.tHself[ts] = tot[0]; }
+  // fixed charges split into inside (multipole) / outside (local) sets, scaled by 1/eps_in
+  const int q0 = tv.chg_off[t], nq = tv.chg_off[t + 1] - q0;
+  double *win = sc.misc, *wout = sc.misc + nq;   // misc holds 4096 + S*S doubles (nq checked on the host)
+  const double *cs = tv.cen + 3 * ts;
+  for (int k = tm.rank; k < nq; k += tm.size) {
+    const double *p = tv.chg_pos + 3 * (size_t)(q0 + k);
+    const double dx = p[0] - cs[0], dy = p[1] - cs[1], dz = p[2] - cs[2];
+    const double cq = tv.chg[q0 + k] / c.prm.idiel;
+    const bool in = (dx * dx + dy * dy + dz * dz) < rad * rad;
+    win[k] = in ? cq : 0.0;
+    wout[k] = in ? 0.0 : cq;
+  }
+  tm.sync();
+  double *Efix = sc.E(10), *Lfix = sc.E(11);
+  numeric_expand<1>(tm, T, sc, tv.chg_pos + 3 * (size_t)q0, nq, cs, win, false, false, NP, rad, Efix);
+  numeric_expand<1>(tm, T, sc, tv.chg_pos + 3 * (size_t)q0, nq, cs, wout, true, false, NP, rad, Lfix);
+  const double eps = c.prm.idiel / c.prm.sdiel;
+  for (int k = tm.rank; k < NP2; k += tm.size) {
+    int n = (int)sqrt((double)k);
+    while (n * n > k) n--;
+    while ((n + 1) * (n + 1) <= k) n++;
+    const double DE = 1.0, DL = rad, VE = eps * (n + 1), VL = -eps * n * rad;
+    tv.Dfix[(size_t)ts * NP2 + k] = DE * Efix[k] + DL * Lfix[k];
+    tv.Vfix[(size_t)ts * NP2 + k] = VE * Efix[k] + VL * Lfix[k];
+  }
+}
+
+// per type sphere: intra-molecular self local expansions (computeMolTypeValues,
+// src/molecule.cpp:544-696)
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup2_kernel(Ctx c, double *scr, long long scr_stride)
+{
+  const Team tm{(int)threadIdx.x, (int)blockDim.x};
+  const Tab &T = c.T;
+  const TypeView &tv = c.tv;
+  const int ts = blockIdx.x;
+  const int NP = T.NP, NP2 = NP * NP;
+  Scr sc = make_scr(scr + (size_t)ts * scr_stride, NP);
+  int t = 0;
+  while (tv.type_off[t + 1] <= ts) t++;
+  const int t0 = tv.type_off[t], ns = tv.type_off[t + 1] - t0, ki = ts - t0;
+  const double ri = tv.rad[ts];
+  double *LFf = tv.LFfar + (size_t)ts * NP2, *LHf = tv.LHfar + (size_t)ts * NP2;
+  double *LFi = tv.LFintra + (size_t)ts * NP2, *LHi = tv.LHintra + (size_t)ts * NP2;
+  double *a = sc.E(10), *bq = sc.E(11);
+  tzero(tm, LFf, NP2);
+  tzero(tm, LHf, NP2);
+  tm.sync();
+  const int nb = tv.near_off[ts], ne = tv.near_off[ts + 1];
+  const double *ci = tv.cen + 3 * ts;
+  // far field (every sphere of the type not on the near list), analytic at full order
+  for (int kj = 0; kj < ns; kj++) {
+    if (kj == ki) continue;
+    bool isnear = false;
+    for (int e = nb; e < ne; e++) if (tv.near[e] == kj) isnear = true;
+    if (isnear) continue;
+    const double *cj = tv.cen + 3 * (t0 + kj);
+    const double P[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+    PairXf X;
+    prep_pair(tm, T, sc, P, NP, NP, tv.rad[t0 + kj], ri, false, X);
+    pair_apply(tm, T, sc, X, true, tv.Fself + (size_t)(t0 + kj) * NP2, a);
+    pair_apply(tm, T, sc, X, false, tv.Hself + (size_t)(t0 + kj) * NP2, bq);
+    for (int i = tm.rank; i < NP2; i += tm.size) { LFf[i] += a[i]; LHf[i] += bq[i]; }
+    tm.sync();
+  }
+  tcopy(tm, LFi, LFf, NP2);
+  tcopy(tm, LHi, LHf, NP2);
+  tm.sync();
+  for (int e = nb; e < ne; e++) {
+    const int kj = tv.near[e];
+    const int tj = t0 + kj;
+    const double *cj = tv.cen + 3 * tj;
+    const double P[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+    const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+    const double rj = tv.rad[tj];
+    const double sep = rho - ri - rj;
+    if (sep > 0 && !(sep < c.prm.min_sep_numeric)) {
+      PairXf X;
+      prep_pair(tm, T, sc, P, NP, NP, rj, ri, false, X);
+      pair_apply(tm, T, sc, X, true, tv.Fself + (size_t)tj * NP2, a);
+      pair_apply(tm, T, sc, X, false, tv.Hself + (size_t)tj * NP2, bq);
+    } else {
+      const int pF = compute_order(NP, rho, tv.tFself[tj], rj), pH = compute_order(NP, rho, tv.tHself[tj], rj);
+      const double *pts = tv.spx + 3 * (size_t)tv.spx_off[tj];
+      const int npt = tv.spx_off[tj + 1] - tv.spx_off[tj];
+      numeric_expand<1>(tm, T, sc, pts, npt, P, tv.qFself + tv.spx_off[tj], true, false, pF, ri, a);
+      numeric_expand<1>(tm, T, sc, pts, npt, P, tv.qHself + tv.spx_off[tj], true, true, pH, ri, bq);
+    }
+    for (int i = tm.rank; i < NP2; i += tm.size) { LFi[i] += a[i]; LHi[i] += bq[i]; }
+    tm.sync();
+  }
+}
+
+}  // namespace pbsam

@@ -1,0 +1,98 @@
+// Device-side views of the molecule-type tables and of a batch of independent
+// systems.  Shared by the kernels (pbsam_kernels.cu) and the C-ABI host code
+// (pbsam_api.cu).
+#pragma once
+#include "pbsam_device.cuh"
+
+namespace pbsam {
+
+// Solver parameters: the reference's compile-time tolerances and cutoffs made
+// runtime values (src/molecule.cpp:6-13, src/expcenter.cpp:16-22,
+// src/BDnam.cpp:82,138-139, src/molecule.h:22).
+struct SolveParams {
+  double max_polar_dev;    // outer stop: avg dev > max_polar_dev^2 continues
+  double solve_tol;        // inner F/H fixed-point stop
+  int solve_max_ct;        // inner iteration cap
+  int max_pol_rounds;      // outer sweep cap
+  double inter_cut;        // inter-molecular polarization cutoff (surface gap)
+  double interact_cut;     // inter-molecular interaction cutoff
+  double min_sep_numeric;  // intra pairs closer than this re-expand numerically
+  double idiel, sdiel;
+};
+
+// Per-sphere constant block layout inside TypeView::cst (NP doubles each).
+enum { CST_H1 = 0, CST_F1, CST_H2, CST_F2, CST_LH1, CST_LF1, CST_LH2, CST_LF2, CST_INVH, CST_CHGH, CST_N };
+
+// Molecule types, concatenated over all types ("type sphere" index ts).
+struct TypeView {
+  int ntypes, TS;
+  const int *type_off;     // [ntypes+1] first type sphere of each type
+  const double *maxR;      // [ntypes]
+  const double *cen;       // [TS][3] sphere centre in the molecule frame
+  const double *rad;       // [TS]
+  const int *spx_off;      // [TS+1] exposed surface points (CSR)
+  const double *spx;       // [TP][3] relative to the sphere centre
+  const int *nspx;         // [TS] number of generated points (quadrature weight 4pi/nspx)
+  const double *Fself, *Hself;       // [TS][NP2]
+  const double *hself_scale;         // [TS]  scale value read with Hself
+  double *qFself, *qHself;           // [TP]
+  double *tFself, *tHself;           // [TS]
+  double *LFintra, *LHintra, *LFfar, *LHfar;   // [TS][NP2]
+  const int *near_off, *near;        // CSR: intra near list (type sphere indices within the type)
+  double *Dfix, *Vfix;               // [TS][NP2]
+  double *cst;                       // [TS][CST_N][NP]
+  const double *imat;                // [TS][NP2*NP2] column-major
+  // charges of each type (for the fixed-charge expansions)
+  const int *chg_off;      // [ntypes+1]
+  const double *chg_pos;   // [TQ][3] relative to the molecule centre
+  const double *chg;       // [TQ]
+};
+
+// Batch of B independent systems with the same list of molecules.
+struct BatchView {
+  int B, nmol, S, SP;        // systems, molecules, spheres and points per system
+  const int *mol_type;       // [nmol]
+  const int *mol_off;        // [nmol+1]
+  const int *sph_ts;         // [S]
+  const int *sph_mol;        // [S]
+  const int *pt_off;         // [S+1]
+  const double *pos, *quat;  // [B][nmol][3], [B][nmol][4]
+  double *F, *H, *Hrot, *HselfRot, *LS, *LFS, *LHS;   // [B][S][NP2]
+  double *hscale, *tF, *tH, *maxgF, *maxgH, *dev;     // [B][S]
+  double *qF, *qH;           // [B][SP]
+  double *gFp, *gHp;         // [B][SP][3]
+  double *gLHN, *gH;         // [B][S][3][NP2]
+  double *cenRot;            // [B][S][3]
+  int *ipol, *ipol_n, *iact, *iact_n;        // [B][S][S], [B][S]
+  int *interMol, *interMol_n;                // [B][nmol][S], [B][nmol]
+  int *intraPol, *intraPol_n, *intraAct, *intraAct_n;
+  int *interX;               // [B][nmol]
+  double *gFw, *gHw, *gHrotw, *tGw;          // [B][S][3][NP2] gradient work set
+  int *gkey;                 // [B][S]
+  double *dgrad;             // [B][S]
+  double2 *molR;             // [B][nmol][rot entries at NP]
+  double *molRS;             // [B][nmol][8] rotation state scalars
+  double *sep;               // [B][S][S] sphere-sphere surface gaps
+  double *scr;               // [B][scr_stride]
+  long long scr_stride;
+  double *force, *torque, *energy;  // [B][nmol][3], [B][nmol][3], [B]
+  int *status;               // [B]
+  int *stats;                // [B][8]: sweeps, inner iterations, solves, grad solves, ...
+};
+
+enum {
+  PBSAM_STATUS_OK = 0,
+  PBSAM_STATUS_OVERLAP = 1,
+  PBSAM_STATUS_NOT_CONVERGED = 2,
+  PBSAM_STATUS_NAN = 3,
+};
+
+struct Ctx {
+  Tab T;
+  TypeView tv;
+  BatchView bv;
+  SolveParams prm;
+  int do_energy;
+};
+
+}  // namespace pbsam

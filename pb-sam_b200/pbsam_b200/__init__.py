@@ -1,0 +1,206 @@
+"""Python host mirror of the B200 PB-SAM drop-in (ctypes over include/pbsam_b200.h).
+
+The reference exposes this path as C++ classes; the names here follow them:
+
+* ``CSystem`` -- ``CSystem::initConstants(kappa, sdiel, temp)`` plus the
+  compile-time tolerances of the reference (src/system.h:19-20), i.e. one
+  solver context on one GPU.
+* ``CSystem.load_moltype`` -- the per-species set-up of ``CBDnam::CBDnam``
+  (src/BDnam.cpp:59-119): PQR, ``imat.sp<k>.out.bin``, ``<name>.<k>.{F,H}.exp``.
+* ``Molecules`` -- the ``vector<CMolecule*>`` of a run, here for ``n_systems``
+  independent copies; ``setPos``/``setOrient`` (src/molecule.h:325-326),
+  ``computeForces`` (src/molecule.h:179) and ``computeTotalIntEnergy``
+  (src/molecule.h:180).
+
+The CUDA library ``lib/libpbsam_b200.so`` must be built (``__graft_entry__.build``);
+there is no CPU fallback: every call runs the sm_100a kernels.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "lib", "libpbsam_b200.so")
+
+PBSAM_SYS_OK = 0
+PBSAM_SYS_OVERLAP = 1
+
+
+class pbsam_params(ctypes.Structure):
+    _fields_ = [("poles", ctypes.c_int), ("salt", ctypes.c_double), ("idiel", ctypes.c_double),
+                ("sdiel", ctypes.c_double), ("temperature", ctypes.c_double),
+                ("max_polar_dev", ctypes.c_double), ("solve_tol", ctypes.c_double),
+                ("solve_max_ct", ctypes.c_int), ("max_pol_rounds", ctypes.c_int),
+                ("inter_cutoff", ctypes.c_double), ("interact_cutoff", ctypes.c_double),
+                ("intra_cutoff", ctypes.c_double), ("min_sep_numeric", ctypes.c_double),
+                ("num_points_x", ctypes.c_int)]
+
+
+# every entry point declared in include/pbsam_b200.h, with ctypes signatures
+_P = ctypes.c_void_p
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+SIGNATURES = {
+    "pbsam_params_default": (None, [ctypes.POINTER(pbsam_params)]),
+    "pbsam_context_create": (ctypes.c_int, [ctypes.POINTER(pbsam_params), ctypes.c_int, ctypes.POINTER(_P)]),
+    "pbsam_context_destroy": (ctypes.c_int, [_P]),
+    "pbsam_context_kappa": (ctypes.c_int, [_P, _DP]),
+    "pbsam_moltype_load": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _IP]),
+    "pbsam_moltype_create": (ctypes.c_int, [_P, ctypes.c_int, _DP, _DP, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP, _IP]),
+    "pbsam_moltype_info": (ctypes.c_int, [_P, ctypes.c_int, _IP, _IP]),
+    "pbsam_system_create": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _IP, ctypes.POINTER(_P)]),
+    "pbsam_system_destroy": (ctypes.c_int, [_P]),
+    "pbsam_system_reset": (ctypes.c_int, [_P]),
+    "pbsam_system_set_poses": (ctypes.c_int, [_P, _P, _P, ctypes.c_int]),
+    "pbsam_system_compute_forces": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int]),
+    "pbsam_system_compute_energy": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "pbsam_system_stats": (ctypes.c_int, [_P, _IP]),
+    "pbsam_system_set_stream": (ctypes.c_int, [_P, _P]),
+    "pbsam_system_last_kernel_ms": (ctypes.c_int, [_P, _DP]),
+    "pbsam_last_error": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("CUDA library not built: %s (run __graft_entry__.build())" % LIB_PATH)
+        _lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(_lib, name)
+            f.restype = res
+            f.argtypes = args
+    return _lib
+
+
+class PbsamError(RuntimeError):
+    pass
+
+
+def _check(rc):
+    if rc != 0:
+        msg = lib().pbsam_last_error()
+        raise PbsamError("pbsam error %d: %s" % (rc, msg.decode() if msg else ""))
+
+
+def default_params(**kw):
+    p = pbsam_params()
+    lib().pbsam_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_DP)
+
+
+class CSystem:
+    """Solver context on one GPU (CSystem::initConstants + solver constants)."""
+
+    def __init__(self, poles=10, salt=0.05, device=0, **kw):
+        self.params = default_params(poles=poles, salt=salt, **kw)
+        h = _P()
+        _check(lib().pbsam_context_create(ctypes.byref(self.params), device, ctypes.byref(h)))
+        self.handle = h
+        self.types = []
+
+    @property
+    def kappa(self):
+        k = ctypes.c_double()
+        _check(lib().pbsam_context_kappa(self.handle, ctypes.byref(k)))
+        return k.value
+
+    def load_moltype(self, pqr, imat_dir, exp_dir, exp_name):
+        t = ctypes.c_int()
+        _check(lib().pbsam_moltype_load(self.handle, pqr.encode(), imat_dir.encode(), exp_dir.encode(),
+                                        exp_name.encode(), ctypes.byref(t)))
+        self.types.append(t.value)
+        return t.value
+
+    def create_moltype(self, centres, radii, chg_pos, chg, imats, fself, hself, hself_scale):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                (centres, radii, chg_pos, chg, imats, fself, hself, hself_scale)]
+        t = ctypes.c_int()
+        _check(lib().pbsam_moltype_create(self.handle, len(arrs[1]), _dptr(arrs[0]), _dptr(arrs[1]), len(arrs[3]),
+                                          _dptr(arrs[2]), _dptr(arrs[3]), _dptr(arrs[4]), _dptr(arrs[5]),
+                                          _dptr(arrs[6]), _dptr(arrs[7]), ctypes.byref(t)))
+        self.types.append(t.value)
+        return t.value
+
+    def moltype_info(self, t):
+        ns, npts = ctypes.c_int(), ctypes.c_int()
+        _check(lib().pbsam_moltype_info(self.handle, t, ctypes.byref(ns), ctypes.byref(npts)))
+        return ns.value, npts.value
+
+    def molecules(self, mol_types, n_systems=1):
+        return Molecules(self, mol_types, n_systems)
+
+    def close(self):
+        if self.handle:
+            _check(lib().pbsam_context_destroy(self.handle))
+            self.handle = None
+
+
+class Molecules:
+    """n_systems independent copies of a list of molecules (vector<CMolecule*>)."""
+
+    def __init__(self, ctx, mol_types, n_systems=1):
+        self.ctx = ctx
+        self.n_mol = len(mol_types)
+        self.n_systems = n_systems
+        mt = (ctypes.c_int * self.n_mol)(*mol_types)
+        h = _P()
+        _check(lib().pbsam_system_create(ctx.handle, n_systems, self.n_mol, mt, ctypes.byref(h)))
+        self.handle = h
+
+    def reset(self):
+        _check(lib().pbsam_system_reset(self.handle))
+
+    def set_poses(self, pos, quat):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(self.n_systems, self.n_mol, 3)
+        quat = np.ascontiguousarray(quat, dtype=np.float64).reshape(self.n_systems, self.n_mol, 4)
+        _check(lib().pbsam_system_set_poses(self.handle, pos.ctypes.data, quat.ctypes.data, 0))
+
+    def set_poses_device(self, pos_ptr, quat_ptr):
+        _check(lib().pbsam_system_set_poses(self.handle, pos_ptr, quat_ptr, 1))
+
+    def compute_forces(self):
+        """Returns (force[n_systems, n_mol, 3], torque[...], status[n_systems])."""
+        f = np.zeros((self.n_systems, self.n_mol, 3))
+        t = np.zeros((self.n_systems, self.n_mol, 3))
+        st = np.zeros(self.n_systems, dtype=np.int32)
+        _check(lib().pbsam_system_compute_forces(self.handle, f.ctypes.data, t.ctypes.data, st.ctypes.data, 0))
+        return f, t, st
+
+    def compute_forces_device(self, force_ptr, torque_ptr, status_ptr):
+        _check(lib().pbsam_system_compute_forces(self.handle, force_ptr, torque_ptr, status_ptr, 1))
+
+    def compute_energy(self):
+        e = np.zeros(self.n_systems)
+        _check(lib().pbsam_system_compute_energy(self.handle, e.ctypes.data, 0))
+        return e
+
+    def stats(self):
+        s = np.zeros((self.n_systems, 8), dtype=np.int32)
+        _check(lib().pbsam_system_stats(self.handle, s.ctypes.data_as(_IP)))
+        return s
+
+    def set_stream(self, stream_handle):
+        _check(lib().pbsam_system_set_stream(self.handle, ctypes.c_void_p(stream_handle)))
+
+    def last_kernel_ms(self):
+        m = ctypes.c_double()
+        _check(lib().pbsam_system_last_kernel_ms(self.handle, ctypes.byref(m)))
+        return m.value
+
+    def close(self):
+        if self.handle:
+            _check(lib().pbsam_system_destroy(self.handle))
+            self.handle = None
