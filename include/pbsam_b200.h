@@ -33,6 +33,7 @@ extern "C" {
 #define PBSAM_SYS_OK 0
 #define PBSAM_SYS_OVERLAP 1   /* two spheres of different molecules overlap
                                  (computeForces returns false, src/molecule.cpp:1090-1097) */
+#define PBSAM_SYS_WAIT_EXPIRED 4 /* a bounded device wait expired; results of the system are void */
 
 typedef struct pbsam_params {
   int poles;              /* pole order p (the reference's N_POLES, src/expansion.h:5-9) */
@@ -114,8 +115,30 @@ int pbsam_system_stats(const pbsam_system *sys, int *stats);
  * calls above synchronise it before returning host results. */
 int pbsam_system_set_stream(pbsam_system *sys, void *stream);
 
+/* Device time per phase of the last force evaluation (or self-polarization), 8
+ * doubles per system in ms: [0] F/H solves, [1] surface charges, [2] numeric
+ * near-field re-expansions, [3] analytic intra re-expansions, [4] inter-molecular
+ * LS re-expansions, [5] gradient re-expansions of H (DTA), [6] whole evaluation. */
+int pbsam_system_phase_ms(const pbsam_system *sys, double *ms);
+
 /* Device time in milliseconds of the last force-kernel launch (CUDA events). */
 int pbsam_system_last_kernel_ms(const pbsam_system *sys, double *ms);
+
+/* Molecule-type preparation (the reference's `pbsam mat` and `pbsam spol`).
+ *
+ * Surface-integral matrices of a molecule's spheres: replaces the CMolecule IMat
+ * constructor with build_IMatE (src/molecule.cpp:279-346, src/expcenter.cpp:910-1033);
+ * centres are absolute, n_points is NUM_POINTS_I (250000 in the reference);
+ * imats receives n_sph * p^4 doubles, the content of imat.sp<k>.out.bin. */
+int pbsam_imat_build(pbsam_context *ctx, int n_sph, const double *centres, const double *radii, int n_points,
+                     double *imats);
+/* Self-polarization of one molecule type: replaces CMolecule::polarize_self
+ * (src/molecule.cpp:1898-1979) as run by `pbsam spol` (src/selfp_makemat.cpp:37-118).
+ * The type's own F/H inputs are ignored.  Outputs are rounded as the reference
+ * writes its .exp files: fself/hself[n_sph*p^2], hself_scale[n_sph]; rounds
+ * receives the number of sweeps. */
+int pbsam_selfpol(pbsam_context *ctx, int type_id, int max_rounds, double *fself, double *hself,
+                  double *hself_scale, int *rounds);
 
 /* Text of the last error on the calling thread. */
 const char *pbsam_last_error(void);

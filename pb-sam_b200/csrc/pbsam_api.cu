@@ -12,6 +12,7 @@
 
 #include "pbsam_b200.h"
 #include "pbsam_kernels.cu"
+#include "pbsam_setup.cu"
 
 using namespace pbsam;
 
@@ -125,6 +126,7 @@ struct HostType {
   std::vector<std::vector<int> > near;
   std::vector<double> fself, hself, hscale, imat;
   std::vector<double> chg_pos, chg;   // relative to the molecule centre
+  std::vector<int> chg_lab;           // sphere each charge is assigned to
 };
 
 struct pbsam_context {
@@ -308,7 +310,8 @@ static int add_type(pbsam_context *c, HostType &&t0, const std::vector<double> &
   // molecule centre = mean sphere centre (src/BDnam.cpp:68-70)
   double rc[3] = {0, 0, 0};
   for (int k = 0; k < ns; k++) for (int d = 0; d < 3; d++) rc[d] += cen_abs[3 * k + d];
-  for (int d = 0; d < 3; d++) rc[d] /= ns;
+  const double inv = 1.0 / ns;
+  for (int d = 0; d < 3; d++) rc[d] *= inv;
   t.cen.resize(3 * ns);
   t.maxR = 0;
   for (int k = 0; k < ns; k++) {
@@ -318,6 +321,16 @@ static int add_type(pbsam_context *c, HostType &&t0, const std::vector<double> &
   }
   for (size_t q = 0; q < t.chg.size(); q++) for (int d = 0; d < 3; d++) t.chg_pos[3 * q + d] -= rc[d];
   make_surface_points(c->prm, t, cen_abs);
+  // assign each charge to the first sphere that contains it (src/molecule.cpp:1001-1023)
+  t.chg_lab.assign(t.chg.size(), -1);
+  for (size_t q = 0; q < t.chg.size(); q++) {
+    for (int k = 0; k < ns; k++) {
+      const double dx = t.chg_pos[3 * q] - t.cen[3 * k], dy = t.chg_pos[3 * q + 1] - t.cen[3 * k + 1],
+                   dz = t.chg_pos[3 * q + 2] - t.cen[3 * k + 2];
+      if (sqrt(dx * dx + dy * dy + dz * dz) + 0.0 <= t.rad[k]) { t.chg_lab[q] = k; break; }
+    }
+    if (t.chg_lab[q] < 0) return fail(PBSAM_E_BADARG, "a charge lies outside every sphere");
+  }
   // intra near lists (src/molecule.cpp:500-535)
   t.near.assign(ns, std::vector<int>());
   for (int kj = 0; kj < ns; kj++)
@@ -328,6 +341,13 @@ static int add_type(pbsam_context *c, HostType &&t0, const std::vector<double> &
     }
   c->types.push_back(std::move(t));
   return (int)c->types.size() - 1;
+}
+static int add_type_checked(pbsam_context *c, HostType &&t, const std::vector<double> &cen_abs, int *type_id)
+{
+  const int r = add_type(c, std::move(t), cen_abs);
+  if (r < 0) return r;
+  *type_id = r;
+  return PBSAM_OK;
 }
 
 extern "C" int pbsam_moltype_load(pbsam_context *c, const char *pqr, const char *imat_dir, const char *exp_dir,
@@ -356,8 +376,7 @@ extern "C" int pbsam_moltype_load(pbsam_context *c, const char *pqr, const char 
     snprintf(fn, sizeof fn, "%s/%s.%d.H.exp", exp_dir, exp_name, k);
     if (!read_exp(fn, NP, t.hself.data() + (size_t)k * NP2, t.hscale[k])) return fail(PBSAM_E_IO, std::string("cannot read ") + fn);
   }
-  *type_id = add_type(c, std::move(t), cen_abs);
-  return PBSAM_OK;
+  return add_type_checked(c, std::move(t), cen_abs, type_id);
 }
 
 extern "C" int pbsam_moltype_create(pbsam_context *c, int n_sph, const double *centres, const double *radii, int n_chg,
@@ -379,8 +398,7 @@ extern "C" int pbsam_moltype_create(pbsam_context *c, int n_sph, const double *c
   t.hself.assign(hself, hself + (size_t)n_sph * NP2);
   t.hscale.assign(hself_scale, hself_scale + n_sph);
   std::vector<double> cen_abs(centres, centres + 3 * n_sph);
-  *type_id = add_type(c, std::move(t), cen_abs);
-  return PBSAM_OK;
+  return add_type_checked(c, std::move(t), cen_abs, type_id);
 }
 
 extern "C" int pbsam_moltype_info(const pbsam_context *c, int id, int *n_sph, int *n_points)
@@ -414,6 +432,19 @@ static int dput(std::vector<void *> &bufs, const T **p, const std::vector<T> &h)
 }
 #define TRY(x) do { int r_ = (x); if (r_) return r_; } while (0)
 
+// opt every team kernel into the dynamic shared memory it needs
+static int set_smem_attrs(int NP)
+{
+  const int smem = (int)team_smem_bytes(NP);
+  CK(cudaFuncSetAttribute(pbsam_forces_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(pbsam_energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(pbsam_setup1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(pbsam_setup2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(pbsam_setup3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(pbsam_selfpol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  return PBSAM_OK;
+}
+
 // upload all molecule types and run the per-type setup kernels
 static int finalize_types(pbsam_context *c)
 {
@@ -422,7 +453,7 @@ static int finalize_types(pbsam_context *c)
   CK(cudaSetDevice(c->device));
   const int NP = c->prm.poles;
   const long NP2 = (long)NP * NP;
-  std::vector<int> type_off(1, 0), spx_off(1, 0), nspx, near_off(1, 0), near, chg_off(1, 0);
+  std::vector<int> type_off(1, 0), spx_off(1, 0), nspx, near_off(1, 0), near, chg_off(1, 0), chg_lab;
   std::vector<double> maxR, cen, rad, spx, Fs, Hs, hsc, imat, chg_pos, chg;
   int maxq = 0, maxns = 0;
   for (auto &t : c->types) {
@@ -440,10 +471,20 @@ static int finalize_types(pbsam_context *c)
     Fs.insert(Fs.end(), t.fself.begin(), t.fself.end());
     Hs.insert(Hs.end(), t.hself.begin(), t.hself.end());
     hsc.insert(hsc.end(), t.hscale.begin(), t.hscale.end());
-    imat.insert(imat.end(), t.imat.begin(), t.imat.end());
+    {
+      const size_t base = imat.size(), stride = imat_stride((int)NP2);
+      imat.resize(base + (size_t)t.ns * stride, 0.0);
+      for (int k = 0; k < t.ns; k++) {
+        const double *src = t.imat.data() + (size_t)k * NP2 * NP2;
+        double *dst = imat.data() + base + (size_t)k * stride;
+        for (long r = 0; r < NP2; r++)
+          for (long cc = 0; cc < NP2; cc++) dst[r * NP2 + cc] = src[cc * NP2 + r];
+      }
+    }
     chg_off.push_back(chg_off.back() + (int)t.chg.size());
     chg_pos.insert(chg_pos.end(), t.chg_pos.begin(), t.chg_pos.end());
     chg.insert(chg.end(), t.chg.begin(), t.chg.end());
+    chg_lab.insert(chg_lab.end(), t.chg_lab.begin(), t.chg_lab.end());
     if ((int)t.chg.size() > maxq) maxq = (int)t.chg.size();
     if (t.ns > maxns) maxns = t.ns;
   }
@@ -458,6 +499,13 @@ static int finalize_types(pbsam_context *c)
   TRY(dput(B, &tv.hself_scale, hsc)); TRY(dput(B, &tv.near_off, near_off)); TRY(dput(B, &tv.near, near));
   TRY(dput(B, &tv.imat, imat)); TRY(dput(B, &tv.chg_off, chg_off)); TRY(dput(B, &tv.chg_pos, chg_pos));
   TRY(dput(B, &tv.chg, chg));
+  TRY(dput(B, &tv.chg_lab, chg_lab));
+  TRY(dalloc(B, &tv.Eass, TS * NP2));
+  const int TE = near_off.back();
+  TRY(dalloc(B, &tv.pR, (size_t)TE * rot_off(NP)));
+  TRY(dalloc(B, &tv.pTH, (size_t)TE * tr_off(NP)));
+  TRY(dalloc(B, &tv.pTF, (size_t)TE * tr_off(NP)));
+  TRY(dalloc(B, &tv.pS, (size_t)TE * 16));
   TRY(dalloc(B, &tv.qFself, TP)); TRY(dalloc(B, &tv.qHself, TP));
   TRY(dalloc(B, &tv.tFself, TS)); TRY(dalloc(B, &tv.tHself, TS));
   TRY(dalloc(B, &tv.LFintra, TS * NP2)); TRY(dalloc(B, &tv.LHintra, TS * NP2));
@@ -477,10 +525,24 @@ static int finalize_types(pbsam_context *c)
   cx.tv = tv;
   cx.prm.idiel = c->prm.idiel; cx.prm.sdiel = c->prm.sdiel;
   cx.prm.min_sep_numeric = c->prm.min_sep_numeric;
-  pbsam_setup1_kernel<<<TS, PBSAM_TEAM>>>(cx, scr, stride);
+  TRY(set_smem_attrs(NP));
+  const size_t smem = team_smem_bytes(NP);
+  pbsam_setup1_kernel<<<TS, PBSAM_TEAM, smem>>>(cx, scr, stride);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
-  if (e == cudaSuccess) { pbsam_setup2_kernel<<<TS, PBSAM_TEAM>>>(cx, scr, stride); e = cudaGetLastError(); }
+  // intra near pair tables, in chunks of CH entries (slim per-block scratch)
+  const int CH = 512;
+  const long long s3 = 4LL * NP * NP + tr_off(2 * NP - 1) + 2 * NP + 8;
+  double *scr3 = nullptr;
+  if (e == cudaSuccess && TE > 0) e = cudaMalloc(&scr3, (size_t)s3 * CH * sizeof(double));
+  for (int e0 = 0; e == cudaSuccess && e0 < TE; e0 += CH) {
+    const int ne = (TE - e0 < CH) ? TE - e0 : CH;
+    pbsam_setup3_kernel<<<ne, PBSAM_TEAM, smem>>>(cx, e0, ne, scr3, s3);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (scr3) cudaFree(scr3);
+  if (e == cudaSuccess) { pbsam_setup2_kernel<<<TS, PBSAM_TEAM, smem>>>(cx, scr, stride); e = cudaGetLastError(); }
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   cudaFree(scr);
   if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("setup kernels: ") + cudaGetErrorString(e));
@@ -549,6 +611,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   chk(dalloc(Bf, &bv.scr, (size_t)B * bv.scr_stride));
   chk(dalloc(Bf, &bv.force, B * n_mol * 3)); chk(dalloc(Bf, &bv.torque, B * n_mol * 3));
   chk(dalloc(Bf, &bv.energy, B)); chk(dalloc(Bf, &bv.status, B)); chk(dalloc(Bf, &bv.stats, B * 8));
+  chk(dalloc(Bf, &bv.tphase, B * 8));
   if (r) {
     for (void *p : Bf) cudaFree(p);
     delete s;
@@ -614,7 +677,7 @@ extern "C" int pbsam_system_compute_forces(pbsam_system *s, double *force, doubl
   if (!s) return fail(PBSAM_E_BADARG, "null system");
   CK(cudaSetDevice(s->ctx->device));
   CK(cudaEventRecord(s->ev0, s->stream));
-  pbsam_forces_kernel<<<s->B, PBSAM_TEAM, 0, s->stream>>>(s->c);
+  pbsam_forces_kernel<<<s->B, PBSAM_TEAM, team_smem_bytes(s->ctx->prm.poles), s->stream>>>(s->c);
   CK(cudaGetLastError());
   CK(cudaEventRecord(s->ev1, s->stream));
   const size_t n = (size_t)s->B * s->nmol * 3;
@@ -633,7 +696,7 @@ extern "C" int pbsam_system_compute_energy(pbsam_system *s, double *energy, int 
 {
   if (!s || !energy) return fail(PBSAM_E_BADARG, "null argument");
   CK(cudaSetDevice(s->ctx->device));
-  pbsam_energy_kernel<<<s->B, PBSAM_TEAM, 0, s->stream>>>(s->c);
+  pbsam_energy_kernel<<<s->B, PBSAM_TEAM, team_smem_bytes(s->ctx->prm.poles), s->stream>>>(s->c);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(energy, s->c.bv.energy, s->B * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s->stream));
   if (!on_device) CK(cudaStreamSynchronize(s->stream));
@@ -652,5 +715,149 @@ extern "C" int pbsam_system_last_kernel_ms(const pbsam_system *s, double *ms)
 {
   if (!s || !ms) return fail(PBSAM_E_BADARG, "null argument");
   *ms = s->last_ms;
+  return PBSAM_OK;
+}
+
+// ------------------------------------------------------------------ IMat builder
+// Surface-integral matrices of a molecule's spheres (pbsam mat: CMolecule IMat
+// constructor, src/molecule.cpp:279-346, getSpherePoints, src/molecule.cpp:901-939,
+// build_IMatE, src/expcenter.cpp:910-1033).  centres are absolute; imats receives
+// n_sph * p^4 doubles (column-major p^2 x p^2 per sphere).
+extern "C" int pbsam_imat_build(pbsam_context *c, int n_sph, const double *centres, const double *radii, int n_points,
+                                double *imats)
+{
+  if (!c || n_sph <= 0 || !centres || !radii || n_points < 3 || !imats) return fail(PBSAM_E_BADARG, "bad argument");
+  CK(cudaSetDevice(c->device));
+  const int P = c->prm.poles, N = P * P;
+  // molecule-centred coordinates as the reference prepares them
+  double rc[3] = {0, 0, 0};
+  for (int k = 0; k < n_sph; k++) for (int d = 0; d < 3; d++) rc[d] += centres[3 * k + d];
+  const double inv = 1.0 / n_sph;
+  for (int d = 0; d < 3; d++) rc[d] *= inv;
+  std::vector<double> cr(3 * n_sph);
+  for (int k = 0; k < n_sph; k++) for (int d = 0; d < 3; d++) cr[3 * k + d] = centres[3 * k + d] - rc[d];
+  // unit-sphere spiral shared by every sphere (src/molecule.cpp:2272-2294)
+  std::vector<double> qx(n_points), qy(n_points), qz(n_points);
+  {
+    const int Np = n_points;
+    double phprev = 0;
+    for (int i = 1; i <= Np; i++) {
+      const double h = -1.0 + 2.0 * (i - 1.0) / (Np - 1.0);
+      const double th = acos(h);
+      double ph = (i == 1 || i == Np) ? 0 : (phprev + 3.6 / sqrt(Np * (1.0 - h * h)));
+      while (ph > 2 * M_PI) ph -= 2 * M_PI;
+      while (ph < -2 * M_PI) ph += 2 * M_PI;
+      phprev = ph;
+      qx[i - 1] = 1 * sin(th) * cos(ph); qy[i - 1] = 1 * sin(th) * sin(ph); qz[i - 1] = 1 * cos(th);
+    }
+  }
+  const int KC = 16384;
+  double *dY = nullptr, *dG = nullptr, *dGs = nullptr, *dIM = nullptr, *dP = nullptr;
+  std::vector<void *> tmp;
+  auto cleanup = [&]() { for (void *p : tmp) cudaFree(p); };
+  if (cudaMalloc(&dY, (size_t)KC * N * sizeof(double)) != cudaSuccess) { cleanup(); return fail(PBSAM_E_NOMEM, "imat Y"); }
+  tmp.push_back(dY);
+  if (cudaMalloc(&dG, (size_t)N * N * sizeof(double)) != cudaSuccess) { cleanup(); return fail(PBSAM_E_NOMEM, "imat G"); }
+  tmp.push_back(dG);
+  if (cudaMalloc(&dIM, (size_t)N * N * sizeof(double)) != cudaSuccess) { cleanup(); return fail(PBSAM_E_NOMEM, "imat"); }
+  tmp.push_back(dIM);
+  if (cudaMalloc(&dGs, (size_t)P * P * sizeof(double)) != cudaSuccess) { cleanup(); return fail(PBSAM_E_NOMEM, "imat Gs"); }
+  tmp.push_back(dGs);
+  if (cudaMalloc(&dP, (size_t)n_points * 3 * sizeof(double)) != cudaSuccess) { cleanup(); return fail(PBSAM_E_NOMEM, "imat pts"); }
+  tmp.push_back(dP);
+  const double dA = 4 * M_PI / (double)(n_points - 1);
+  for (int k = 0; k < n_sph; k++) {
+    std::vector<int> neigh;
+    for (int j = 0; j < n_sph; j++) {
+      if (j == k) continue;
+      const double sr = radii[k] + radii[j];
+      const double dx = centres[3 * k] - centres[3 * j], dy = centres[3 * k + 1] - centres[3 * j + 1],
+                   dz = centres[3 * k + 2] - centres[3 * j + 2];
+      if (dx * dx + dy * dy + dz * dz < sr * sr) neigh.push_back(j);
+    }
+    std::vector<double> E, Bp;
+    for (int i = 0; i < n_points; i++) {
+      const double px = radii[k] * qx[i], py = radii[k] * qy[i], pz = radii[k] * qz[i];
+      bool buried = false;
+      for (int j : neigh) {
+        const double dx = (px + cr[3 * k]) - cr[3 * j], dy = (py + cr[3 * k + 1]) - cr[3 * j + 1],
+                     dz = (pz + cr[3 * k + 2]) - cr[3 * j + 2];
+        if (dx * dx + dy * dy + dz * dz < radii[j] * radii[j] * 1.0) { buried = true; break; }
+      }
+      std::vector<double> &dst = buried ? Bp : E;
+      dst.push_back(px); dst.push_back(py); dst.push_back(pz);
+    }
+    const int npe = (int)E.size() / 3, npb = (int)Bp.size() / 3;
+    const int buried = (npe <= npb) ? 0 : 1;
+    const std::vector<double> &pts = buried ? Bp : E;
+    const int K = (int)pts.size() / 3;
+    CK(cudaMemset(dG, 0, (size_t)N * N * sizeof(double)));
+    CK(cudaMemset(dGs, 0, (size_t)P * P * sizeof(double)));
+    if (K > 0) CK(cudaMemcpy(dP, pts.data(), pts.size() * sizeof(double), cudaMemcpyHostToDevice));
+    for (int h0 = 0; h0 < K; h0 += KC) {
+      const int kc = (K - h0 < KC) ? K - h0 : KC;
+      imat_sh_kernel<<<(kc + 127) / 128, 128>>>(c->T, dP + 3 * (size_t)h0, kc, P, dY);
+      dim3 g((N + GT - 1) / GT, (N + GT - 1) / GT);
+      gram_kernel<<<g, 256>>>(dY, kc, N, dG);
+      gram_simpson_kernel<<<(P * P + 127) / 128, 128>>>(dY, kc, P, h0, dGs);
+      CK(cudaGetLastError());
+    }
+    const long long tot = (long long)N * N;
+    imat_assemble_kernel<<<(unsigned)((tot + 255) / 256), 256>>>(c->T, dG, dGs, P, dA, buried, dIM);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(imats + (size_t)k * N * N, dIM, (size_t)N * N * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  cleanup();
+  return PBSAM_OK;
+}
+
+// ------------------------------------------------------------------ self-polarization
+// pbsam spol (src/selfp_makemat.cpp:37-118, CMolecule::polarize_self,
+// src/molecule.cpp:1898-1979) for molecule type type_id (its own F/H inputs are
+// ignored).  Outputs are rounded as the reference writes them to .exp files
+// (8 significant digits, |x| < 1e-15 -> 0, src/readutil.cpp:541-556,
+// src/expansion.cpp:913-929): fself/hself[n_sph * p^2], hself_scale[n_sph].
+static double round8(double x)
+{
+  if (fabs(x) < 1e-15) return 0.0;
+  char b[64];
+  snprintf(b, sizeof b, "%.8g", x);
+  return strtod(b, nullptr);
+}
+
+extern "C" int pbsam_selfpol(pbsam_context *c, int type_id, int max_rounds, double *fself, double *hself,
+                             double *hself_scale, int *rounds)
+{
+  if (!c || type_id < 0 || type_id >= (int)c->types.size() || !fself || !hself || !hself_scale || max_rounds < 1)
+    return fail(PBSAM_E_BADARG, "bad argument");
+  pbsam_system *s = nullptr;
+  const int mt[1] = {type_id};
+  TRY(pbsam_system_create(c, 1, 1, mt, &s));
+  int *drounds = nullptr;
+  if (cudaMalloc(&drounds, sizeof(int)) != cudaSuccess) { pbsam_system_destroy(s); return fail(PBSAM_E_NOMEM, "rounds"); }
+  pbsam_selfpol_kernel<<<1, PBSAM_TEAM, team_smem_bytes(c->prm.poles), s->stream>>>(s->c, c->tv.Eass, max_rounds, drounds);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  const int ns = c->types[type_id].ns, NP2 = c->prm.poles * c->prm.poles;
+  std::vector<double> F((size_t)ns * NP2), H((size_t)ns * NP2);
+  int r = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(F.data(), s->c.bv.F, F.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(H.data(), s->c.bv.H, H.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(&r, drounds, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(drounds);
+  pbsam_system_destroy(s);
+  if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("self-polarization: ") + cudaGetErrorString(e));
+  for (size_t i = 0; i < F.size(); i++) { fself[i] = round8(F[i]); hself[i] = round8(H[i]); }
+  for (int k = 0; k < ns; k++) hself_scale[k] = round8(1.0 / c->types[type_id].rad[k]);
+  if (rounds) *rounds = r;
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_system_phase_ms(const pbsam_system *s, double *ms)
+{
+  if (!s || !ms) return fail(PBSAM_E_BADARG, "null argument");
+  CK(cudaSetDevice(s->ctx->device));
+  CK(cudaMemcpy(ms, s->c.bv.tphase, (size_t)s->B * 8 * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < s->B * 8; i++) ms[i] *= 1e-6;
   return PBSAM_OK;
 }

@@ -198,9 +198,14 @@ struct RotState {
 };
 
 // CRotCoeff::initParams + computeCoeff + computeGradCoeff (src/rotcoeff.cpp:154-244, 779-850).
-// shbuf: scratch of (2p-1)^2 doubles.
+// The recursion in m runs level by level in two shared-memory buffers lvA/lvB of
+// (2p-1)^2 complex entries (level entry (n, s) at n*n + n + s); R receives the
+// entries with n < min(p, nout) in the [n][n+s][m] layout (a prefix of the full
+// layout), which is all the rotation apply reads.  With grad, dR (full layout,
+// n < 2p-1, global) is computed alongside.  shbuf: (2p-1)^2 doubles of scratch.
 __device__ void rot_compute(const Team &tm, const Tab &T, double theta, double phi, double xi, int p, bool grad,
-                            RotState &rs, double2 *R, double2 *dR, double *shbuf)
+                            RotState &rs, double2 *R, double2 *dR, double *shbuf, double2 *lvA, double2 *lvB,
+                            int nout = 1 << 20)
 {
   rs.p = p; rs.R = R; rs.dR = dR; rs.xi = xi;
   double sint = sin(theta);
@@ -222,59 +227,61 @@ __device__ void rot_compute(const Team &tm, const Tab &T, double theta, double p
   { double sx, cx; sincos(xi, &sx, &cx); rs.exxi = make_double2(cx, sx); }
   if (rs.sing) return;
   const int NN = 2 * p - 1;
+  const int pout = p < nout ? p : nout;
   sh_full(tm, T, theta, phi, NN, shbuf);
   tm.sync();
   // level m = 0 from the spherical harmonics
-  for (int idx = tm.rank; idx < NN * (2 * NN - 1); idx += tm.size) {
-    int n = idx / (2 * NN - 1), s = idx % (2 * NN - 1) - (NN - 1);
-    if (n >= NN || s < -n || s > n) continue;
-    R[rot_at(n, s, 0)] = comp(shbuf, n, -s);
+  for (int idx = tm.rank; idx < NN * NN; idx += tm.size) {
+    int n = (int)sqrt((double)idx);
+    while (n * n > idx) n--;
+    while ((n + 1) * (n + 1) <= idx) n++;
+    const int s = idx - n * n - n;
+    const double2 v = comp(shbuf, n, -s);
+    lvA[idx] = v;
+    if (n < pout) R[rot_at(n, s, 0)] = v;
     if (grad) {
-      double2 v;
-      if (n == 0) v = make_double2(0.0, 0.0);
-      else {
-        int as = s < 0 ? -s : s;
-        double2 w;
-        if (as == 0) {
-          w = cscale(-sqrt((double)n * (n + 1)), cmul(rs.exiphi, comp(shbuf, n, 1)));
-        } else if (as < n) {
-          w = csub(cscale(as * rs.cott, comp(shbuf, n, as)),
-                   cscale(sqrt((double)(n - as) * (n + as + 1)), cmul(rs.exiphi, comp(shbuf, n, as + 1))));
-        } else {
-          w = cscale(n * rs.cott, comp(shbuf, n, n));
-        }
-        // dROT(n,-s,0) = w for s >= 0; dROT(n,s,0) = conj(w)
-        v = (s <= 0) ? w : cconj(w);
-        if (as == 0) v = w;
-      }
-      dR[rot_at(n, s, 0)] = v;
+      double2 w;
+      const int as = s < 0 ? -s : s;
+      if (n == 0) w = make_double2(0.0, 0.0);
+      else if (as == 0) w = cscale(-sqrt((double)n * (n + 1)), cmul(rs.exiphi, comp(shbuf, n, 1)));
+      else if (as < n)
+        w = csub(cscale(as * rs.cott, comp(shbuf, n, as)),
+                 cscale(sqrt((double)(n - as) * (n + as + 1)), cmul(rs.exiphi, comp(shbuf, n, as + 1))));
+      else w = cscale(n * rs.cott, comp(shbuf, n, n));
+      // w = dROT(n, -|s|, 0); dROT(n, |s|, 0) = conj(w)
+      dR[rot_at(n, s, 0)] = (s <= 0) ? w : cconj(w);
     }
   }
   tm.sync();
   const double r1 = -0.5 * (1 + rs.cost), r2 = 0.5 * (1 - rs.cost), r3 = -rs.sint;
   const double dr1 = 0.5 * rs.sint, dr2 = dr1, dr3 = -rs.cost;
+  double2 *cur = lvA, *nxt = lvB;
   for (int m = 0; m < p - 1; m++) {
     const int n0 = m + 2, n1 = 2 * p - m - 1;          // n in [n0, n1)
     const int W = 2 * (n1 - 1) - 1;                     // widest s range
     const int cnt = (n1 - n0) * W;
     for (int idx = tm.rank; idx < cnt; idx += tm.size) {
-      int n = n0 + idx / W, s = idx % W - (W / 2);
+      const int n = n0 + idx / W, s = idx % W - (W / 2);
       if (s <= -n || s >= n) continue;
       const int as = s < 0 ? -s : s;
-      double2 d1 = cscale(r1 * T.ETA(n, s - 1), R[rot_at(n, s - 1, m)]);
-      double2 d2 = cscale(r2 * T.ETA(n, -s - 1), R[rot_at(n, s + 1, m)]);
-      double2 d3 = cscale(r3 * T.ZETA(n - 1, as), R[rot_at(n, s, m)]);
-      double2 acc = cadd(cadd(cmul(d1, rs.exiphi), cmul(d2, rs.exphi)), d3);
-      R[rot_at(n - 1, s, m + 1)] = cdivr(cmul(rs.exxi, acc), T.ETA(n, m));
+      const double2 a = cur[n * n + n + s - 1], b = cur[n * n + n + s + 1], c = cur[n * n + n + s];
+      const double2 d1 = cscale(r1 * T.ETA(n, s - 1), a);
+      const double2 d2 = cscale(r2 * T.ETA(n, -s - 1), b);
+      const double2 d3 = cscale(r3 * T.ZETA(n - 1, as), c);
+      const double2 acc = cadd(cadd(cmul(d1, rs.exiphi), cmul(d2, rs.exphi)), d3);
+      const double2 v = cdivr(cmul(rs.exxi, acc), T.ETA(n, m));
+      nxt[(n - 1) * (n - 1) + (n - 1) + s] = v;
+      if (n - 1 < pout) R[rot_at(n - 1, s, m + 1)] = v;
       if (grad) {
-        double2 e1 = cscale(T.ETA(n, s - 1), cadd(cscale(r1, dR[rot_at(n, s - 1, m)]), cscale(dr1, R[rot_at(n, s - 1, m)])));
-        double2 e2 = cscale(T.ETA(n, -s - 1), cadd(cscale(r2, dR[rot_at(n, s + 1, m)]), cscale(dr2, R[rot_at(n, s + 1, m)])));
-        double2 e3 = cscale(T.ZETA(n - 1, as), cadd(cscale(r3, dR[rot_at(n, s, m)]), cscale(dr3, R[rot_at(n, s, m)])));
-        double2 a2 = cadd(cadd(cmul(e1, rs.exiphi), cmul(e2, rs.exphi)), e3);
+        const double2 e1 = cscale(T.ETA(n, s - 1), cadd(cscale(r1, dR[rot_at(n, s - 1, m)]), cscale(dr1, a)));
+        const double2 e2 = cscale(T.ETA(n, -s - 1), cadd(cscale(r2, dR[rot_at(n, s + 1, m)]), cscale(dr2, b)));
+        const double2 e3 = cscale(T.ZETA(n - 1, as), cadd(cscale(r3, dR[rot_at(n, s, m)]), cscale(dr3, c)));
+        const double2 a2 = cadd(cadd(cmul(e1, rs.exiphi), cmul(e2, rs.exphi)), e3);
         dR[rot_at(n - 1, s, m + 1)] = cdivr(cmul(rs.exxi, a2), T.ETA(n, m));
       }
     }
     tm.sync();
+    double2 *t = cur; cur = nxt; nxt = t;
   }
 }
 

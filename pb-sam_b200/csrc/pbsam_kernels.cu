@@ -28,6 +28,10 @@ struct Scr {
   double *part;          // PBSAM_NCH * 3 * NP2
   double *sol;           // 6 * 3 * NP2 (solver work)
   double *misc;          // 4096
+  double2 *lvA, *lvB;    // shared memory: rotation recursion levels, (2NP-1)^2 each
+  double *stage;         // shared memory (aliases the levels): IMat row stages
+  unsigned long long *bars;  // shared memory: one mbarrier per stage
+  double *xs;            // shared memory: matvec operand, 3 * NP2
   __device__ double *E(int i) const { return e + (size_t)i * NP2; }
   __device__ double *G(int i) const { return g + (size_t)i * 3 * NP2; }
 };
@@ -50,9 +54,42 @@ __host__ __device__ inline long long scr_doubles(int NP, long long S)
   return n;
 }
 
-__device__ Scr make_scr(double *base, int NP)
+// IMat streaming: NSTAGE shared-memory stages of rows_per_stage rows each
+#define PBSAM_NSTAGE 3
+#define PBSAM_STAGE_BYTES (56 * 1024)
+__host__ __device__ inline int rows_per_stage(int NP2)
+{
+  int rb = PBSAM_STAGE_BYTES / (NP2 * 8);
+  int cap = (NP2 + PBSAM_NSTAGE - 1) / PBSAM_NSTAGE;   // all stages together hold the whole matrix
+  cap = (cap + 1) & ~1;
+  if (rb > cap) rb = cap;
+  rb &= ~1;
+  return rb < 2 ? 2 : rb;
+}
+// dynamic shared memory of every team kernel: [max(rotation levels, IMat stages)][operand x][mbarriers]
+__host__ __device__ inline size_t team_smem_bytes(int NP)
+{
+  const size_t NN = 2 * NP - 1, NP2 = (size_t)NP * NP;
+  size_t lv = 2 * NN * NN * sizeof(double2);
+  const size_t st = (size_t)PBSAM_NSTAGE * rows_per_stage((int)NP2) * NP2 * sizeof(double);
+  if (st > lv) lv = st;
+  return lv + 3 * NP2 * sizeof(double) + 64;
+}
+
+__device__ Scr make_scr(double *base, int NP, void *smem)
 {
   Scr s;
+  {
+    const int NN = 2 * NP - 1, NP2 = NP * NP;
+    size_t lv = 2 * (size_t)NN * NN * sizeof(double2);
+    const size_t st = (size_t)PBSAM_NSTAGE * rows_per_stage(NP2) * NP2 * sizeof(double);
+    if (st > lv) lv = st;
+    s.lvA = (double2 *)smem;
+    s.lvB = s.lvA + NN * NN;
+    s.stage = (double *)smem;
+    s.xs = (double *)((char *)smem + lv);
+    s.bars = (unsigned long long *)((char *)smem + lv + 3 * (size_t)NP2 * sizeof(double));
+  }
   const int NP2 = NP * NP;
   const int NN = 2 * NP - 1;
   const long long rotE = rot_off(NN), trE = tr_off(NN);
@@ -73,6 +110,24 @@ __device__ Scr make_scr(double *base, int NP)
   s.misc = p;
   return s;
 }
+
+// ------------------------------------------------------------------ phase timers
+enum { PH_SOLVE = 0, PH_SURF, PH_NUMERIC, PH_INTRA, PH_LS, PH_DTA, PH_TOTAL, PH_N };
+__device__ __forceinline__ unsigned long long gtimer()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+struct PhaseClock {
+  double *acc;
+  unsigned long long t0;
+  __device__ void start(const Team &tm) { if (tm.rank == 0) t0 = gtimer(); }
+  __device__ void stop(const Team &tm, int ph) { if (tm.rank == 0 && acc) acc[ph] += (double)(gtimer() - t0); }
+};
+
+// per-sphere stride of the row-major IMat store (even, so every row block is 16-byte aligned)
+__host__ __device__ inline size_t imat_stride(int NP2) { return ((size_t)NP2 * NP2 + 1) & ~(size_t)1; }
 
 // ------------------------------------------------------------------ team helpers
 __device__ __forceinline__ void tcopy(const Team &tm, double *dst, const double *src, int n)
@@ -126,7 +181,7 @@ __device__ void prep_pair(const Team &tm, const Tab &T, const Scr &sc, const dou
   const Sph S = cart2sph(P[0], P[1], P[2]);
   const int prot = pF > pH ? pF : pH;
   X.pH = pH; X.pF = pF;
-  rot_compute(tm, T, S.theta, S.phi, PB_PI, prot, grad, X.rs, sc.R, sc.dR, sc.sh);
+  rot_compute(tm, T, S.theta, S.phi, PB_PI, prot, grad, X.rs, sc.R, sc.dR, sc.sh, sc.lvA, sc.lvB);
   trans_compute(tm, T, S.rho, T.kappa, pH, sS, sT, grad, X.th, sc.TH, sc.dTH, sc.kbuf);
   if (pF > 0) trans_compute(tm, T, S.rho, 0.0, pF, sS, sT, false, X.tf, sc.TF, nullptr, sc.kbuf);
   if (tm.rank == 0) {
@@ -144,6 +199,31 @@ __device__ void prep_pair(const Team &tm, const Tab &T, const Scr &sc, const dou
     const double irst = ir / st, irct = ir * ct;
     double m[9] = {st * cp, irct * cp, -irst * sp, st * sp, irct * sp, irst * cp, ct, -ir * st, 0.0};
     for (int i = 0; i < 9; i++) X.Rm[i] = m[i];
+  }
+  tm.sync();
+}
+
+// Prepared intra-molecular pair from the molecule-type tables (coefficients of
+// near pair entry e computed once at set-up; the per-pair orders only truncate them).
+__device__ void table_pair(const Team &tm, const Tab &T, const TypeView &tv, const Scr &sc, int e, int pH, int pF,
+                           double sS, double sT, PairXf &X)
+{
+  const int NP = T.NP;
+  const double *v = tv.pS + 16 * (size_t)e;
+  X.pH = pH; X.pF = pF;
+  X.rs.p = pH > pF ? pH : pF;
+  X.rs.sing = v[0] != 0.0;
+  X.rs.cost = v[1]; X.rs.sint = v[2]; X.rs.cott = v[3]; X.rs.xi = v[4];
+  X.rs.exphi = make_double2(v[5], v[6]);
+  X.rs.exiphi = cconj(X.rs.exphi);
+  X.rs.exxi = make_double2(v[7], v[8]);
+  X.rs.R = tv.pR + (size_t)e * rot_off(NP);
+  X.rs.dR = nullptr;
+  X.th.p = pH; X.th.scalei = sS; X.th.scaleo = sT; X.th.T = tv.pTH + (size_t)e * tr_off(NP); X.th.dT = nullptr;
+  X.tf.p = pF; X.tf.scalei = sS; X.tf.scaleo = sT; X.tf.T = tv.pTF + (size_t)e * tr_off(NP); X.tf.dT = nullptr;
+  if (tm.rank == 0) {
+    sc.fact[0] = 1.0;
+    for (int n = 1; n < NP; n++) sc.fact[n] = sc.fact[n - 1] * (sT / sS);
   }
   tm.sync();
 }
@@ -349,6 +429,120 @@ __device__ void surface_q(const Team &tm, const Tab &T, const double *pts, int N
   for (int k = 0; k < NC; k++) tot[k] = team_sum(tm, ta[k], red);
 }
 
+// ------------------------------------------------------------------ IMat product
+// Y[d*NP2 + i] = scale[n(i)] * sum_k IMT[i][k] x[d*NP2 + k] for d < D (applyMMat,
+// src/lautil.cpp:57-72, followed by revertF / revertH).  IMT is the IMat stored
+// row-major with 16-byte aligned rows of even count per stage; row blocks stream
+// from HBM into PBSAM_NSTAGE shared-memory stages with bulk asynchronous copies
+// completed on one mbarrier per stage, one warp per row reading the stage, the
+// D operands in shared memory.  Every wait is bounded: on expiry the team's error
+// flag is set and the result is abandoned.
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, int count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(unsigned long long *bar)
+{
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity)
+{
+  for (long it = 0; it < (1L << 24); it++) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ void imat_apply(const Team &tm, const Scr &sc, const double *IMT, const double *x, int NP2, int D,
+                           double *Y, const double *scale, int *err)
+{
+  const int lane = tm.rank & 31, warp = tm.rank >> 5, nw = tm.size >> 5;
+  const int RB = rows_per_stage(NP2);
+  const int nblk = (NP2 + RB - 1) / RB;
+  const bool async_ok = (NP2 % 2 == 0) && ((((unsigned long long)IMT) & 15ULL) == 0);
+  volatile int *fail = (volatile int *)(sc.bars + PBSAM_NSTAGE);
+  int issued = 0, done = 0;
+  if (async_ok) {
+    if (tm.rank == 0) {
+      *fail = 0;
+      for (int q = 0; q < PBSAM_NSTAGE; q++) mbar_init(&sc.bars[q], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tm.sync();
+    issued = nblk < PBSAM_NSTAGE ? nblk : PBSAM_NSTAGE;
+    if (tm.rank == 0)
+      for (int q = 0; q < issued; q++) {
+        const int r0 = q * RB, nr = (NP2 - r0 < RB) ? NP2 - r0 : RB;
+        bulk_load(sc.stage + (size_t)q * RB * NP2, IMT + (size_t)r0 * NP2, (unsigned)(nr * NP2 * 8), &sc.bars[q]);
+      }
+  }
+  for (int blk = 0; blk < nblk; blk++) {
+    const int q = blk % PBSAM_NSTAGE;
+    const int r0 = blk * RB, nr = (NP2 - r0 < RB) ? NP2 - r0 : RB;
+    const double *rows;
+    if (async_ok) {
+      if (!mbar_wait(&sc.bars[q], (unsigned)((blk / PBSAM_NSTAGE) & 1))) *fail = 1;
+      rows = sc.stage + (size_t)q * RB * NP2;
+    } else rows = IMT + (size_t)r0 * NP2;
+    for (int rr = warp; rr < nr; rr += nw) {
+      const double *row = rows + (size_t)rr * NP2;
+      const int i = r0 + rr;
+      double acc[3] = {0.0, 0.0, 0.0};
+      for (int k = lane; k < NP2; k += 32) {
+        const double a = row[k];
+        for (int d = 0; d < D; d++) acc[d] += a * x[d * NP2 + k];
+      }
+      int n = (int)sqrt((double)i);
+      while (n * n > i) n--;
+      while ((n + 1) * (n + 1) <= i) n++;
+      for (int d = 0; d < D; d++) {
+        double v = acc[d];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) Y[d * NP2 + i] = v * scale[n];
+      }
+    }
+    tm.sync();
+    done = blk + 1;
+    if (async_ok && *fail) break;
+    if (async_ok && blk + PBSAM_NSTAGE < nblk) {
+      if (tm.rank == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const int b2 = blk + PBSAM_NSTAGE, s0 = b2 * RB, n2 = (NP2 - s0 < RB) ? NP2 - s0 : RB;
+        bulk_load(sc.stage + (size_t)q * RB * NP2, IMT + (size_t)s0 * NP2, (unsigned)(n2 * NP2 * 8), &sc.bars[q]);
+      }
+      issued++;
+    }
+  }
+  if (async_ok) {
+    if (*fail) {
+      // a wait expired: drain this team's copies still in flight (bounded), report, move on
+      if (tm.rank == 0) {
+        for (int b2 = done; b2 < issued; b2++) mbar_wait(&sc.bars[b2 % PBSAM_NSTAGE], (unsigned)((b2 / PBSAM_NSTAGE) & 1));
+        if (err) *err = 1;
+      }
+    }
+    tm.sync();
+    if (tm.rank == 0)
+      for (int q = 0; q < PBSAM_NSTAGE; q++) mbar_inval(&sc.bars[q]);
+    tm.sync();
+  }
+}
+
 // ------------------------------------------------------------------ F/H inner solve
 // Fixed-point solve of one sphere's surface-charge expansions
 // (CSolExpCenter::solveFH, src/expcenter.cpp:1079-1370) for D = 1 (F, H) or
@@ -361,8 +555,8 @@ __device__ double solve_fh(const Team &tm, const Tab &T, const TypeView &tv, con
   const int NP = T.NP, NP2 = NP * NP, len = D * NP2;
   const double *cst = tv.cst + (size_t)ts * CST_N * NP;
   const double *Dfix = tv.Dfix + (size_t)ts * NP2, *Vfix = tv.Vfix + (size_t)ts * NP2;
-  const double *IM = tv.imat + (size_t)ts * NP2 * NP2;
-  double *fbase = sc.sol, *hbase = sc.sol + len, *fx = sc.sol + 2 * len, *hx = sc.sol + 3 * len;
+  const double *IM = tv.imat + (size_t)ts * imat_stride(NP2);
+  double *fbase = sc.sol, *hbase = sc.sol + len, *fx = sc.xs, *hx = sc.xs;
   double *oldH = sc.sol + 4 * len, *outH = sc.sol + 5 * len;
   for (int k = tm.rank; k < len; k += tm.size) {
     const int kk = k % NP2;
@@ -391,16 +585,7 @@ __device__ double solve_fh(const Team &tm, const Tab &T, const TypeView &tv, con
       fx[k] = fbase[k] + cst[CST_H1 * NP + n] * H[k] + cst[CST_F1 * NP + n] * F[k];
     }
     tm.sync();
-    for (int k = tm.rank; k < len; k += tm.size) {
-      const int d = k / NP2, i = k % NP2;
-      int n = (int)sqrt((double)i);
-      while (n * n > i) n--;
-      while ((n + 1) * (n + 1) <= i) n++;
-      const double *x = fx + d * NP2;
-      double s = 0.0;
-      for (int kk = 0; kk < NP2; kk++) s += IM[(size_t)kk * NP2 + i] * x[kk];
-      F[k] = s * T.CONST3[n];
-    }
+    imat_apply(tm, sc, IM, sc.xs, NP2, D, F, T.CONST3, stats ? stats + 7 : nullptr);
     tm.sync();
     for (int k = tm.rank; k < len; k += tm.size) {
       const int kk = k % NP2;
@@ -410,16 +595,7 @@ __device__ double solve_fh(const Team &tm, const Tab &T, const TypeView &tv, con
       hx[k] = hbase[k] + cst[CST_H2 * NP + n] * H[k] + cst[CST_F2 * NP + n] * F[k];
     }
     tm.sync();
-    for (int k = tm.rank; k < len; k += tm.size) {
-      const int d = k / NP2, i = k % NP2;
-      int n = (int)sqrt((double)i);
-      while (n * n > i) n--;
-      while ((n + 1) * (n + 1) <= i) n++;
-      const double *x = hx + d * NP2;
-      double s = 0.0;
-      for (int kk = 0; kk < NP2; kk++) s += IM[(size_t)kk * NP2 + i] * x[kk];
-      H[k] = s * cst[CST_INVH * NP + n];
-    }
+    imat_apply(tm, sc, IM, sc.xs, NP2, D, H, cst + CST_INVH * NP, stats ? stats + 7 : nullptr);
     tm.sync();
     // computeDev over complex entries (d, n, m)
     double part = 0.0;
@@ -477,6 +653,7 @@ struct Sys {
   int b, NP, NP2, S;
   Scr sc;
   double *red;
+  double *tph;
   __device__ int ts(int s) const { return c->bv.sph_ts[s]; }
   __device__ int mol(int s) const { return c->bv.sph_mol[s]; }
   __device__ double rad(int s) const { return c->tv.rad[ts(s)]; }
@@ -540,6 +717,8 @@ __device__ void add_vec_into(const Team &tm, double *dst, const double *src, int
 __device__ void reexpand_LS(const Team &tm, const Sys &y, int s, bool fromSelf)
 {
   const Tab &T = y.c->T;
+  PhaseClock pc{y.tph, 0};
+  pc.start(tm);
   double *LSrot = y.sc.E(6), *tL = y.sc.E(7);
   tzero(tm, LSrot, y.NP2);
   tm.sync();
@@ -563,6 +742,7 @@ __device__ void reexpand_LS(const Team &tm, const Sys &y, int s, bool fromSelf)
   const RotState mr = y.molrot(y.mol(s));
   rot_apply_xi(tm, mr, LSrot, y.LS(s), y.NP, false, y.NP);
   tm.sync();
+  pc.stop(tm, PH_LS);
 }
 
 // F/H solve + surface charges of one sphere (src/expcenter.cpp:594-629)
@@ -570,7 +750,11 @@ __device__ double solve_surface(const Team &tm, const Sys &y, int s, bool rotH)
 {
   const Tab &T = y.c->T;
   const int ts = y.ts(s);
+  PhaseClock pc{y.tph, 0};
+  pc.start(tm);
   double dv = solve_fh(tm, T, y.c->tv, y.c->prm, y.sc, ts, 1, y.F(s), y.H(s), y.LFS(s), y.LHS(s), y.red, y.stats());
+  pc.stop(tm, PH_SOLVE);
+  pc.start(tm);
   if (rotH) {
     const RotState mr = y.molrot(y.mol(s));
     rot_apply_xi(tm, mr, y.H(s), y.Hrot(s), y.NP, true, y.NP);
@@ -581,6 +765,7 @@ __device__ double solve_surface(const Team &tm, const Sys &y, int s, bool rotH)
   surface_q<1>(tm, T, y.spx(s), y.npts(s), dA, y.F(s), T.CONST2, y.qF(s), tot, y.red);
   double tF = tot[0];
   surface_q<1>(tm, T, y.spx(s), y.npts(s), dA, y.H(s), cst + CST_CHGH * y.NP, y.qH(s), tot, y.red);
+  pc.stop(tm, PH_SURF);
   if (tm.rank == 0) {
     y.c->bv.tF[y.sc1(s)] = tF;
     y.c->bv.tH[y.sc1(s)] = tot[0];
@@ -629,14 +814,18 @@ __device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s)
     const double sep = rho - y.rad(s) - rj;
     const int pF = compute_order(y.NP, rho, y.c->bv.tF[y.sc1(s2)], rj);
     const int pH = compute_order(y.NP, rho, y.c->bv.tH[y.sc1(s2)], rj);
+    PhaseClock pc{y.tph, 0};
+    pc.start(tm);
     if (sep > 0 && !(sep < y.c->prm.min_sep_numeric)) {
       PairXf X;
-      prep_pair(tm, T, y.sc, P, pH, pF, rj, y.rad(s), false, X);
+      table_pair(tm, T, y.c->tv, y.sc, e, pH, pF, rj, y.rad(s), X);
       pair_apply(tm, T, y.sc, X, true, y.F(s2), a);
       pair_apply(tm, T, y.sc, X, false, y.H(s2), bq);
+      pc.stop(tm, PH_INTRA);
     } else {
       numeric_expand<1>(tm, T, y.sc, y.spx(s2), y.npts(s2), P, y.qF(s2), true, false, pF, y.rad(s), a);
       numeric_expand<1>(tm, T, y.sc, y.spx(s2), y.npts(s2), P, y.qH(s2), true, true, pH, y.rad(s), bq);
+      pc.stop(tm, PH_NUMERIC);
     }
     for (int t = tm.rank; t < y.NP2; t += tm.size) { y.LFS(s)[t] += a[t]; y.LHS(s)[t] += bq[t]; }
     tm.sync();
@@ -658,6 +847,8 @@ __device__ double recompute(const Team &tm, const Sys &y, int s)             // 
 __device__ void grad_xform_from(const Team &tm, const Sys &y, int s, int sm, bool self, double *acc)
 {
   const Tab &T = y.c->T;
+  PhaseClock pc{y.tph, 0};
+  pc.start(tm);
   double ci[3], cm[3];
   y.cen_lab(s, ci);
   y.cen_lab(sm, cm);
@@ -670,6 +861,7 @@ __device__ void grad_xform_from(const Team &tm, const Sys &y, int s, int sm, boo
   double *G = y.sc.G(0);
   pair_apply_grad(tm, T, y.sc, X, self ? y.HselfRot(sm) : y.Hrot(sm), G);
   add_vec_into(tm, acc, G, 3 * y.NP2);
+  pc.stop(tm, PH_DTA);
 }
 
 __device__ void prepare_dta_iself(const Team &tm, const Sys &y, int s)     // src/molecule.cpp:1584-1628
@@ -734,7 +926,12 @@ __device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int
     const int pH = compute_order(y.NP, rho, bv.maxgH[y.sc1(sm)], rm);
     if (sep > 0 && !(sep < y.c->prm.min_sep_numeric)) {
       PairXf X;
-      prep_pair(tm, T, y.sc, P, pH, pF, rm, y.rad(s), false, X);
+      const int kloc = sm - bv.mol_off[i];
+      int e = -1;
+      for (int q = y.c->tv.near_off[ts]; q < y.c->tv.near_off[ts + 1]; q++)
+        if (y.c->tv.near[q] == kloc) { e = q; break; }
+      if (e >= 0) table_pair(tm, T, y.c->tv, y.sc, e, pH, pF, rm, y.rad(s), X);
+      else prep_pair(tm, T, y.sc, P, pH, pF, rm, y.rad(s), false, X);
       const int km = bv.gkey[y.sc1(sm)];
       for (int cc = 0; cc < 3; cc++) {
         pair_apply(tm, T, y.sc, X, true, y.gw(bv.gFw, km) + cc * NP2, tL);
@@ -751,7 +948,10 @@ __device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int
   }
   add_vec_into(tm, LGH, LGH2, 3 * NP2);
   double *gF = y.gw(bv.gFw, key), *gHk = y.gw(bv.gHw, key);
+  PhaseClock pc{y.tph, 0};
+  pc.start(tm);
   const double dv = solve_fh(tm, T, y.c->tv, y.c->prm, y.sc, ts, 3, gF, gHk, LGF, LGH, y.red, y.stats());
+  pc.stop(tm, PH_SOLVE);
   for (int cc = 0; cc < 3; cc++) rot_apply_xi(tm, mr, gHk + cc * NP2, y.gw(bv.gHrotw, key) + cc * NP2, y.NP, true, y.NP);
   tm.sync();
   // exposed gradient charges (src/expcenter.cpp:1377-1412)
@@ -792,6 +992,7 @@ __device__ double inprod_ml(const double *M, double mscale, const double *L, dou
 // ------------------------------------------------------------------ the force kernel
 __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
 {
+  extern __shared__ double2 dsm[];
   __shared__ double red[PBSAM_TEAM];
   __shared__ double shv[16];
   const Team tm{(int)threadIdx.x, (int)blockDim.x};
@@ -800,14 +1001,18 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
   if (b >= bv.B) return;
   Sys y;
   y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = bv.S;
-  y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP);
+  y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP, dsm);
   y.red = red;
+  y.tph = bv.tphase + (size_t)b * 8;
   const int S = bv.S, nmol = bv.nmol, NP2 = y.NP2;
   int *st = y.stats();
+  PhaseClock total{y.tph, 0};
   if (tm.rank == 0) {
     for (int k = 0; k < 8; k++) st[k] = 0;
+    for (int k = 0; k < 8; k++) y.tph[k] = 0.0;
     bv.status[b] = PBSAM_STATUS_OK;
   }
+  total.start(tm);
   for (int t = tm.rank; t < nmol * 3; t += tm.size) {
     bv.force[(size_t)b * nmol * 3 + t] = 0.0;
     bv.torque[(size_t)b * nmol * 3 + t] = 0.0;
@@ -904,7 +1109,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
     quat_angles(qn, th, ph, xi);
     RotState rs;
     double2 *Rm = bv.molR + ((size_t)b * nmol + i) * rot_off(2 * y.NP - 1);
-    rot_compute(tm, T, th, ph, xi, y.NP, false, rs, Rm, nullptr, y.sc.sh);
+    rot_compute(tm, T, th, ph, xi, y.NP, false, rs, Rm, nullptr, y.sc.sh, y.sc.lvA, y.sc.lvB);
     if (tm.rank == 0) {
       double *v = bv.molRS + ((size_t)b * nmol + i) * 16;
       v[0] = rs.sing ? 1.0 : 0.0; v[1] = rs.cost; v[2] = rs.sint; v[3] = rs.cott; v[4] = rs.xi;
@@ -1077,6 +1282,8 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
     qrot(qn, Tq, bv.torque + ((size_t)b * nmol + i) * 3);
   }
   tm.sync();
+  if (tm.rank == 0 && st[7] != 0) bv.status[b] = PBSAM_STATUS_WAIT_EXPIRED;
+  total.stop(tm, PH_TOTAL);
   (void)shv;
 }
 
@@ -1084,6 +1291,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
 // molecule-frame H, src/moldynamics.cpp:358-386, src/molecule.cpp:1850-1890)
 __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c)
 {
+  extern __shared__ double2 dsm[];
   __shared__ double red[PBSAM_TEAM];
   const Team tm{(int)threadIdx.x, (int)blockDim.x};
   const BatchView &bv = c.bv;
@@ -1091,8 +1299,9 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c)
   if (b >= bv.B) return;
   Sys y;
   y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = bv.S;
-  y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP);
+  y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP, dsm);
   y.red = red;
+  y.tph = nullptr;
   const Tab &T = c.T;
   double pot = 0.0;
   if (bv.status[b] == PBSAM_STATUS_OK) {
@@ -1173,13 +1382,14 @@ __global__ void pbsam_init_kernel(Ctx c)
 // Dirichlet/Neumann terms (src/expcenter.cpp:513-552, 1041-1060)
 __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup1_kernel(Ctx c, double *scr, long long scr_stride)
 {
+  extern __shared__ double2 dsm[];
   __shared__ double red[PBSAM_TEAM];
   const Team tm{(int)threadIdx.x, (int)blockDim.x};
   const Tab &T = c.T;
   const TypeView &tv = c.tv;
   const int ts = blockIdx.x;
   const int NP = T.NP, NP2 = NP * NP;
-  Scr sc = make_scr(scr + (size_t)ts * scr_stride, NP);
+  Scr sc = make_scr(scr + (size_t)ts * scr_stride, NP, dsm);
   int t = 0;
   while (tv.type_off[t + 1] <= ts) t++;
   const double rad = tv.rad[ts];
@@ -1230,6 +1440,12 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup1_kernel(Ctx c, double 
   double *Efix = sc.E(10), *Lfix = sc.E(11);
   numeric_expand<1>(tm, T, sc, tv.chg_pos + 3 * (size_t)q0, nq, cs, win, false, false, NP, rad, Efix);
   numeric_expand<1>(tm, T, sc, tv.chg_pos + 3 * (size_t)q0, nq, cs, wout, true, false, NP, rad, Lfix);
+  // multipole of the charges assigned to this sphere (CExpCenter::setFixedCharges, src/expcenter.cpp:88-103)
+  for (int k = tm.rank; k < nq; k += tm.size)
+    win[k] = (tv.chg_lab[q0 + k] == ts - tv.type_off[t]) ? tv.chg[q0 + k] / c.prm.idiel : 0.0;
+  tm.sync();
+  numeric_expand<1>(tm, T, sc, tv.chg_pos + 3 * (size_t)q0, nq, cs, win, false, false, NP, rad,
+                    tv.Eass + (size_t)ts * NP2);
   const double eps = c.prm.idiel / c.prm.sdiel;
   for (int k = tm.rank; k < NP2; k += tm.size) {
     int n = (int)sqrt((double)k);
@@ -1245,12 +1461,13 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup1_kernel(Ctx c, double 
 // src/molecule.cpp:544-696)
 __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup2_kernel(Ctx c, double *scr, long long scr_stride)
 {
+  extern __shared__ double2 dsm[];
   const Team tm{(int)threadIdx.x, (int)blockDim.x};
   const Tab &T = c.T;
   const TypeView &tv = c.tv;
   const int ts = blockIdx.x;
   const int NP = T.NP, NP2 = NP * NP;
-  Scr sc = make_scr(scr + (size_t)ts * scr_stride, NP);
+  Scr sc = make_scr(scr + (size_t)ts * scr_stride, NP, dsm);
   int t = 0;
   while (tv.type_off[t + 1] <= ts) t++;
   const int t0 = tv.type_off[t], ns = tv.type_off[t + 1] - t0, ki = ts - t0;
@@ -1291,7 +1508,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup2_kernel(Ctx c, double 
     const double sep = rho - ri - rj;
     if (sep > 0 && !(sep < c.prm.min_sep_numeric)) {
       PairXf X;
-      prep_pair(tm, T, sc, P, NP, NP, rj, ri, false, X);
+      table_pair(tm, T, tv, sc, e, NP, NP, rj, ri, X);
       pair_apply(tm, T, sc, X, true, tv.Fself + (size_t)tj * NP2, a);
       pair_apply(tm, T, sc, X, false, tv.Hself + (size_t)tj * NP2, bq);
     } else {
@@ -1304,6 +1521,48 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup2_kernel(Ctx c, double 
     for (int i = tm.rank; i < NP2; i += tm.size) { LFi[i] += a[i]; LHi[i] += bq[i]; }
     tm.sync();
   }
+}
+
+// per near pair entry e: rotation and translation coefficients at the full pole
+// order (CXFormAIntra::reset, src/xforms.cpp:213-227), kept as the prefixes the
+// apply reads (rotation n < NP, translation l < NP); entries re-expanded
+// numerically are left unused.
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup3_kernel(Ctx c, int e0, int ne, double *scr, long long stride)
+{
+  extern __shared__ double2 dsm[];
+  const Team tm{(int)threadIdx.x, (int)blockDim.x};
+  const Tab &T = c.T;
+  const TypeView &tv = c.tv;
+  const int NP = T.NP;
+  const int e = e0 + blockIdx.x;
+  if (blockIdx.x >= ne) return;
+  const int NN = 2 * NP - 1;
+  double *sh = scr + (size_t)blockIdx.x * stride;
+  double *TH = sh + 4 * NP * NP, *kbuf = TH + tr_off(NN);
+  double2 *lvA = dsm, *lvB = dsm + NN * NN;
+  int ts = 0;
+  while (tv.near_off[ts + 1] <= e) ts++;
+  int t = 0;
+  while (tv.type_off[t + 1] <= ts) t++;
+  const int tj = tv.type_off[t] + tv.near[e];
+  const double *ci = tv.cen + 3 * ts, *cj = tv.cen + 3 * tj;
+  const double P[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+  const Sph S = cart2sph(P[0], P[1], P[2]);
+  const double sep = S.rho - tv.rad[ts] - tv.rad[tj];
+  if (!(sep > 0 && !(sep < c.prm.min_sep_numeric))) return;
+  RotState rs;
+  rot_compute(tm, T, S.theta, S.phi, PB_PI, NP, false, rs, tv.pR + (size_t)e * rot_off(NP), nullptr, sh, lvA, lvB);
+  if (tm.rank == 0) {
+    double *v = tv.pS + 16 * (size_t)e;
+    v[0] = rs.sing ? 1.0 : 0.0; v[1] = rs.cost; v[2] = rs.sint; v[3] = rs.cott; v[4] = rs.xi;
+    v[5] = rs.exphi.x; v[6] = rs.exphi.y; v[7] = rs.exxi.x; v[8] = rs.exxi.y;
+  }
+  TransState ts1;
+  trans_compute(tm, T, S.rho, T.kappa, NP, tv.rad[tj], tv.rad[ts], false, ts1, TH, nullptr, kbuf);
+  for (int i = tm.rank; i < tr_off(NP); i += tm.size) tv.pTH[(size_t)e * tr_off(NP) + i] = TH[i];
+  tm.sync();
+  trans_compute(tm, T, S.rho, 0.0, NP, tv.rad[tj], tv.rad[ts], false, ts1, TH, nullptr, kbuf);
+  for (int i = tm.rank; i < tr_off(NP); i += tm.size) tv.pTF[(size_t)e * tr_off(NP) + i] = TH[i];
 }
 
 }  // namespace pbsam

@@ -46,6 +46,12 @@ struct TypeView {
   const int *chg_off;      // [ntypes+1]
   const double *chg_pos;   // [TQ][3] relative to the molecule centre
   const double *chg;       // [TQ]
+  const int *chg_lab;      // [TQ] sphere (within the type) each charge is assigned to
+  double *Eass;            // [TS][NP2] multipole of the assigned charges (self-polarization start)
+  // coefficient tables of the intra near pairs, one per near-list entry
+  double2 *pR;             // [TE][rot_off(NP)]
+  double *pTH, *pTF;       // [TE][tr_off(NP)] screened / unscreened translation
+  double *pS;              // [TE][16] rotation scalars
 };
 
 // Batch of B independent systems with the same list of molecules.
@@ -78,6 +84,8 @@ struct BatchView {
   double *force, *torque, *energy;  // [B][nmol][3], [B][nmol][3], [B]
   int *status;               // [B]
   int *stats;                // [B][8]: sweeps, inner iterations, solves, grad solves, ...
+  double *tphase;            // [B][8] device time per phase (ns): solve, surface charges,
+                             // numeric near field, analytic intra, inter LS, gradient DTA, total
 };
 
 enum {
@@ -85,6 +93,7 @@ enum {
   PBSAM_STATUS_OVERLAP = 1,
   PBSAM_STATUS_NOT_CONVERGED = 2,
   PBSAM_STATUS_NAN = 3,
+  PBSAM_STATUS_WAIT_EXPIRED = 4,
 };
 
 struct Ctx {

@@ -59,6 +59,9 @@ SIGNATURES = {
     "pbsam_system_stats": (ctypes.c_int, [_P, _IP]),
     "pbsam_system_set_stream": (ctypes.c_int, [_P, _P]),
     "pbsam_system_last_kernel_ms": (ctypes.c_int, [_P, _DP]),
+    "pbsam_system_phase_ms": (ctypes.c_int, [_P, _DP]),
+    "pbsam_imat_build": (ctypes.c_int, [_P, ctypes.c_int, _DP, _DP, ctypes.c_int, _DP]),
+    "pbsam_selfpol": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _IP]),
     "pbsam_last_error": (ctypes.c_char_p, []),
 }
 
@@ -134,6 +137,26 @@ class CSystem:
         self.types.append(t.value)
         return t.value
 
+    def build_imats(self, centres, radii, n_points=250000):
+        """IMats of a molecule's spheres (the reference's `pbsam mat`): [n_sph, p^2, p^2] column-major."""
+        centres = np.ascontiguousarray(centres, dtype=np.float64)
+        radii = np.ascontiguousarray(radii, dtype=np.float64)
+        P2 = self.params.poles ** 2
+        out = np.zeros((len(radii), P2 * P2))
+        _check(lib().pbsam_imat_build(self.handle, len(radii), _dptr(centres), _dptr(radii), n_points, _dptr(out)))
+        return out
+
+    def self_polarize(self, type_id, max_rounds=1700):
+        """Self-polarized (F, H, H scale, sweeps) of a type, rounded as the reference's .exp files."""
+        ns, _ = self.moltype_info(type_id)
+        P2 = self.params.poles ** 2
+        F = np.zeros((ns, P2))
+        H = np.zeros((ns, P2))
+        sc = np.zeros(ns)
+        r = ctypes.c_int()
+        _check(lib().pbsam_selfpol(self.handle, type_id, max_rounds, _dptr(F), _dptr(H), _dptr(sc), ctypes.byref(r)))
+        return F, H, sc, r.value
+
     def moltype_info(self, t):
         ns, npts = ctypes.c_int(), ctypes.c_int()
         _check(lib().pbsam_moltype_info(self.handle, t, ctypes.byref(ns), ctypes.byref(npts)))
@@ -191,6 +214,13 @@ class Molecules:
         s = np.zeros((self.n_systems, 8), dtype=np.int32)
         _check(lib().pbsam_system_stats(self.handle, s.ctypes.data_as(_IP)))
         return s
+
+    def phase_ms(self):
+        """Device ms per phase of the last evaluation: solve, surface charges, numeric,
+        analytic intra, inter LS, gradient DTA, total."""
+        m = np.zeros((self.n_systems, 8))
+        _check(lib().pbsam_system_phase_ms(self.handle, _dptr(m)))
+        return m
 
     def set_stream(self, stream_handle):
         _check(lib().pbsam_system_set_stream(self.handle, ctypes.c_void_p(stream_handle)))

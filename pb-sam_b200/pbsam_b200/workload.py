@@ -1,0 +1,131 @@
+"""Synthetic workloads with the shapes of the benchmark configurations.
+
+Configuration "pose sweep, p = 30": two molecules of 60 dielectric spheres
+(radii U(3,8) A, overlaps 0.5-1.5 A), 2000 charges U(-0.8,0.8) shifted to net
++4 / -4, eps_in 4, eps_out 78, 0.05 M, 298.15 K, pole order 30, inter-molecular
+polarization cutoff 10 A; molecule B placed at centre distances 30, 32, ..., 80 A
+from molecule A along a random axis with random orientations (26 poses).  A
+distance at which two spheres would overlap is raised to the first distance
+with a 1 A minimum surface gap (the reference cannot evaluate overlapping
+poses), so every pose is a valid force evaluation.
+
+Inputs are prepared on the GPU like the reference's `pbsam mat` and `pbsam spol`
+(250 000 quadrature points per sphere) and written in the reference's file
+formats when a directory is given, so the reference binaries can read them.
+"""
+import os
+import struct
+
+import numpy as np
+
+from . import synth
+
+SWEEP_P30 = dict(n_sph=60, r=(3.0, 8.0), n_q=2000, q_amp=0.8, nets=(4.0, -4.0), poles=30, salt=0.05,
+                 idiel=4.0, dists=[30.0 + 2 * k for k in range(26)], min_gap=1.0, seeds=(2101, 2102),
+                 pose_seed=2103)
+SWEEP_P10 = dict(n_sph=8, r=(3.0, 6.0), n_q=300, q_amp=0.6, nets=(2.0, -2.0), poles=10, salt=0.05,
+                 idiel=4.0, dists=[20.0 + 2 * k for k in range(11)], min_gap=1.0, seeds=(1, 2), pose_seed=7)
+
+
+def molecules(cfg):
+    return [synth.make_molecule(cfg["n_sph"], cfg["r"][0], cfg["r"][1], cfg["n_q"], cfg["q_amp"], net, seed=s)
+            for net, s in zip(cfg["nets"], cfg["seeds"])]
+
+
+def poses(cfg, mols, rank=0):
+    """[n_pose, 2, 3] positions and [n_pose, 2, 4] quaternions (molecule A at the origin)."""
+    rng = np.random.default_rng(cfg["pose_seed"] + 7919 * rank)
+    a = (mols[0].centres, mols[0].radii)
+    b = (mols[1].centres, mols[1].radii)
+    pos, quat, dist = [], [], []
+    for d in cfg["dists"]:
+        qa, qb, ax = synth.random_quat(rng), synth.random_quat(rng), synth.random_axis(rng)
+        dd = d
+        if synth.min_gap(a, np.zeros(3), qa, b, d * ax, qb) < cfg["min_gap"]:
+            dd = synth.place_at_gap(a, qa, b, qb, ax, cfg["min_gap"])
+        pos.append([[0.0, 0.0, 0.0], list(dd * ax)])
+        quat.append([list(qa), list(qb)])
+        dist.append(dd)
+    return np.array(pos), np.array(quat), np.array(dist)
+
+
+def _pqr_round(mol):
+    """Coordinates and charges as they read back from the PQR text (what the reference sees)."""
+    import tempfile
+    with tempfile.NamedTemporaryFile("w", suffix=".pqr", delete=False) as fh:
+        path = fh.name
+    synth.write_pqr(mol, path)
+    out = synth.read_pqr(path)
+    os.remove(path)
+    return out
+
+
+def write_imat(path, imat, poles):
+    with open(path, "wb") as fh:
+        fh.write(struct.pack("i", poles))
+        fh.write(np.ascontiguousarray(imat, dtype=np.float64).tobytes())
+
+
+def _fmt8(x):
+    return "0" if abs(x) < 1e-15 else "%.8g" % x
+
+
+def write_exp(path, coeffs, poles, scale):
+    """Expansion text file as src/readutil.cpp:541-556 writes it."""
+    with open(path, "w") as fh:
+        fh.write("%d\n%s\n1000\n" % (poles, _fmt8(scale)))
+        for n in range(poles):
+            fh.write(" ".join(_fmt8(v) for v in coeffs[n * n:(n + 1) * (n + 1)]) + " \n")
+        fh.write("\n")
+
+
+def prepare(cfg, device=0, outdir=None, log=print):
+    """Build IMats and self-polarized expansions on the GPU; returns
+    (moltype specs for CSystem.create_moltype, prep timings, file specs or None)."""
+    import time
+    import pbsam_b200 as pb
+    mols = molecules(cfg)
+    specs, files, tm = [], [], {}
+    prep = pb.CSystem(poles=cfg["poles"], salt=cfg["salt"], idiel=cfg["idiel"], device=device)
+    types = []
+    imats_all = []
+    for k, m in enumerate(mols):
+        cen, rad, pos, q = _pqr_round(m)
+        t0 = time.time()
+        im = prep.build_imats(cen, rad)
+        tm["imat_s_%d" % k] = time.time() - t0
+        imats_all.append(im)
+        ns = len(rad)
+        P2 = cfg["poles"] ** 2
+        types.append(prep.create_moltype(cen, rad, pos, q, im, np.zeros((ns, P2)), np.zeros((ns, P2)), 1.0 / rad))
+        specs.append(dict(centres=cen, radii=rad, chg_pos=pos, chg=q, imats=im))
+    for k, t in enumerate(types):
+        t0 = time.time()
+        F, H, sc, rounds = prep.self_polarize(t)
+        tm["selfpol_s_%d" % k] = time.time() - t0
+        tm["selfpol_rounds_%d" % k] = rounds
+        specs[k].update(fself=F, hself=H, hself_scale=sc)
+    prep.close()
+    if outdir:
+        for k, (m, sp) in enumerate(zip(mols, specs)):
+            tag = "AB"[k]
+            os.makedirs(os.path.join(outdir, "im" + tag), exist_ok=True)
+            os.makedirs(os.path.join(outdir, "exp" + tag), exist_ok=True)
+            synth.write_pqr(m, os.path.join(outdir, "mol%s.pqr" % tag))
+            for i in range(len(sp["radii"])):
+                write_imat(os.path.join(outdir, "im" + tag, "imat.sp%d.out.bin" % i), sp["imats"][i], cfg["poles"])
+                write_exp(os.path.join(outdir, "exp" + tag, "mol%s.0.%d.F.exp" % (tag, i)), sp["fself"][i],
+                          cfg["poles"], sp["hself_scale"][i])
+                write_exp(os.path.join(outdir, "exp" + tag, "mol%s.0.%d.H.exp" % (tag, i)), sp["hself"][i],
+                          cfg["poles"], sp["hself_scale"][i])
+            files.append((os.path.join(outdir, "mol%s.pqr" % tag), os.path.join(outdir, "im" + tag),
+                          os.path.join(outdir, "exp" + tag), "mol%s.0" % tag))
+    return specs, tm, (files if outdir else None)
+
+
+def open_context(cfg, specs, device=0, **kw):
+    import pbsam_b200 as pb
+    ctx = pb.CSystem(poles=cfg["poles"], salt=cfg["salt"], idiel=cfg["idiel"], device=device, **kw)
+    types = [ctx.create_moltype(sp["centres"], sp["radii"], sp["chg_pos"], sp["chg"], sp["imats"], sp["fself"],
+                                sp["hself"], sp["hself_scale"]) for sp in specs]
+    return ctx, types
