@@ -7,15 +7,16 @@ centre distances 30, 32, ..., 80 A (raised to a 1 A minimum gap where spheres
 would overlap), random orientations; every pose is an independent system and one
 step evaluates CMolecule::computeForces for all 26 of them (mutual polarization,
 gradient solves, forces and torques).  Inputs (IMats, self-polarized F/H) are
-prepared on the GPU before timing, exactly like the reference's `pbsam mat` and
+prepared on the GPU before timing, like the reference's `pbsam mat` and
 `pbsam spol`.  The IMats (120 x 6.5 MB) exceed L2, so no flush is needed.
 
 Multi-GPU: one process per GPU (torchrun), each rank solves its own batch of 26
 poses (weak scaling, no data-path collective); rank 0 prints the max-over-ranks
 device time.  --impl reference times the reference's own CPU implementation
-(oracle/_ref, compiled from the reference sources) on the same workload.
+(oracle/_ref, compiled from the reference sources) on the same poses.
 """
 import argparse
+import datetime
 import json
 import os
 import subprocess
@@ -31,22 +32,26 @@ sys.path.insert(0, os.path.join(REPO, "oracle"))
 
 METRIC = "pol. solves/s (computeForces calls per second), pose sweep p=30"
 UNIT = "solves/s"
+WORKLOAD = ("pose sweep p=30: 2 molecules x 60 spheres (r 3-8 A), 2000 charges (net +4/-4), "
+            "26 centre distances 30-80 A, eps 4/78, 0.05 M, 298.15 K")
 
 
 def measured_peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return d.get("hbm_gbs", 6650.0), "measured"
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
     return 6650.0, "fallback"
 
 
 class ClockSampler:
-    """nvidia-smi clocks during the timed region."""
+    """nvidia-smi SM clocks and throttle reasons of one GPU during the timed region."""
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, gpu):
-        self.gpu = gpu
-        self.path = tempfile.mktemp(suffix=".csv")
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
         self.proc = None
 
     def __enter__(self):
@@ -54,7 +59,7 @@ class ClockSampler:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu_id), "--query-gpu=" + q,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
@@ -68,7 +73,6 @@ class ClockSampler:
 
     def summary(self):
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         try:
             for ln in open(self.path):
                 f = [x.strip() for x in ln.split(",")]
@@ -79,19 +83,43 @@ class ClockSampler:
                     mx = float(f[2])
                 except ValueError:
                     continue
-                for n, v in zip(names, f[5:9]):
+                for n, v in zip(self.NAMES, f[5:9]):
                     if v.lower().startswith("active"):
                         reasons.add(n)
         except OSError:
             pass
+        os.remove(self.path)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
                 "samples": len(sm)}
 
 
+def gpu_id_for_smi(local):
+    import torch
+    try:
+        u = str(torch.cuda.get_device_properties(local).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return str(local)
+
+
+def measured_traffic_per_inner_iteration():
+    """DRAM bytes (read + write) per inner F/H iteration of the force kernel, from
+    the ncu capture summarised in profiles/ (a small case of the same kernel;
+    traffic grows with the inner iterations, which dominate it)."""
+    p = os.path.join(REPO, "profiles", "pbsam_forces_kernel_p30_traffic.txt")
+    if os.path.exists(p):
+        for ln in open(p):
+            t = ln.split()
+            if len(t) == 2 and t[0] == "dram_bytes_per_inner_iteration":
+                return float(t[1])
+    return None
+
+
 def algorithmic_bytes(stats, poles):
-    """IMat bytes the solve must stream: two applications per inner F/H iteration
-    (8 p^4 bytes each; the three gradient components share one read)."""
-    return float(np.sum(stats[:, 1])) * 2 * 8 * poles ** 4
+    """IMat bytes the solve must stream: every inner F/H iteration applies the
+    p^2 x p^2 FP64 IMat twice (8 p^4 bytes each; D = 3 gradient solves share one
+    read of the matrix across their three operands)."""
+    return float(np.sum(stats[:, 1])) * 2 * 8 * float(poles) ** 4
 
 
 def run_ours(args):
@@ -100,16 +128,18 @@ def run_ours(args):
     from pbsam_b200 import replicas, workload
     rank, world, local = replicas.rank_env()
     if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     torch.cuda.set_device(local)
     cfg = dict(workload.SWEEP_P30)
     t0 = time.time()
     specs, prep_t, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds)
     ctx, types = workload.open_context(cfg, specs, device=local)
     mols = workload.molecules(cfg)
-    pos, quat, dist_ = workload.poses(cfg, mols, rank=rank)
-    B = len(dist_)
+    pos, quat, _ = workload.poses(cfg, mols, rank=rank)
+    B = len(pos)
     sysb = ctx.molecules(types, n_systems=B)
+    stream = torch.cuda.current_stream()
+    sysb.set_stream(stream.cuda_stream)
     prep_s = time.time() - t0
     # device-resident inputs for the kernel-only rate
     dpos = torch.tensor(pos, dtype=torch.float64, device="cuda")
@@ -128,40 +158,44 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    kernel_ms = []
-    with ClockSampler(local) as clk:
+    with ClockSampler(gpu_id_for_smi(local)) as clk:
         torch.cuda.synchronize()
-        e0.record()
+        e0.record(stream)
         for _ in range(args.steps):
             step_device()
-        e1.record()
+        e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    clocks = clk.summary()
     if world > 1:
         dist.barrier()
     ms_max = replicas.max_over_ranks(ms, dist if world > 1 else None)
     status = dS.cpu().numpy()
     stats = sysb.stats()
     phases = sysb.phase_ms()
-    # e2e: through the C ABI with host buffers (H2D poses, D2H forces/torques/status) each step
+    # e2e: the public API with host buffers; H2D of the poses and D2H of forces,
+    # torques and status inside the timed region, every step
     hp, hq = np.ascontiguousarray(pos), np.ascontiguousarray(quat)
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
-    t1 = time.time()
+    ee0.record(stream)
     for _ in range(args.steps):
         sysb.set_poses(hp, hq)
         f, t, st = sysb.compute_forces()
+    ee1.record(stream)
     torch.cuda.synchronize()
-    e2e_s = time.time() - t1
-    e2e_max = replicas.max_over_ranks(e2e_s, dist if world > 1 else None)
-    # one launch timed alone for the roofline
-    sysb.set_poses_device(dpos.data_ptr(), dquat.data_ptr())
-    sysb.compute_forces_device(dF.data_ptr(), dT.data_ptr(), dS.data_ptr())
-    torch.cuda.synchronize()
-    one_ms = sysb.last_kernel_ms()
-    launch_stats = sysb.stats()
+    e2e_ms = ee0.elapsed_time(ee1)
+    e2e_max = replicas.max_over_ranks(e2e_ms, dist if world > 1 else None)
+    # roofline of the (only) kernel of a step: its algorithmic IMat bytes over its
+    # average duration inside the timed region
     peak, peak_kind = measured_peaks()
-    nbytes = algorithmic_bytes(launch_stats, cfg["poles"])
-    achieved = nbytes / (one_ms * 1e-3) / 1e9
+    launch_ms = ms / args.steps
+    nbytes = algorithmic_bytes(stats, cfg["poles"])
+    achieved = nbytes / (launch_ms * 1e-3) / 1e9
+    traffic = args.traffic_per_launch
+    per_it = measured_traffic_per_inner_iteration()
+    if traffic is None and per_it is not None:
+        traffic = per_it * float(np.sum(stats[:, 1]))
     out = None
     if rank == 0:
         units = B * world * args.steps
@@ -170,27 +204,28 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator; IMats and self-polarized expansions built on the GPU)",
-            "config": {"workload": "pose sweep p=30: 2 molecules x 60 spheres (r 3-8 A), 2000 charges, "
-                                   "26 centre distances 30-80 A, 0.05 M, eps 4/78",
-                       "poles": cfg["poles"], "systems_per_gpu": B, "spheres_per_system": 120,
-                       "parallelism": "replicas: %d ranks x %d independent systems" % (world, B),
-                       "l2": "inputs larger than L2 (120 IMats x 6.5 MB), no flush"},
-            "e2e": {"value": units / e2e_max, "unit": UNIT,
+            "config": {"workload": WORKLOAD, "poles": cfg["poles"], "systems_per_gpu": B,
+                       "spheres_per_system": 2 * cfg["n_sph"],
+                       "parallelism": "replicas: %d rank(s) x %d independent systems" % (world, B),
+                       "l2": "no flush: inputs larger than L2 (120 IMats x 6.5 MB = 778 MB)"},
+            "e2e": {"value": units / (e2e_max * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": int(hp.nbytes + hq.nbytes),
-                    "d2h_bytes_per_step": int(2 * f.nbytes + st.nbytes)},
+                    "d2h_bytes_per_step": int(f.nbytes + t.nbytes + st.nbytes)},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "pbsam_forces_kernel", "launch_ms": one_ms,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": peak_kind, "kernel": "pbsam_forces_kernel", "launch_ms": launch_ms,
                          "algorithmic_bytes_per_launch": nbytes},
-            "clocks": clk.summary(),
-            "status_ok": int(np.sum(status == 0)),
+            "clocks": clocks,
+            "systems_ok": int(np.sum(status == 0)),
             "inner_iterations_per_step": int(np.sum(stats[:, 1])),
-            "phase_ms_max_system": [round(float(x), 1) for x in phases[np.argmax(phases[:, 6])][:7]],
+            "slowest_system_phase_ms": dict(zip(
+                ["solve", "surface", "numeric", "intra", "LS", "DTA", "grad_reexp", "total"],
+                [round(float(x), 1) for x in phases[int(np.argmax(phases[:, 7]))]])),
             "prep_s": round(prep_s, 1), "prep": prep_t,
         }
         if args.cpu_baseline:
-            out["cpu_baseline"] = cpu_baseline(cfg, specs, pos, quat, args)
+            out["cpu_baseline"] = cpu_baseline(cfg, specs, pos, quat, stats, args)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -199,85 +234,96 @@ def run_ours(args):
     return out
 
 
+# ---------------------------------------------------------------- reference CPU leg
 def _ref_harness(poles):
     return os.path.join(REPO, "oracle", "_ref", "p%d_fast" % poles, "harness")
 
 
-def _write_inputs(cfg, specs, outdir):
-    from pbsam_b200 import workload
-    mols = workload.molecules(cfg)
-    files = []
-    for k, (m, sp) in enumerate(zip(mols, specs)):
-        tag = "AB"[k]
-        for sub in ("im" + tag, "exp" + tag):
-            os.makedirs(os.path.join(outdir, sub), exist_ok=True)
-        workload.synth.write_pqr(m, os.path.join(outdir, "mol%s.pqr" % tag))
-        for i in range(len(sp["radii"])):
-            workload.write_imat(os.path.join(outdir, "im" + tag, "imat.sp%d.out.bin" % i), sp["imats"][i], cfg["poles"])
-            workload.write_exp(os.path.join(outdir, "exp" + tag, "mol%s.0.%d.F.exp" % (tag, i)), sp["fself"][i],
-                               cfg["poles"], sp["hself_scale"][i])
-            workload.write_exp(os.path.join(outdir, "exp" + tag, "mol%s.0.%d.H.exp" % (tag, i)), sp["hself"][i],
-                               cfg["poles"], sp["hself_scale"][i])
-        files.append((os.path.join(outdir, "mol%s.pqr" % tag), os.path.join(outdir, "im" + tag),
-                      os.path.join(outdir, "exp" + tag), "mol%s.0" % tag))
-    return files
+def _pose_spec(path, cfg, files, pos, quat):
+    with open(path, "w") as fh:
+        fh.write("salt %r\nidiel %r\ndump 0\nenergy 0\n" % (cfg["salt"], cfg["idiel"]))
+        for fl in files:
+            fh.write("moltype %s %s %s %s\n" % fl)
+        fh.write("frame\n")
+        for m in range(len(pos)):
+            fh.write("mol %d %s %s\n" % (m, " ".join("%.17g" % v for v in pos[m]),
+                                         " ".join("%.17g" % v for v in quat[m])))
 
 
-def _run_poses(files, cfg, pos, quat, idx, budget_s, ncores, outdir):
-    """Run the reference harness on poses idx (one fresh process per pose, ncores at a
-    time) until budget_s; returns (completed poses, elapsed s)."""
+def _sample_poses(its, ncores, max_its):
+    """Poses of the bounded CPU sample: up to ncores poses whose inner-iteration
+    count is at most max_its, spread over that range (one process per core)."""
+    order = [int(i) for i in np.argsort(its, kind="stable") if its[i] <= max_its]
+    if len(order) <= ncores:
+        return order
+    pick = np.linspace(0, len(order) - 1, ncores).round().astype(int)
+    return sorted(set(order[k] for k in pick))
+
+
+def run_reference_sample(cfg, files, pos, quat, idx, limit_s, workdir):
+    """Runs the reference harness on poses idx concurrently (one single-threaded
+    process per pose); returns {pose: computeForces seconds (the harness' timer)}."""
     import oracle
-    procs, done, t0, k = [], 0, time.time(), 0
-    while True:
-        while len(procs) < ncores and k < len(idx) and time.time() - t0 < budget_s:
-            j = idx[k]
-            spec = os.path.join(outdir, "spec%d.txt" % k)
-            with open(spec, "w") as fh:
-                fh.write("salt %r\nidiel %r\ndump 0\nenergy 0\n" % (cfg["salt"], cfg["idiel"]))
-                for f in files:
-                    fh.write("moltype %s %s %s %s\n" % f)
-                fh.write("frame\n")
-                for m in range(2):
-                    fh.write("mol %d %s %s\n" % (m, " ".join("%.17g" % v for v in pos[j][m]),
-                                                 " ".join("%.17g" % v for v in quat[j][m])))
-            env = dict(os.environ, OMP_NUM_THREADS="1")
-            procs.append(subprocess.Popen([_ref_harness(cfg["poles"]), spec, spec + ".out"], env=env,
-                                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
-            k += 1
-        if not procs:
-            break
-        time.sleep(0.2)
-        still = []
-        for p in procs:
-            if p.poll() is None:
-                if time.time() - t0 > budget_s * 4:
-                    p.kill()
-                    p.wait()
-                else:
-                    still.append(p)
-            elif p.returncode == 0:
-                done += 1
-        procs = still
-        if k >= len(idx) and not procs:
-            break
-    _ = oracle
-    return done, time.time() - t0
+    procs = []
+    for j in idx:
+        spec = os.path.join(workdir, "pose%d.txt" % j)
+        _pose_spec(spec, cfg, files, pos[j], quat[j])
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        procs.append((j, spec, subprocess.Popen([_ref_harness(cfg["poles"]), spec, spec + ".out"], env=env,
+                                                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)))
+    t0 = time.time()
+    out = {}
+    for j, spec, p in procs:
+        try:
+            p.wait(timeout=max(1.0, limit_s - (time.time() - t0)))
+        except subprocess.TimeoutExpired:
+            p.kill()
+            p.wait()
+            continue
+        if p.returncode == 0:
+            fr = oracle.parse(spec + ".out")
+            if fr and fr[0]["ok"]:
+                out[j] = float(fr[0]["info"][0])
+    return out
 
 
-def cpu_baseline(cfg, specs, pos, quat, args):
-    """The reference (compiled from its sources with its Makefile flags and a plain cblas
-    stand-in for MKL) on a bounded sample of the same poses, one single-threaded process
-    per pose (its OpenMP path races) on all host cores."""
+def reference_rate(times, its, n_cores):
+    """Whole-job rate of the reference on n_cores for all poses, from the sample:
+    per-pose time modelled as a + b * inner iterations (least squares over the
+    sample; the counts are the GPU solve's, which follows the same iteration), the
+    single-threaded solves packed on the cores: T = max(sum t / cores, max t)."""
+    js = sorted(times)
+    x = np.array([its[j] for j in js], dtype=float)
+    y = np.array([times[j] for j in js])
+    if len(js) >= 2 and np.ptp(x) > 0:
+        b, a = np.polyfit(x, y, 1)
+        a = max(a, 0.0)
+    else:
+        a, b = 0.0, float(np.sum(y) / max(np.sum(x), 1.0))
+    t_all = a + b * np.asarray(its, dtype=float)
+    T = max(float(np.sum(t_all)) / n_cores, float(np.max(t_all)))
+    return len(its) / T, dict(a_s=round(float(a), 4), b_ms_per_inner_iteration=round(float(b) * 1e3, 4),
+                              est_total_cpu_s=round(float(np.sum(t_all)), 1), est_makespan_s=round(T, 1))
+
+
+def cpu_baseline(cfg, specs, pos, quat, stats, args):
+    from pbsam_b200 import workload
     if not os.path.exists(_ref_harness(cfg["poles"])):
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "reference binary not built"}
     ncores = os.cpu_count() or 1
+    its = stats[:, 1]
     with tempfile.TemporaryDirectory() as td:
-        files = _write_inputs(cfg, specs, td)
-        order = list(range(len(pos)))[::-1]          # sweep from the far end (cheapest poses first)
-        done, el = _run_poses(files, cfg, pos, quat, order, args.cpu_budget, ncores, td)
-    return {"value": done / el if el > 0 else None, "unit": UNIT, "cores": min(ncores, len(pos)), "kind": "reference",
-            "sample": "%d poses completed in %.0f s (budget %d s), far end of the sweep first, 1 thread per pose"
-                      % (done, el, args.cpu_budget)}
+        files = workload.write_inputs(cfg, specs, td)
+        idx = _sample_poses(its, ncores, args.cpu_sample_its)
+        times = run_reference_sample(cfg, files, pos, quat, idx, args.cpu_limit, td)
+    if not times:
+        return {"value": None, "unit": UNIT, "cores": ncores, "kind": "reference", "sample": "no pose finished"}
+    rate, model = reference_rate(times, its, ncores)
+    return {"value": rate, "unit": UNIT, "cores": ncores, "kind": "reference",
+            "sample": "%d poses (inner iterations %s) run concurrently, 1 thread each, computeForces timed by the "
+                      "reference harness (max %.1f s); whole sweep extrapolated per inner iteration" % (
+                          len(times), sorted(int(its[j]) for j in times), max(times.values())),
+            "model": model}
 
 
 def run_reference(args):
@@ -288,24 +334,41 @@ def run_reference(args):
     cfg = dict(workload.SWEEP_P30)
     if not os.path.exists(_ref_harness(cfg["poles"])):
         return {"impl": "reference", "unavailable": "reference binary oracle/_ref/p30_fast/harness not built"}
+    import torch
+    torch.cuda.set_device(local)
+    # inputs and the per-pose iteration counts come from the GPU preparation; the
+    # timed work is the reference's own computeForces on the host cores
     specs, _, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds)
+    ctx, types = workload.open_context(cfg, specs, device=local)
     mols = workload.molecules(cfg)
     pos, quat, _ = workload.poses(cfg, mols)
+    sysb = ctx.molecules(types, n_systems=len(pos))
+    sysb.set_poses(pos, quat)
+    sysb.compute_forces()
+    stats = sysb.stats()
+    sysb.close()
+    ctx.close()
     ncores = os.cpu_count() or 1
-    vals = []
+    its = stats[:, 1]
+    vals, samples = [], []
     with tempfile.TemporaryDirectory() as td:
-        files = _write_inputs(cfg, specs, td)
-        order = list(range(len(pos)))[::-1]
+        files = workload.write_inputs(cfg, specs, td)
+        idx = _sample_poses(its, ncores, args.cpu_sample_its)
         for s in range(args.warmup + args.steps):
-            done, el = _run_poses(files, cfg, pos, quat, order, args.cpu_budget, ncores, td)
-            if s >= args.warmup:
-                vals.append(done / el)
+            times = run_reference_sample(cfg, files, pos, quat, idx, args.cpu_limit, td)
+            if s >= args.warmup and times:
+                v, model = reference_rate(times, its, ncores)
+                vals.append(v)
+                samples.append(model)
+    if not vals:
+        return {"impl": "reference", "unavailable": "no reference pose finished within %d s" % args.cpu_limit}
     v = float(np.mean(vals))
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic", "config": {"workload": "pose sweep p=30 (same poses)"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": min(ncores, len(pos)), "kind": "reference",
-                             "sample": "poses from the far end of the sweep, %d s per step" % args.cpu_budget},
+            "warmup": args.warmup, "ms_per_step": 1e3 * len(pos) / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": WORKLOAD},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores, "kind": "reference",
+                             "sample": "%d poses per step run concurrently, 1 thread each; whole sweep extrapolated "
+                                       "per inner iteration" % len(idx), "model": samples[-1]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -317,7 +380,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--selfpol-rounds", type=int, default=1700)
     ap.add_argument("--cpu-baseline", type=int, default=1)
-    ap.add_argument("--cpu-budget", type=int, default=30)
+    ap.add_argument("--cpu-sample-its", type=int, default=6000,
+                    help="largest inner-iteration count of a pose in the CPU sample")
+    ap.add_argument("--cpu-limit", type=int, default=60, help="seconds before a sample pose is abandoned")
+    ap.add_argument("--traffic-per-launch", type=float, default=None,
+                    help="DRAM bytes per launch measured by ncu (scaled from a small capture)")
     args = ap.parse_args()
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out is not None:

@@ -33,7 +33,6 @@ extern "C" {
 #define PBSAM_SYS_OK 0
 #define PBSAM_SYS_OVERLAP 1   /* two spheres of different molecules overlap
                                  (computeForces returns false, src/molecule.cpp:1090-1097) */
-#define PBSAM_SYS_WAIT_EXPIRED 4 /* a bounded device wait expired; results of the system are void */
 
 typedef struct pbsam_params {
   int poles;              /* pole order p (the reference's N_POLES, src/expansion.h:5-9) */
@@ -118,7 +117,9 @@ int pbsam_system_set_stream(pbsam_system *sys, void *stream);
 /* Device time per phase of the last force evaluation (or self-polarization), 8
  * doubles per system in ms: [0] F/H solves, [1] surface charges, [2] numeric
  * near-field re-expansions, [3] analytic intra re-expansions, [4] inter-molecular
- * LS re-expansions, [5] gradient re-expansions of H (DTA), [6] whole evaluation. */
+ * LS re-expansions, [5] gradient re-expansions of H (DTA), [6] re-expansions of
+ * the gradient solves (inter and intra, before each gradient F/H solve), [7] whole
+ * evaluation.  [0]-[6] do not overlap; [7] includes everything. */
 int pbsam_system_phase_ms(const pbsam_system *sys, double *ms);
 
 /* Device time in milliseconds of the last force-kernel launch (CUDA events). */

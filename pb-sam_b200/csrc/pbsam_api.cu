@@ -477,8 +477,9 @@ static int finalize_types(pbsam_context *c)
       for (int k = 0; k < t.ns; k++) {
         const double *src = t.imat.data() + (size_t)k * NP2 * NP2;
         double *dst = imat.data() + base + (size_t)k * stride;
+        const long ld = imat_ld((int)NP2);
         for (long r = 0; r < NP2; r++)
-          for (long cc = 0; cc < NP2; cc++) dst[r * NP2 + cc] = src[cc * NP2 + r];
+          for (long cc = 0; cc < NP2; cc++) dst[r * ld + cc] = src[cc * NP2 + r];
       }
     }
     chg_off.push_back(chg_off.back() + (int)t.chg.size());

@@ -13,25 +13,24 @@
 
 namespace pbsam {
 
-#define PBSAM_TEAM 256
-#define PBSAM_NCH 64            // max point chunks in a numeric expansion
+#define PBSAM_TEAM 512
 
 // ------------------------------------------------------------------ scratch
 struct Scr {
   int NP2;
+  int ld;                // row stride of the IMat and of the matvec operands (NP2 rounded up to even)
+  int tile_pts;          // points per numeric-expansion tile
   double *sh;            // (2NP)^2
   double2 *R, *dR;       // rotation coefficients
   double *TH, *dTH, *TF; // translation coefficients
   double *kbuf, *fact;   // 2NP+2, NP
   double *e;             // 16 * NP2
   double *g;             // 8 * 3 * NP2
-  double *part;          // PBSAM_NCH * 3 * NP2
   double *sol;           // 6 * 3 * NP2 (solver work)
   double *misc;          // 4096
   double2 *lvA, *lvB;    // shared memory: rotation recursion levels, (2NP-1)^2 each
-  double *stage;         // shared memory (aliases the levels): IMat row stages
-  unsigned long long *bars;  // shared memory: one mbarrier per stage
-  double *xs;            // shared memory: matvec operand, 3 * NP2
+  double *tile;          // shared memory (aliases the levels): numeric-expansion point tiles
+  double *xs;            // shared memory: matvec operands, 3 * ld
   __device__ double *E(int i) const { return e + (size_t)i * NP2; }
   __device__ double *G(int i) const { return g + (size_t)i * 3 * NP2; }
 };
@@ -48,52 +47,53 @@ __host__ __device__ inline long long scr_doubles(int NP, long long S)
   n += 2 * NP + 2 + NP + 8;     // kbuf, fact
   n += 16 * NP2;                // e
   n += 8 * 3 * NP2;             // g
-  n += (long long)PBSAM_NCH * 3 * NP2;   // part
   n += 6 * 3 * NP2;             // sol
   n += 4096 + S * S;            // misc + list building workspace
   return n;
 }
 
-// IMat streaming: NSTAGE shared-memory stages of rows_per_stage rows each
-#define PBSAM_NSTAGE 3
-#define PBSAM_STAGE_BYTES (56 * 1024)
-__host__ __device__ inline int rows_per_stage(int NP2)
+// IMat rows and matvec operands are stored with an even stride so that every row
+// starts on a 16-byte boundary (double2 loads); the pad column is zero.
+__host__ __device__ inline int imat_ld(int NP2) { return (NP2 + 1) & ~1; }
+// per-sphere stride of the row-major IMat store
+__host__ __device__ inline size_t imat_stride(int NP2) { return (size_t)NP2 * imat_ld(NP2); }
+
+// numeric-expansion tile: per point the P^2 harmonics, 2 x P radial factors,
+// 5 geometry words and 2 x 3 weights
+__host__ __device__ inline size_t tile_point_bytes(int NP) { return ((size_t)NP * NP + 2 * NP + 11) * sizeof(double); }
+__host__ __device__ inline size_t dyn_region_bytes(int NP)
 {
-  int rb = PBSAM_STAGE_BYTES / (NP2 * 8);
-  int cap = (NP2 + PBSAM_NSTAGE - 1) / PBSAM_NSTAGE;   // all stages together hold the whole matrix
-  cap = (cap + 1) & ~1;
-  if (rb > cap) rb = cap;
-  rb &= ~1;
-  return rb < 2 ? 2 : rb;
+  const size_t NN = 2 * NP - 1;
+  size_t lv = 2 * NN * NN * sizeof(double2);
+  size_t tp = (160 * 1024) / tile_point_bytes(NP);
+  if (tp > 32) tp = 32;
+  if (tp < 1) tp = 1;
+  const size_t tb = tp * tile_point_bytes(NP);
+  return ((lv > tb ? lv : tb) + 15) & ~(size_t)15;
 }
-// dynamic shared memory of every team kernel: [max(rotation levels, IMat stages)][operand x][mbarriers]
+// dynamic shared memory of every team kernel: [rotation levels | numeric tiles][matvec operands]
 __host__ __device__ inline size_t team_smem_bytes(int NP)
 {
-  const size_t NN = 2 * NP - 1, NP2 = (size_t)NP * NP;
-  size_t lv = 2 * NN * NN * sizeof(double2);
-  const size_t st = (size_t)PBSAM_NSTAGE * rows_per_stage((int)NP2) * NP2 * sizeof(double);
-  if (st > lv) lv = st;
-  return lv + 3 * NP2 * sizeof(double) + 64;
+  return dyn_region_bytes(NP) + 3 * (size_t)imat_ld(NP * NP) * sizeof(double) + 64;
 }
 
 __device__ Scr make_scr(double *base, int NP, void *smem)
 {
   Scr s;
-  {
-    const int NN = 2 * NP - 1, NP2 = NP * NP;
-    size_t lv = 2 * (size_t)NN * NN * sizeof(double2);
-    const size_t st = (size_t)PBSAM_NSTAGE * rows_per_stage(NP2) * NP2 * sizeof(double);
-    if (st > lv) lv = st;
-    s.lvA = (double2 *)smem;
-    s.lvB = s.lvA + NN * NN;
-    s.stage = (double *)smem;
-    s.xs = (double *)((char *)smem + lv);
-    s.bars = (unsigned long long *)((char *)smem + lv + 3 * (size_t)NP2 * sizeof(double));
-  }
   const int NP2 = NP * NP;
   const int NN = 2 * NP - 1;
+  {
+    const size_t lv = dyn_region_bytes(NP);
+    s.lvA = (double2 *)smem;
+    s.lvB = s.lvA + NN * NN;
+    s.tile = (double *)smem;
+    int tp = (int)(lv / tile_point_bytes(NP));
+    s.tile_pts = tp > 64 ? 64 : tp;
+    s.xs = (double *)((char *)smem + lv);
+  }
   const long long rotE = rot_off(NN), trE = tr_off(NN);
   s.NP2 = NP2;
+  s.ld = imat_ld(NP2);
   double *p = base;
   s.sh = p; p += 4 * NP * NP;
   s.R = (double2 *)p; p += 2 * rotE;
@@ -105,14 +105,13 @@ __device__ Scr make_scr(double *base, int NP, void *smem)
   s.fact = p; p += NP + 8;
   s.e = p; p += 16 * NP2;
   s.g = p; p += 8 * 3 * NP2;
-  s.part = p; p += (long long)PBSAM_NCH * 3 * NP2;
   s.sol = p; p += 6 * 3 * NP2;
   s.misc = p;
   return s;
 }
 
 // ------------------------------------------------------------------ phase timers
-enum { PH_SOLVE = 0, PH_SURF, PH_NUMERIC, PH_INTRA, PH_LS, PH_DTA, PH_TOTAL, PH_N };
+enum { PH_SOLVE = 0, PH_SURF, PH_NUMERIC, PH_INTRA, PH_LS, PH_DTA, PH_GRX, PH_TOTAL, PH_N };
 __device__ __forceinline__ unsigned long long gtimer()
 {
   unsigned long long t;
@@ -126,8 +125,6 @@ struct PhaseClock {
   __device__ void stop(const Team &tm, int ph) { if (tm.rank == 0 && acc) acc[ph] += (double)(gtimer() - t0); }
 };
 
-// per-sphere stride of the row-major IMat store (even, so every row block is 16-byte aligned)
-__host__ __device__ inline size_t imat_stride(int NP2) { return ((size_t)NP2 * NP2 + 1) & ~(size_t)1; }
 
 // ------------------------------------------------------------------ team helpers
 __device__ __forceinline__ void tcopy(const Team &tm, double *dst, const double *src, int n)
@@ -295,91 +292,174 @@ __device__ void pair_apply_grad(const Team &tm, const Tab &T, const Scr &sc, con
 // local: true = local expansion (k-hat radial part, e^{-kappa rho}/rho (a/rho)^n),
 // false = multipole ((rho/a)^n, unscreened).  out: NC expansions of NP2, P degrees
 // written, zero-padded to NP.
+//
+// Two weight sets over the same points (the F and H charges of one sphere) are
+// expanded together so the spherical harmonics are evaluated once per point.
+// The points stream through shared memory in tiles: one thread per (point, set)
+// builds the radial factors, one thread per (point, column pair) writes the point's
+// harmonics, then every thread adds the tile's points, in point order, into the
+// coefficients it owns (registers; coefficient c = rank + j * size).
+struct NumSet {
+  const double *w;    // weights (nullptr: set unused)
+  bool local, kappa;
+  int P;              // degrees
+  double *out;
+};
+#define PBSAM_NUM_CPT 2   // coefficients per thread: NP2 <= PBSAM_NUM_CPT * team size
+
+__device__ __forceinline__ void radial_factors(const Tab &T, double rho, double ch, bool local, bool kappa, int P,
+                                               double scale, double *rad)
+{
+  if (local) {
+    const double val = kappa ? rho * T.kappa : 0.0;
+    // k-hat_n (src/expansion.cpp:421-436) times e^{-val}/rho (scale/rho)^n
+    double km2 = 1.0, km1 = 1.0 + val;
+    const double vs = val * val;
+    double r = 1.0 / rho;
+    double k = ch * (r * (kappa ? exp(-val) : 1.0));
+    r *= scale;
+    for (int n = 0; n < P; n++) {
+      double kn;
+      if (n == 0) kn = 1.0;
+      else if (n == 1) kn = (val != 0.0) ? km1 : 1.0;
+      else {
+        kn = (val != 0.0) ? km1 + vs * km2 * T.C4[n] : 1.0;
+        km2 = km1; km1 = kn;
+      }
+      rad[n] = kn * k;
+      k *= r;
+    }
+  } else {
+    double k = ch;
+    const double r = rho * (1.0 / scale);
+    for (int n = 0; n < P; n++) { rad[n] = 1.0 * k; k *= r; }
+  }
+}
+
+template <int NC>
+__device__ void numeric_expand2(const Team &tm, const Tab &T, const Scr &sc, const double *pts, int N,
+                                const double *shift, double scale, NumSet A, NumSet B)
+{
+  const int NP = T.NP, NP2 = NP * NP;
+  const bool useB = B.w != nullptr;
+  const int P = (useB && B.P > A.P) ? B.P : A.P, P2 = P * P;
+  const int PA2 = A.P * A.P, PB2 = useB ? B.P * B.P : 0;
+  const int TP = sc.tile_pts;
+  double *Yt = sc.tile;                        // [TP][P2] harmonics
+  double *ra = Yt + (size_t)TP * P2;           // [TP][P]  radial factors, set A
+  double *rb = ra + (size_t)TP * P;            // [TP][P]  radial factors, set B
+  double *pg = rb + (size_t)TP * P;            // [TP][5]  cos t, sin t, phi, set A valid, set B valid
+  double *pw = pg + 5 * TP;                    // [TP][6]  weights A, B
+  double accA[PBSAM_NUM_CPT][NC], accB[PBSAM_NUM_CPT][NC];
+  int deg[PBSAM_NUM_CPT];
+#pragma unroll
+  for (int j = 0; j < PBSAM_NUM_CPT; j++) {
+    const int c = tm.rank + j * tm.size;
+    int n = (int)sqrt((double)c);
+    while (n * n > c) n--;
+    while ((n + 1) * (n + 1) <= c) n++;
+    deg[j] = n;
+#pragma unroll
+    for (int k = 0; k < NC; k++) { accA[j][k] = 0.0; accB[j][k] = 0.0; }
+  }
+  const int npair = (P + 1) / 2;
+  for (int h0 = 0; h0 < N; h0 += TP) {
+    const int nt = (N - h0 < TP) ? N - h0 : TP;
+    // per (point, set): weights, validity, radial factors; set A also the angles
+    for (int u = tm.rank; u < 2 * nt; u += tm.size) {
+      const int t = u >> 1, set = u & 1;
+      const NumSet &S = set ? B : A;
+      const int h = h0 + t;
+      bool ok = false;
+      double wv[NC];
+      if (!set || useB) {
+        if (NC == 1) {
+          wv[0] = S.w[h];
+          ok = wv[0] != 0.0;
+        } else {
+          wv[0] = S.w[3 * h]; wv[1] = S.w[3 * h + 1]; wv[2] = S.w[3 * h + 2];
+          ok = !(wv[0] * wv[0] + wv[1] * wv[1] + wv[2] * wv[2] < 1e-15);
+        }
+        for (int k = 0; k < NC; k++) pw[6 * t + 3 * set + k] = wv[k];
+      }
+      pg[5 * t + 3 + set] = ok ? 1.0 : 0.0;
+      const double dx = pts[3 * h] - shift[0], dy = pts[3 * h + 1] - shift[1], dz = pts[3 * h + 2] - shift[2];
+      const Sph s = cart2sph(dx, dy, dz);
+      if (set == 0) {
+        double st, ct;
+        sincos(s.theta, &st, &ct);
+        pg[5 * t] = ct; pg[5 * t + 1] = st; pg[5 * t + 2] = s.phi;
+      }
+      if (ok) radial_factors(T, s.rho, (NC == 1) ? wv[0] : 1.0, S.local, S.kappa, S.P, scale,
+                             (set ? rb : ra) + (size_t)t * P);
+    }
+    tm.sync();
+    for (int u = tm.rank; u < nt * npair; u += tm.size) {
+      const int t = u / npair, cp = u % npair;
+      if (pg[5 * t + 3] == 0.0 && pg[5 * t + 4] == 0.0) continue;
+      double *yt = Yt + (size_t)t * P2;
+      const double ct = pg[5 * t], st = pg[5 * t + 1], ph = pg[5 * t + 2];
+      const int m1 = cp, m2 = P - 1 - cp;
+      auto put = [&](int m) {
+        return [&, m](int n, double re, double im) {
+          if (m == 0) yt[IDX(n)] = re;
+          else { yt[IDX(n) + 2 * m - 1] = re; yt[IDX(n) + 2 * m] = im; }
+        };
+      };
+      sh_column(T, ct, st, ph, m1, P, put(m1));
+      if (m2 != m1) sh_column(T, ct, st, ph, m2, P, put(m2));
+    }
+    tm.sync();
+    for (int t = 0; t < nt; t++) {
+      const bool okA = pg[5 * t + 3] != 0.0, okB = pg[5 * t + 4] != 0.0;
+      if (!okA && !okB) continue;
+      const double *yt = Yt + (size_t)t * P2;
+#pragma unroll
+      for (int j = 0; j < PBSAM_NUM_CPT; j++) {
+        const int c = tm.rank + j * tm.size;
+        if (c < P2) {
+          const double yv = yt[c];
+          if (okA && c < PA2) {
+            const double v = yv * ra[(size_t)t * P + deg[j]];
+            if (NC == 1) accA[j][0] += v;
+            else {
+#pragma unroll
+              for (int k = 0; k < NC; k++) accA[j][k] += pw[6 * t + k] * v;
+            }
+          }
+          if (okB && c < PB2) {
+            const double v = yv * rb[(size_t)t * P + deg[j]];
+            if (NC == 1) accB[j][0] += v;
+            else {
+#pragma unroll
+              for (int k = 0; k < NC; k++) accB[j][k] += pw[6 * t + 3 + k] * v;
+            }
+          }
+        }
+      }
+    }
+    tm.sync();
+  }
+#pragma unroll
+  for (int j = 0; j < PBSAM_NUM_CPT; j++) {
+    const int c = tm.rank + j * tm.size;
+    if (c < NP2)
+#pragma unroll
+      for (int k = 0; k < NC; k++) {
+        A.out[(size_t)k * NP2 + c] = (c < PA2) ? accA[j][k] : 0.0;
+        if (useB) B.out[(size_t)k * NP2 + c] = (c < PB2) ? accB[j][k] : 0.0;
+      }
+  }
+  tm.sync();
+}
+
 template <int NC>
 __device__ void numeric_expand(const Team &tm, const Tab &T, const Scr &sc, const double *pts, int N,
                                const double *shift, const double *w, bool local, bool kappa, int P, double scale,
                                double *out)
 {
-  const int NP2 = T.NP * T.NP;
-  const int npair = (P + 1) / 2;
-  int C = tm.size / npair;
-  if (C > PBSAM_NCH) C = PBSAM_NCH;
-  if (C < 1) C = 1;
-  const int cp = tm.rank % npair, c = tm.rank / npair;
-  if (c < C) {
-    const int m1 = cp, m2 = P - 1 - cp;
-    const int n1 = P - m1;                      // degrees in column m1
-    double acc[NC][2 * 33 + 2];
-    for (int k = 0; k < NC; k++)
-      for (int i = 0; i < 2 * P + 2; i++) acc[k][i] = 0.0;
-    double rad[33];
-    for (int h = c; h < N; h += C) {
-      double wv[NC];
-      if (NC == 1) {
-        wv[0] = w[h];
-        if (wv[0] == 0.0) continue;
-      } else {
-        wv[0] = w[3 * h]; wv[1] = w[3 * h + 1]; wv[2] = w[3 * h + 2];
-        if (wv[0] * wv[0] + wv[1] * wv[1] + wv[2] * wv[2] < 1e-15) continue;
-      }
-      const double dx = pts[3 * h] - shift[0], dy = pts[3 * h + 1] - shift[1], dz = pts[3 * h + 2] - shift[2];
-      const Sph s = cart2sph(dx, dy, dz);
-      const double ch = (NC == 1) ? wv[0] : 1.0;
-      if (local) {
-        const double val = kappa ? s.rho * T.kappa : 0.0;
-        bessel_k(T, rad, P + 1, val);
-        double r = 1.0 / s.rho;
-        double k = ch * (r * (kappa ? exp(-val) : 1.0));
-        r *= scale;
-        for (int n = 0; n < P; n++) { rad[n] = rad[n] * k; k *= r; }
-      } else {
-        double k = ch;
-        const double r = s.rho * (1.0 / scale);
-        for (int n = 0; n < P; n++) { rad[n] = 1.0 * k; k *= r; }
-      }
-      double st, ct;
-      sincos(s.theta, &st, &ct);
-      auto body = [&](int base, int m0) {
-        return [&, base, m0](int n, double re, double im) {
-          const double rr = rad[n];
-          const int ix = base + 2 * (n - m0);
-          if (NC == 1) {
-            acc[0][ix] += re * rr;
-            acc[0][ix + 1] += im * rr;
-          } else {
-            const double vr = re * rr, vi = im * rr;
-            for (int k = 0; k < NC; k++) { acc[k][ix] += wv[k] * vr; acc[k][ix + 1] += wv[k] * vi; }
-          }
-        };
-      };
-      sh_column(T, ct, st, s.phi, m1, P, body(0, m1));
-      if (m2 != m1) sh_column(T, ct, st, s.phi, m2, P, body(2 * n1, m2));
-    }
-    // write this chunk's partials for the thread's columns
-    for (int k = 0; k < NC; k++) {
-      double *pp = sc.part + ((size_t)c * NC + k) * NP2;
-      for (int n = m1; n < P; n++) {
-        const int ix = 2 * (n - m1);
-        if (m1 == 0) pp[IDX(n)] = acc[k][ix];
-        else { pp[IDX(n) + 2 * m1 - 1] = acc[k][ix]; pp[IDX(n) + 2 * m1] = acc[k][ix + 1]; }
-      }
-      if (m2 != m1)
-        for (int n = m2; n < P; n++) {
-          const int ix = 2 * n1 + 2 * (n - m2);
-          if (m2 == 0) pp[IDX(n)] = acc[k][ix];
-          else { pp[IDX(n) + 2 * m2 - 1] = acc[k][ix]; pp[IDX(n) + 2 * m2] = acc[k][ix + 1]; }
-        }
-    }
-  }
-  tm.sync();
-  for (int i = tm.rank; i < NC * NP2; i += tm.size) {
-    const int k = i / NP2, j = i % NP2;
-    double v = 0.0;
-    if (j < P * P)
-      for (int cc = 0; cc < C; cc++) v += sc.part[((size_t)cc * NC + k) * NP2 + j];
-    out[(size_t)k * NP2 + j] = v;
-  }
-  tm.sync();
+  numeric_expand2<NC>(tm, T, sc, pts, N, shift, scale, NumSet{w, local, kappa, P, out},
+                      NumSet{nullptr, false, false, 0, nullptr});
 }
 
 // ------------------------------------------------------------------ surface charges
@@ -430,117 +510,88 @@ __device__ void surface_q(const Team &tm, const Tab &T, const double *pts, int N
 }
 
 // ------------------------------------------------------------------ IMat product
-// Y[d*NP2 + i] = scale[n(i)] * sum_k IMT[i][k] x[d*NP2 + k] for d < D (applyMMat,
+// Y[d*NP2 + i] = scale[n(i)] * sum_k IMT[i][k] x[d*ld + k] for d < D (applyMMat,
 // src/lautil.cpp:57-72, followed by revertF / revertH).  IMT is the IMat stored
-// row-major with 16-byte aligned rows of even count per stage; row blocks stream
-// from HBM into PBSAM_NSTAGE shared-memory stages with bulk asynchronous copies
-// completed on one mbarrier per stage, one warp per row reading the stage, the
-// D operands in shared memory.  Every wait is bounded: on expiry the team's error
-// flag is set and the result is abandoned.
-__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, int count)
-{
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_inval(unsigned long long *bar)
-{
-  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
-{
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity)
-{
-  for (long it = 0; it < (1L << 24); it++) {
-    unsigned ok;
-    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-                 : "=r"(ok)
-                 : "r"(smem_u32(bar)), "r"(parity)
-                 : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-
-__device__ void imat_apply(const Team &tm, const Scr &sc, const double *IMT, const double *x, int NP2, int D,
-                           double *Y, const double *scale, int *err)
+// row-major with an even row stride ld (zero pad column), x holds the D operands
+// in shared memory with the same stride (zero pad).  Each warp owns four rows at a
+// time and its lanes stride the rows with 16-byte read-only loads, two column
+// blocks per step, so 128 bytes per lane are in flight; the D operands share every
+// loaded IMat element.  The row sums are reduced across the warp in a fixed order.
+template <int D>
+__device__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const double *x, int NP2, double *Y,
+                             const double *scale)
 {
   const int lane = tm.rank & 31, warp = tm.rank >> 5, nw = tm.size >> 5;
-  const int RB = rows_per_stage(NP2);
-  const int nblk = (NP2 + RB - 1) / RB;
-  const bool async_ok = (NP2 % 2 == 0) && ((((unsigned long long)IMT) & 15ULL) == 0);
-  volatile int *fail = (volatile int *)(sc.bars + PBSAM_NSTAGE);
-  int issued = 0, done = 0;
-  if (async_ok) {
-    if (tm.rank == 0) {
-      *fail = 0;
-      for (int q = 0; q < PBSAM_NSTAGE; q++) mbar_init(&sc.bars[q], 1);
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  const int NV = ld >> 1;
+  const double2 *x2 = (const double2 *)x;
+  for (int r0 = warp * 4; r0 < NP2; r0 += nw * 4) {
+    const double2 *rp[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int r = (r0 + j < NP2) ? r0 + j : NP2 - 1;
+      rp[j] = (const double2 *)(IMT + (size_t)r * ld);
     }
-    tm.sync();
-    issued = nblk < PBSAM_NSTAGE ? nblk : PBSAM_NSTAGE;
-    if (tm.rank == 0)
-      for (int q = 0; q < issued; q++) {
-        const int r0 = q * RB, nr = (NP2 - r0 < RB) ? NP2 - r0 : RB;
-        bulk_load(sc.stage + (size_t)q * RB * NP2, IMT + (size_t)r0 * NP2, (unsigned)(nr * NP2 * 8), &sc.bars[q]);
-      }
-  }
-  for (int blk = 0; blk < nblk; blk++) {
-    const int q = blk % PBSAM_NSTAGE;
-    const int r0 = blk * RB, nr = (NP2 - r0 < RB) ? NP2 - r0 : RB;
-    const double *rows;
-    if (async_ok) {
-      if (!mbar_wait(&sc.bars[q], (unsigned)((blk / PBSAM_NSTAGE) & 1))) *fail = 1;
-      rows = sc.stage + (size_t)q * RB * NP2;
-    } else rows = IMT + (size_t)r0 * NP2;
-    for (int rr = warp; rr < nr; rr += nw) {
-      const double *row = rows + (size_t)rr * NP2;
-      const int i = r0 + rr;
-      double acc[3] = {0.0, 0.0, 0.0};
-      for (int k = lane; k < NP2; k += 32) {
-        const double a = row[k];
-        for (int d = 0; d < D; d++) acc[d] += a * x[d * NP2 + k];
-      }
-      int n = (int)sqrt((double)i);
-      while (n * n > i) n--;
-      while ((n + 1) * (n + 1) <= i) n++;
+    double acc[4][D];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int d = 0; d < D; d++) acc[j][d] = 0.0;
+    int k = lane;
+    for (; k + 32 < NV; k += 64) {
+      double2 a[4], b[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) { a[j] = __ldg(rp[j] + k); b[j] = __ldg(rp[j] + k + 32); }
+#pragma unroll
       for (int d = 0; d < D; d++) {
-        double v = acc[d];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) Y[d * NP2 + i] = v * scale[n];
+        const double2 u = x2[d * NV + k], v = x2[d * NV + k + 32];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          acc[j][d] += a[j].x * u.x + a[j].y * u.y;
+          acc[j][d] += b[j].x * v.x + b[j].y * v.y;
+        }
       }
     }
-    tm.sync();
-    done = blk + 1;
-    if (async_ok && *fail) break;
-    if (async_ok && blk + PBSAM_NSTAGE < nblk) {
-      if (tm.rank == 0) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const int b2 = blk + PBSAM_NSTAGE, s0 = b2 * RB, n2 = (NP2 - s0 < RB) ? NP2 - s0 : RB;
-        bulk_load(sc.stage + (size_t)q * RB * NP2, IMT + (size_t)s0 * NP2, (unsigned)(n2 * NP2 * 8), &sc.bars[q]);
+    if (k < NV) {
+      double2 a[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) a[j] = __ldg(rp[j] + k);
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        const double2 u = x2[d * NV + k];
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[j][d] += a[j].x * u.x + a[j].y * u.y;
       }
-      issued++;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        double v = acc[j][d];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc[j][d] = v;
+      }
+    if (lane < 4) {
+      const int i = r0 + lane;
+      if (i < NP2) {
+        int n = (int)sqrt((double)i);
+        while (n * n > i) n--;
+        while ((n + 1) * (n + 1) <= i) n++;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (j == lane)
+#pragma unroll
+            for (int d = 0; d < D; d++) Y[d * NP2 + i] = acc[j][d] * scale[n];
+      }
     }
   }
-  if (async_ok) {
-    if (*fail) {
-      // a wait expired: drain this team's copies still in flight (bounded), report, move on
-      if (tm.rank == 0) {
-        for (int b2 = done; b2 < issued; b2++) mbar_wait(&sc.bars[b2 % PBSAM_NSTAGE], (unsigned)((b2 / PBSAM_NSTAGE) & 1));
-        if (err) *err = 1;
-      }
-    }
-    tm.sync();
-    if (tm.rank == 0)
-      for (int q = 0; q < PBSAM_NSTAGE; q++) mbar_inval(&sc.bars[q]);
-    tm.sync();
-  }
+}
+
+__device__ __forceinline__ void imat_apply(const Team &tm, const double *IMT, int ld, const double *x, int NP2, int D,
+                                           double *Y, const double *scale)
+{
+  if (D == 1) imat_apply_t<1>(tm, IMT, ld, x, NP2, Y, scale);
+  else imat_apply_t<3>(tm, IMT, ld, x, NP2, Y, scale);
 }
 
 // ------------------------------------------------------------------ F/H inner solve
@@ -556,8 +607,12 @@ __device__ double solve_fh(const Team &tm, const Tab &T, const TypeView &tv, con
   const double *cst = tv.cst + (size_t)ts * CST_N * NP;
   const double *Dfix = tv.Dfix + (size_t)ts * NP2, *Vfix = tv.Vfix + (size_t)ts * NP2;
   const double *IM = tv.imat + (size_t)ts * imat_stride(NP2);
+  const int ld = sc.ld;
   double *fbase = sc.sol, *hbase = sc.sol + len, *fx = sc.xs, *hx = sc.xs;
   double *oldH = sc.sol + 4 * len, *outH = sc.sol + 5 * len;
+  // the operands' pad columns stay zero (the IMat pad column is zero too)
+  for (int d = tm.rank; d < D; d += tm.size)
+    for (int k = NP2; k < ld; k++) sc.xs[d * ld + k] = 0.0;
   for (int k = tm.rank; k < len; k += tm.size) {
     const int kk = k % NP2;
     int n = (int)sqrt((double)kk);
@@ -582,20 +637,20 @@ __device__ double solve_fh(const Team &tm, const Tab &T, const TypeView &tv, con
       int n = (int)sqrt((double)kk);
       while (n * n > kk) n--;
       while ((n + 1) * (n + 1) <= kk) n++;
-      fx[k] = fbase[k] + cst[CST_H1 * NP + n] * H[k] + cst[CST_F1 * NP + n] * F[k];
+      fx[(k / NP2) * ld + kk] = fbase[k] + cst[CST_H1 * NP + n] * H[k] + cst[CST_F1 * NP + n] * F[k];
     }
     tm.sync();
-    imat_apply(tm, sc, IM, sc.xs, NP2, D, F, T.CONST3, stats ? stats + 7 : nullptr);
+    imat_apply(tm, IM, ld, sc.xs, NP2, D, F, T.CONST3);
     tm.sync();
     for (int k = tm.rank; k < len; k += tm.size) {
       const int kk = k % NP2;
       int n = (int)sqrt((double)kk);
       while (n * n > kk) n--;
       while ((n + 1) * (n + 1) <= kk) n++;
-      hx[k] = hbase[k] + cst[CST_H2 * NP + n] * H[k] + cst[CST_F2 * NP + n] * F[k];
+      hx[(k / NP2) * ld + kk] = hbase[k] + cst[CST_H2 * NP + n] * H[k] + cst[CST_F2 * NP + n] * F[k];
     }
     tm.sync();
-    imat_apply(tm, sc, IM, sc.xs, NP2, D, H, cst + CST_INVH * NP, stats ? stats + 7 : nullptr);
+    imat_apply(tm, IM, ld, sc.xs, NP2, D, H, cst + CST_INVH * NP);
     tm.sync();
     // computeDev over complex entries (d, n, m)
     double part = 0.0;
@@ -823,8 +878,8 @@ __device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s)
       pair_apply(tm, T, y.sc, X, false, y.H(s2), bq);
       pc.stop(tm, PH_INTRA);
     } else {
-      numeric_expand<1>(tm, T, y.sc, y.spx(s2), y.npts(s2), P, y.qF(s2), true, false, pF, y.rad(s), a);
-      numeric_expand<1>(tm, T, y.sc, y.spx(s2), y.npts(s2), P, y.qH(s2), true, true, pH, y.rad(s), bq);
+      numeric_expand2<1>(tm, T, y.sc, y.spx(s2), y.npts(s2), P, y.rad(s), NumSet{y.qF(s2), true, false, pF, a},
+                         NumSet{y.qH(s2), true, true, pH, bq});
       pc.stop(tm, PH_NUMERIC);
     }
     for (int t = tm.rank; t < y.NP2; t += tm.size) { y.LFS(s)[t] += a[t]; y.LHS(s)[t] += bq[t]; }
@@ -881,6 +936,8 @@ __device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int
   const int NP2 = y.NP2, i = y.mol(s), ts = y.ts(s);
   double *tGrot = y.sc.G(1), *LGH = y.sc.G(2), *LGF = y.sc.G(3), *LGH2 = y.sc.G(4), *tmpG = y.sc.G(5);
   double *tL = y.sc.E(7);
+  PhaseClock gx{y.tph, 0};
+  gx.start(tm);
   tcopy(tm, tGrot, y.gw(bv.tGw, key), 3 * NP2);
   tm.sync();
   double ci[3];
@@ -940,13 +997,15 @@ __device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int
         add_vec_into(tm, LGH2 + cc * NP2, tL, NP2);
       }
     } else {
-      numeric_expand<3>(tm, T, y.sc, y.spx(sm), y.npts(sm), P, y.gFp(sm), true, false, pF, y.rad(s), tmpG);
+      double *tmpH = y.sc.G(6);
+      numeric_expand2<3>(tm, T, y.sc, y.spx(sm), y.npts(sm), P, y.rad(s), NumSet{y.gFp(sm), true, false, pF, tmpG},
+                         NumSet{y.gHp(sm), true, true, pH, tmpH});
       add_vec_into(tm, LGF, tmpG, 3 * NP2);
-      numeric_expand<3>(tm, T, y.sc, y.spx(sm), y.npts(sm), P, y.gHp(sm), true, true, pH, y.rad(s), tmpG);
-      add_vec_into(tm, LGH2, tmpG, 3 * NP2);
+      add_vec_into(tm, LGH2, tmpH, 3 * NP2);
     }
   }
   add_vec_into(tm, LGH, LGH2, 3 * NP2);
+  gx.stop(tm, PH_GRX);
   double *gF = y.gw(bv.gFw, key), *gHk = y.gw(bv.gHw, key);
   PhaseClock pc{y.tph, 0};
   pc.start(tm);
@@ -1282,7 +1341,6 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
     qrot(qn, Tq, bv.torque + ((size_t)b * nmol + i) * 3);
   }
   tm.sync();
-  if (tm.rank == 0 && st[7] != 0) bv.status[b] = PBSAM_STATUS_WAIT_EXPIRED;
   total.stop(tm, PH_TOTAL);
   (void)shv;
 }
@@ -1515,8 +1573,8 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup2_kernel(Ctx c, double 
       const int pF = compute_order(NP, rho, tv.tFself[tj], rj), pH = compute_order(NP, rho, tv.tHself[tj], rj);
       const double *pts = tv.spx + 3 * (size_t)tv.spx_off[tj];
       const int npt = tv.spx_off[tj + 1] - tv.spx_off[tj];
-      numeric_expand<1>(tm, T, sc, pts, npt, P, tv.qFself + tv.spx_off[tj], true, false, pF, ri, a);
-      numeric_expand<1>(tm, T, sc, pts, npt, P, tv.qHself + tv.spx_off[tj], true, true, pH, ri, bq);
+      numeric_expand2<1>(tm, T, sc, pts, npt, P, ri, NumSet{tv.qFself + tv.spx_off[tj], true, false, pF, a},
+                         NumSet{tv.qHself + tv.spx_off[tj], true, true, pH, bq});
     }
     for (int i = tm.rank; i < NP2; i += tm.size) { LFi[i] += a[i]; LHi[i] += bq[i]; }
     tm.sync();

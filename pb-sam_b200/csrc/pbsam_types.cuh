@@ -85,7 +85,8 @@ struct BatchView {
   int *status;               // [B]
   int *stats;                // [B][8]: sweeps, inner iterations, solves, grad solves, ...
   double *tphase;            // [B][8] device time per phase (ns): solve, surface charges,
-                             // numeric near field, analytic intra, inter LS, gradient DTA, total
+                             // numeric near field, analytic intra, inter LS, gradient DTA,
+                             // gradient-solve re-expansions, total
 };
 
 enum {
@@ -93,7 +94,6 @@ enum {
   PBSAM_STATUS_OVERLAP = 1,
   PBSAM_STATUS_NOT_CONVERGED = 2,
   PBSAM_STATUS_NAN = 3,
-  PBSAM_STATUS_WAIT_EXPIRED = 4,
 };
 
 struct Ctx {

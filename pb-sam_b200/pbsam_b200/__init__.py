@@ -217,7 +217,7 @@ class Molecules:
 
     def phase_ms(self):
         """Device ms per phase of the last evaluation: solve, surface charges, numeric,
-        analytic intra, inter LS, gradient DTA, total."""
+        analytic intra, inter LS, gradient DTA, gradient-solve re-expansions, total."""
         m = np.zeros((self.n_systems, 8))
         _check(lib().pbsam_system_phase_ms(self.handle, _dptr(m)))
         return m

@@ -79,48 +79,54 @@ def write_exp(path, coeffs, poles, scale):
         fh.write("\n")
 
 
-def prepare(cfg, device=0, outdir=None, log=print):
+def write_inputs(cfg, specs, outdir):
+    """Write prepared inputs in the reference's formats (PQR, imat.sp<k>.out.bin,
+    <name>.<k>.{F,H}.exp); returns per molecule (pqr, imat dir, exp dir, exp name)."""
+    mols = molecules(cfg)
+    files = []
+    for k, (m, sp) in enumerate(zip(mols, specs)):
+        tag = "AB"[k]
+        os.makedirs(os.path.join(outdir, "im" + tag), exist_ok=True)
+        os.makedirs(os.path.join(outdir, "exp" + tag), exist_ok=True)
+        synth.write_pqr(m, os.path.join(outdir, "mol%s.pqr" % tag))
+        for i in range(len(sp["radii"])):
+            write_imat(os.path.join(outdir, "im" + tag, "imat.sp%d.out.bin" % i), sp["imats"][i], cfg["poles"])
+            write_exp(os.path.join(outdir, "exp" + tag, "mol%s.0.%d.F.exp" % (tag, i)), sp["fself"][i],
+                      cfg["poles"], sp["hself_scale"][i])
+            write_exp(os.path.join(outdir, "exp" + tag, "mol%s.0.%d.H.exp" % (tag, i)), sp["hself"][i],
+                      cfg["poles"], sp["hself_scale"][i])
+        files.append((os.path.join(outdir, "mol%s.pqr" % tag), os.path.join(outdir, "im" + tag),
+                      os.path.join(outdir, "exp" + tag), "mol%s.0" % tag))
+    return files
+
+
+def prepare(cfg, device=0, outdir=None, selfpol_rounds=1700):
     """Build IMats and self-polarized expansions on the GPU; returns
     (moltype specs for CSystem.create_moltype, prep timings, file specs or None)."""
     import time
     import pbsam_b200 as pb
     mols = molecules(cfg)
-    specs, files, tm = [], [], {}
+    specs, tm = [], {}
     prep = pb.CSystem(poles=cfg["poles"], salt=cfg["salt"], idiel=cfg["idiel"], device=device)
     types = []
-    imats_all = []
     for k, m in enumerate(mols):
         cen, rad, pos, q = _pqr_round(m)
         t0 = time.time()
         im = prep.build_imats(cen, rad)
-        tm["imat_s_%d" % k] = time.time() - t0
-        imats_all.append(im)
+        tm["imat_s_%d" % k] = round(time.time() - t0, 2)
         ns = len(rad)
         P2 = cfg["poles"] ** 2
         types.append(prep.create_moltype(cen, rad, pos, q, im, np.zeros((ns, P2)), np.zeros((ns, P2)), 1.0 / rad))
         specs.append(dict(centres=cen, radii=rad, chg_pos=pos, chg=q, imats=im))
     for k, t in enumerate(types):
         t0 = time.time()
-        F, H, sc, rounds = prep.self_polarize(t)
-        tm["selfpol_s_%d" % k] = time.time() - t0
-        tm["selfpol_rounds_%d" % k] = rounds
+        F, H, sc, rounds = prep.self_polarize(t, max_rounds=selfpol_rounds)
+        tm["selfpol_s_%d" % k] = round(time.time() - t0, 2)
+        tm["selfpol_sweeps_%d" % k] = rounds
         specs[k].update(fself=F, hself=H, hself_scale=sc)
     prep.close()
-    if outdir:
-        for k, (m, sp) in enumerate(zip(mols, specs)):
-            tag = "AB"[k]
-            os.makedirs(os.path.join(outdir, "im" + tag), exist_ok=True)
-            os.makedirs(os.path.join(outdir, "exp" + tag), exist_ok=True)
-            synth.write_pqr(m, os.path.join(outdir, "mol%s.pqr" % tag))
-            for i in range(len(sp["radii"])):
-                write_imat(os.path.join(outdir, "im" + tag, "imat.sp%d.out.bin" % i), sp["imats"][i], cfg["poles"])
-                write_exp(os.path.join(outdir, "exp" + tag, "mol%s.0.%d.F.exp" % (tag, i)), sp["fself"][i],
-                          cfg["poles"], sp["hself_scale"][i])
-                write_exp(os.path.join(outdir, "exp" + tag, "mol%s.0.%d.H.exp" % (tag, i)), sp["hself"][i],
-                          cfg["poles"], sp["hself_scale"][i])
-            files.append((os.path.join(outdir, "mol%s.pqr" % tag), os.path.join(outdir, "im" + tag),
-                          os.path.join(outdir, "exp" + tag), "mol%s.0" % tag))
-    return specs, tm, (files if outdir else None)
+    files = write_inputs(cfg, specs, outdir) if outdir else None
+    return specs, tm, files
 
 
 def open_context(cfg, specs, device=0, **kw):
