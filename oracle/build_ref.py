@@ -83,6 +83,12 @@ TIGHT = [
 ]
 
 
+# self-polarization capped at 25 sweeps (to trace a molecule whose sweeps do not converge)
+CAP25 = [
+    ("molecule.cpp", "const int MAX_POL_ROUNDS_SELF = 1700;", "const int MAX_POL_ROUNDS_SELF = 25;"),
+]
+
+
 def _replace_once(text, old, new, fname):
     n = text.count(old)
     if n != 1:
@@ -103,6 +109,8 @@ def stage_sources(poles, mode):
     patches.append(("expansion.h", "#define N_POLES 15", "#define N_POLES %d" % poles))
     if mode == "tight":
         patches += TIGHT
+    if mode == "cap25":
+        patches += CAP25
     for fname, old, new in patches:
         path = os.path.join(dst, fname)
         with open(path) as fh:

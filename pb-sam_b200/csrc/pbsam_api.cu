@@ -453,7 +453,7 @@ static int finalize_types(pbsam_context *c)
   CK(cudaSetDevice(c->device));
   const int NP = c->prm.poles;
   const long NP2 = (long)NP * NP;
-  std::vector<int> type_off(1, 0), spx_off(1, 0), nspx, near_off(1, 0), near, chg_off(1, 0), chg_lab;
+  std::vector<int> type_off(1, 0), spx_off(1, 0), nspx, near_off(1, 0), near, chg_off(1, 0), chg_lab, pair_off(1, 0);
   std::vector<double> maxR, cen, rad, spx, Fs, Hs, hsc, imat, chg_pos, chg;
   int maxq = 0, maxns = 0;
   for (auto &t : c->types) {
@@ -466,6 +466,7 @@ static int finalize_types(pbsam_context *c)
       nspx.push_back(t.nspx[k]);
       near_off.push_back(near_off.back() + (int)t.near[k].size());
       near.insert(near.end(), t.near[k].begin(), t.near[k].end());
+      pair_off.push_back(pair_off.back() + t.ns - 1);
     }
     spx.insert(spx.end(), t.spx.begin(), t.spx.end());
     Fs.insert(Fs.end(), t.fself.begin(), t.fself.end());
@@ -501,8 +502,9 @@ static int finalize_types(pbsam_context *c)
   TRY(dput(B, &tv.imat, imat)); TRY(dput(B, &tv.chg_off, chg_off)); TRY(dput(B, &tv.chg_pos, chg_pos));
   TRY(dput(B, &tv.chg, chg));
   TRY(dput(B, &tv.chg_lab, chg_lab));
+  TRY(dput(B, &tv.pair_off, pair_off));
   TRY(dalloc(B, &tv.Eass, TS * NP2));
-  const int TE = near_off.back();
+  const int TE = pair_off.back();   // ordered intra pairs of all types
   TRY(dalloc(B, &tv.pR, (size_t)TE * rot_off(NP)));
   TRY(dalloc(B, &tv.pTH, (size_t)TE * tr_off(NP)));
   TRY(dalloc(B, &tv.pTF, (size_t)TE * tr_off(NP)));
@@ -531,7 +533,7 @@ static int finalize_types(pbsam_context *c)
   pbsam_setup1_kernel<<<TS, PBSAM_TEAM, smem>>>(cx, scr, stride);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
-  // intra near pair tables, in chunks of CH entries (slim per-block scratch)
+  // intra pair tables, in chunks of CH entries (slim per-block scratch)
   const int CH = 512;
   const long long s3 = 4LL * NP * NP + tr_off(2 * NP - 1) + 2 * NP + 8;
   double *scr3 = nullptr;

@@ -27,6 +27,7 @@ struct Scr {
   double *e;             // 16 * NP2
   double *g;             // 8 * 3 * NP2
   double *sol;           // 6 * 3 * NP2 (solver work)
+  double *mv;            // 12 * NP2 (multi-vector pair transform stages)
   double *misc;          // 4096
   double2 *lvA, *lvB;    // shared memory: rotation recursion levels, (2NP-1)^2 each
   double *tile;          // shared memory (aliases the levels): numeric-expansion point tiles
@@ -48,6 +49,7 @@ __host__ __device__ inline long long scr_doubles(int NP, long long S)
   n += 16 * NP2;                // e
   n += 8 * 3 * NP2;             // g
   n += 6 * 3 * NP2;             // sol
+  n += 12 * NP2;                // mv
   n += 4096 + S * S;            // misc + list building workspace
   return n;
 }
@@ -106,6 +108,7 @@ __device__ Scr make_scr(double *base, int NP, void *smem)
   s.e = p; p += 16 * NP2;
   s.g = p; p += 8 * 3 * NP2;
   s.sol = p; p += 6 * 3 * NP2;
+  s.mv = p; p += 12 * NP2;
   s.misc = p;
   return s;
 }
@@ -201,7 +204,7 @@ __device__ void prep_pair(const Team &tm, const Tab &T, const Scr &sc, const dou
 }
 
 // Prepared intra-molecular pair from the molecule-type tables (coefficients of
-// near pair entry e computed once at set-up; the per-pair orders only truncate them).
+// intra pair entry e computed once at set-up; the per-pair orders only truncate them).
 __device__ void table_pair(const Team &tm, const Tab &T, const TypeView &tv, const Scr &sc, int e, int pH, int pF,
                            double sS, double sT, PairXf &X)
 {
@@ -225,6 +228,12 @@ __device__ void table_pair(const Team &tm, const Tab &T, const TypeView &tv, con
   tm.sync();
 }
 
+// table entry of the intra pair (ki -> target, kj -> source) of type sphere ts = type_off + ki
+__device__ __forceinline__ int intra_pair(const TypeView &tv, int ts, int ki, int kj)
+{
+  return tv.pair_off[ts] + (kj < ki ? kj : kj - 1);
+}
+
 // rotate -> translate -> rotate back (src/xforms.cpp:122-132, 260-270); Mout zero-padded to NP
 __device__ void pair_apply(const Team &tm, const Tab &T, const Scr &sc, const PairXf &X, bool useF, const double *Min,
                            double *Mout)
@@ -237,6 +246,173 @@ __device__ void pair_apply(const Team &tm, const Tab &T, const Scr &sc, const Pa
   trans_apply(tm, ts, sc.fact, tM, tL, false, p);
   tm.sync();
   rot_apply(tm, X.rs, tL, Mout, p, false, T.NP);
+  tm.sync();
+}
+
+// ------------------------------------------------------------------ multi-vector pair transform
+// Several expansions through the same pair transform at once (the x, y, z
+// components of a gradient, and the F and H expansions of one source): the
+// rotation coefficients are read once per entry for all vectors and each stage
+// is one pass of the team.  Vector v uses the unscreened translation at order pF
+// (useF) or the screened one at order pH; per vector the arithmetic is that of
+// pair_apply.  ACC: out[v] += result, else out[v] = result zero-padded to NP.
+#define PBSAM_MV 6
+struct MultiVec {
+  int n;
+  const double *in[PBSAM_MV];
+  double *out[PBSAM_MV];
+  bool useF[PBSAM_MV];
+};
+
+// rotation of vector v (degrees < p[v]) for every v at once (rot_apply per vector)
+template <bool ACC>
+__device__ void rot_apply_multi(const Team &tm, const RotState &rs, int nv, const double *const *in, double *const *out,
+                                const int *pv, int pmax, bool bFor, int zero_to)
+{
+  if (!ACC)
+    for (int v = 0; v < nv; v++)
+      for (int i = tm.rank + pv[v] * pv[v]; i < zero_to * zero_to; i += tm.size) out[v][i] = 0.0;
+  if (rs.sing) {
+    for (int i = tm.rank; i < pmax * pmax; i += tm.size) {
+      int n = (int)sqrt((double)i);
+      while (n * n > i) n--;
+      while ((n + 1) * (n + 1) <= i) n++;
+      const int mm = i - n * n;
+      double sgn = 1.0;
+      if (rs.cost == -1.0) {
+        if (mm == 0) sgn = (n % 2 == 0) ? 1.0 : -1.0;
+        else { int s0 = (n % 2 == 0) ? 1 : -1; sgn = ((mm - 1) % 2 == 0) ? s0 : -s0; }
+      }
+      for (int v = 0; v < nv; v++) {
+        if (n >= pv[v]) continue;
+        const double r = (rs.cost == -1.0) ? sgn * in[v][i] : in[v][i];
+        if (ACC) out[v][i] += r;
+        else out[v][i] = r;
+      }
+    }
+    return;
+  }
+  const int cnt = pmax * (pmax + 1) / 2;
+  for (int idx = tm.rank; idx < cnt; idx += tm.size) {
+    int n = (int)((sqrt(8.0 * idx + 1.0) - 1.0) * 0.5);
+    while (n * (n + 1) / 2 > idx) n--;
+    while ((n + 1) * (n + 2) / 2 <= idx) n++;
+    const int k = idx - n * (n + 1) / 2;
+    double2 o[PBSAM_MV];
+    bool act[PBSAM_MV];
+#pragma unroll
+    for (int v = 0; v < PBSAM_MV; v++) act[v] = v < nv && n < pv[v];
+    if (bFor) {
+      const int m = k;
+      const double2 r0 = rs.R[rot_at(n, 0, m)];
+#pragma unroll
+      for (int v = 0; v < PBSAM_MV; v++)
+        if (act[v]) o[v] = cmul(r0, make_double2(in[v][IDX(n)], 0.0));
+      for (int s = 1; s <= n; s++) {
+        const double2 rp = rs.R[rot_at(n, s, m)], rn = rs.R[rot_at(n, -s, m)];
+#pragma unroll
+        for (int v = 0; v < PBSAM_MV; v++)
+          if (act[v]) {
+            const double2 inc = make_double2(in[v][IDX(n) + 2 * s - 1], in[v][IDX(n) + 2 * s]);
+            o[v] = cadd(o[v], cadd(cmul(rp, inc), cmul(rn, cconj(inc))));
+          }
+      }
+    } else {
+      const int s = k;
+      const double2 r0 = rs.R[rot_at(n, -s, 0)];
+#pragma unroll
+      for (int v = 0; v < PBSAM_MV; v++)
+        if (act[v]) o[v] = cmul(r0, make_double2(in[v][IDX(n)], 0.0));
+      for (int m = 1; m <= n; m++) {
+        const double2 rp = cconj(rs.R[rot_at(n, s, m)]), rn = rs.R[rot_at(n, -s, m)];
+#pragma unroll
+        for (int v = 0; v < PBSAM_MV; v++)
+          if (act[v]) {
+            const double2 inc = make_double2(in[v][IDX(n) + 2 * m - 1], in[v][IDX(n) + 2 * m]);
+            o[v] = cadd(o[v], cadd(cmul(rp, inc), cmul(rn, cconj(inc))));
+          }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < PBSAM_MV; v++) {
+      if (!act[v]) continue;
+      if (k == 0) {
+        if (ACC) out[v][IDX(n)] += o[v].x;
+        else out[v][IDX(n)] = o[v].x;
+      } else {
+        if (ACC) { out[v][IDX(n) + 2 * k - 1] += o[v].x; out[v][IDX(n) + 2 * k] += o[v].y; }
+        else { out[v][IDX(n) + 2 * k - 1] = o[v].x; out[v][IDX(n) + 2 * k] = o[v].y; }
+      }
+    }
+  }
+}
+
+// forward translation of every vector (trans_apply per vector, deriv = false)
+__device__ void trans_apply_multi(const Team &tm, const PairXf &X, const double *fact, int nv, const double *const *in,
+                                  double *const *out, const bool *useF, int pmax)
+{
+  bool has[2] = {false, false};   // [0] some vector uses F, [1] some uses H
+  for (int v = 0; v < nv; v++) has[useF[v] ? 0 : 1] = true;
+  for (int i = tm.rank; i < pmax * pmax; i += tm.size) {
+    int n = (int)sqrt((double)i);
+    while (n * n > i) n--;
+    while ((n + 1) * (n + 1) <= i) n++;
+    const int mm = i - n * n;
+    const int m = (mm + 1) / 2;
+    for (int g = 0; g < 2; g++) {
+      if (!has[g]) continue;     // (the F transform is not prepared when no vector uses it)
+      const bool gF = (g == 0);
+      const TransState &ts = gF ? X.tf : X.th;
+      const int p = ts.p;
+      if (n >= p) continue;
+      double acc[PBSAM_MV];
+      bool act[PBSAM_MV];
+#pragma unroll
+      for (int v = 0; v < PBSAM_MV; v++) { act[v] = v < nv && useF[v] == gF; acc[v] = 0.0; }
+      const double *C = ts.T;
+      int l;
+      for (l = m; l <= n; l++) {
+        const double t = ((n + l) % 2 == 0) ? C[tr_at(n, l, m)] : -C[tr_at(n, l, m)];
+        const double f = fact[n - l];
+#pragma unroll
+        for (int v = 0; v < PBSAM_MV; v++)
+          if (act[v]) acc[v] += f * t * in[v][IDX(l) + mm];
+      }
+      for (; l < p; l++) {
+        const double c = C[tr_at(l, n, m)];
+#pragma unroll
+        for (int v = 0; v < PBSAM_MV; v++)
+          if (act[v]) acc[v] += c * in[v][IDX(l) + mm];
+      }
+#pragma unroll
+      for (int v = 0; v < PBSAM_MV; v++)
+        if (act[v]) out[v][i] = acc[v];
+    }
+  }
+}
+
+__device__ void pair_apply_multi(const Team &tm, const Tab &T, const Scr &sc, const PairXf &X, const MultiVec &V,
+                                 bool accumulate)
+{
+  int pv[PBSAM_MV];
+  const double *tMc[PBSAM_MV];
+  double *tM[PBSAM_MV], *tL[PBSAM_MV];
+  int pmax = 0;
+  for (int v = 0; v < PBSAM_MV; v++) {
+    pv[v] = (v < V.n) ? (V.useF[v] ? X.pF : X.pH) : 0;
+    if (pv[v] > pmax) pmax = pv[v];
+    tM[v] = sc.mv + (size_t)v * sc.NP2;
+    tMc[v] = tM[v];
+    tL[v] = sc.mv + (size_t)(PBSAM_MV + v) * sc.NP2;
+  }
+  rot_apply_multi<false>(tm, X.rs, V.n, V.in, tM, pv, pmax, true, 0);
+  tm.sync();
+  trans_apply_multi(tm, X, sc.fact, V.n, tMc, tL, V.useF, pmax);
+  tm.sync();
+  const double *tLc[PBSAM_MV];
+  for (int v = 0; v < PBSAM_MV; v++) tLc[v] = tL[v];
+  if (accumulate) rot_apply_multi<true>(tm, X.rs, V.n, tLc, V.out, pv, pmax, false, T.NP);
+  else rot_apply_multi<false>(tm, X.rs, V.n, tLc, V.out, pv, pmax, false, T.NP);
   tm.sync();
 }
 
@@ -873,9 +1049,12 @@ __device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s)
     pc.start(tm);
     if (sep > 0 && !(sep < y.c->prm.min_sep_numeric)) {
       PairXf X;
-      table_pair(tm, T, y.c->tv, y.sc, e, pH, pF, rj, y.rad(s), X);
-      pair_apply(tm, T, y.sc, X, true, y.F(s2), a);
-      pair_apply(tm, T, y.sc, X, false, y.H(s2), bq);
+      table_pair(tm, T, y.c->tv, y.sc, intra_pair(y.c->tv, ts, s - mo, kj), pH, pF, rj, y.rad(s), X);
+      MultiVec V;
+      V.n = 2;
+      V.in[0] = y.F(s2); V.out[0] = a; V.useF[0] = true;
+      V.in[1] = y.H(s2); V.out[1] = bq; V.useF[1] = false;
+      pair_apply_multi(tm, T, y.sc, X, V, false);
       pc.stop(tm, PH_INTRA);
     } else {
       numeric_expand2<1>(tm, T, y.sc, y.spx(s2), y.npts(s2), P, y.rad(s), NumSet{y.qF(s2), true, false, pF, a},
@@ -953,10 +1132,10 @@ __device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int
     PairXf X;
     prep_pair(tm, T, y.sc, P, p, 0, y.rad(sm), y.rad(s), false, X);
     const double *src = y.gw(bv.gHrotw, bv.gkey[y.sc1(sm)]);
-    for (int cc = 0; cc < 3; cc++) {
-      pair_apply(tm, T, y.sc, X, false, src + cc * NP2, tL);
-      add_vec_into(tm, tGrot + cc * NP2, tL, NP2);
-    }
+    MultiVec V;
+    V.n = 3;
+    for (int cc = 0; cc < 3; cc++) { V.in[cc] = src + cc * NP2; V.out[cc] = tGrot + cc * NP2; V.useF[cc] = false; }
+    pair_apply_multi(tm, T, y.sc, X, V, true);
   }
   const RotState mr = y.molrot(i);
   for (int cc = 0; cc < 3; cc++) rot_apply_xi(tm, mr, tGrot + cc * NP2, LGH + cc * NP2, y.NP, false, y.NP);
@@ -983,19 +1162,16 @@ __device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int
     const int pH = compute_order(y.NP, rho, bv.maxgH[y.sc1(sm)], rm);
     if (sep > 0 && !(sep < y.c->prm.min_sep_numeric)) {
       PairXf X;
-      const int kloc = sm - bv.mol_off[i];
-      int e = -1;
-      for (int q = y.c->tv.near_off[ts]; q < y.c->tv.near_off[ts + 1]; q++)
-        if (y.c->tv.near[q] == kloc) { e = q; break; }
-      if (e >= 0) table_pair(tm, T, y.c->tv, y.sc, e, pH, pF, rm, y.rad(s), X);
-      else prep_pair(tm, T, y.sc, P, pH, pF, rm, y.rad(s), false, X);
+      table_pair(tm, T, y.c->tv, y.sc, intra_pair(y.c->tv, ts, s - bv.mol_off[i], sm - bv.mol_off[i]), pH, pF, rm,
+                 y.rad(s), X);
       const int km = bv.gkey[y.sc1(sm)];
+      MultiVec V;
+      V.n = 6;
       for (int cc = 0; cc < 3; cc++) {
-        pair_apply(tm, T, y.sc, X, true, y.gw(bv.gFw, km) + cc * NP2, tL);
-        add_vec_into(tm, LGF + cc * NP2, tL, NP2);
-        pair_apply(tm, T, y.sc, X, false, y.gw(bv.gHw, km) + cc * NP2, tL);
-        add_vec_into(tm, LGH2 + cc * NP2, tL, NP2);
+        V.in[cc] = y.gw(bv.gFw, km) + cc * NP2; V.out[cc] = LGF + cc * NP2; V.useF[cc] = true;
+        V.in[3 + cc] = y.gw(bv.gHw, km) + cc * NP2; V.out[3 + cc] = LGH2 + cc * NP2; V.useF[3 + cc] = false;
       }
+      pair_apply_multi(tm, T, y.sc, X, V, true);
     } else {
       double *tmpH = y.sc.G(6);
       numeric_expand2<3>(tm, T, y.sc, y.spx(sm), y.npts(sm), P, y.rad(s), NumSet{y.gFp(sm), true, false, pF, tmpG},
@@ -1053,7 +1229,6 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
 {
   extern __shared__ double2 dsm[];
   __shared__ double red[PBSAM_TEAM];
-  __shared__ double shv[16];
   const Team tm{(int)threadIdx.x, (int)blockDim.x};
   const BatchView &bv = c.bv;
   const int b = blockIdx.x;
@@ -1342,7 +1517,6 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
   }
   tm.sync();
   total.stop(tm, PH_TOTAL);
-  (void)shv;
 }
 
 // interaction energy with the reference's convention (unrotated centres and
@@ -1544,12 +1718,13 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup2_kernel(Ctx c, double 
     bool isnear = false;
     for (int e = nb; e < ne; e++) if (tv.near[e] == kj) isnear = true;
     if (isnear) continue;
-    const double *cj = tv.cen + 3 * (t0 + kj);
-    const double P[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
     PairXf X;
-    prep_pair(tm, T, sc, P, NP, NP, tv.rad[t0 + kj], ri, false, X);
-    pair_apply(tm, T, sc, X, true, tv.Fself + (size_t)(t0 + kj) * NP2, a);
-    pair_apply(tm, T, sc, X, false, tv.Hself + (size_t)(t0 + kj) * NP2, bq);
+    table_pair(tm, T, tv, sc, intra_pair(tv, ts, ki, kj), NP, NP, tv.rad[t0 + kj], ri, X);
+    MultiVec V;
+    V.n = 2;
+    V.in[0] = tv.Fself + (size_t)(t0 + kj) * NP2; V.out[0] = a; V.useF[0] = true;
+    V.in[1] = tv.Hself + (size_t)(t0 + kj) * NP2; V.out[1] = bq; V.useF[1] = false;
+    pair_apply_multi(tm, T, sc, X, V, false);
     for (int i = tm.rank; i < NP2; i += tm.size) { LFf[i] += a[i]; LHf[i] += bq[i]; }
     tm.sync();
   }
@@ -1566,9 +1741,12 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup2_kernel(Ctx c, double 
     const double sep = rho - ri - rj;
     if (sep > 0 && !(sep < c.prm.min_sep_numeric)) {
       PairXf X;
-      table_pair(tm, T, tv, sc, e, NP, NP, rj, ri, X);
-      pair_apply(tm, T, sc, X, true, tv.Fself + (size_t)tj * NP2, a);
-      pair_apply(tm, T, sc, X, false, tv.Hself + (size_t)tj * NP2, bq);
+      table_pair(tm, T, tv, sc, intra_pair(tv, ts, ki, kj), NP, NP, rj, ri, X);
+      MultiVec V;
+      V.n = 2;
+      V.in[0] = tv.Fself + (size_t)tj * NP2; V.out[0] = a; V.useF[0] = true;
+      V.in[1] = tv.Hself + (size_t)tj * NP2; V.out[1] = bq; V.useF[1] = false;
+      pair_apply_multi(tm, T, sc, X, V, false);
     } else {
       const int pF = compute_order(NP, rho, tv.tFself[tj], rj), pH = compute_order(NP, rho, tv.tHself[tj], rj);
       const double *pts = tv.spx + 3 * (size_t)tv.spx_off[tj];
@@ -1581,10 +1759,10 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup2_kernel(Ctx c, double 
   }
 }
 
-// per near pair entry e: rotation and translation coefficients at the full pole
+// per intra pair entry e: rotation and translation coefficients at the full pole
 // order (CXFormAIntra::reset, src/xforms.cpp:213-227), kept as the prefixes the
-// apply reads (rotation n < NP, translation l < NP); entries re-expanded
-// numerically are left unused.
+// apply reads (rotation n < NP, translation l < NP); entries of pairs that are
+// re-expanded numerically are left unused.
 __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup3_kernel(Ctx c, int e0, int ne, double *scr, long long stride)
 {
   extern __shared__ double2 dsm[];
@@ -1599,10 +1777,11 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup3_kernel(Ctx c, int e0,
   double *TH = sh + 4 * NP * NP, *kbuf = TH + tr_off(NN);
   double2 *lvA = dsm, *lvB = dsm + NN * NN;
   int ts = 0;
-  while (tv.near_off[ts + 1] <= e) ts++;
+  while (tv.pair_off[ts + 1] <= e) ts++;
   int t = 0;
   while (tv.type_off[t + 1] <= ts) t++;
-  const int tj = tv.type_off[t] + tv.near[e];
+  const int ki = ts - tv.type_off[t], j = e - tv.pair_off[ts];
+  const int tj = tv.type_off[t] + (j < ki ? j : j + 1);
   const double *ci = tv.cen + 3 * ts, *cj = tv.cen + 3 * tj;
   const double P[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
   const Sph S = cart2sph(P[0], P[1], P[2]);

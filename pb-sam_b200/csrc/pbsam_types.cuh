@@ -48,7 +48,9 @@ struct TypeView {
   const double *chg;       // [TQ]
   const int *chg_lab;      // [TQ] sphere (within the type) each charge is assigned to
   double *Eass;            // [TS][NP2] multipole of the assigned charges (self-polarization start)
-  // coefficient tables of the intra near pairs, one per near-list entry
+  // coefficient tables of the intra pairs: one entry per ordered pair (ki, kj != ki)
+  // of each type, entry pair_off[ts] + (kj < ki ? kj : kj - 1)
+  const int *pair_off;     // [TS+1]
   double2 *pR;             // [TE][rot_off(NP)]
   double *pTH, *pTF;       // [TE][tr_off(NP)] screened / unscreened translation
   double *pS;              // [TE][16] rotation scalars
