@@ -137,6 +137,9 @@ def run_ours(args):
     ctx, types = workload.open_context(cfg, specs, device=local)
     mols = workload.molecules(cfg)
     pos, quat, _ = workload.poses(cfg, mols, rank=rank)
+    if args.poses:
+        sel = [int(x) for x in args.poses.split(",")]
+        pos, quat = pos[sel], quat[sel]
     B = len(pos)
     sysb = ctx.molecules(types, n_systems=B)
     stream = torch.cuda.current_stream()
@@ -205,7 +208,8 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator; IMats and self-polarized expansions built on the GPU)",
-            "config": {"workload": WORKLOAD, "poles": cfg["poles"], "systems_per_gpu": B,
+            "config": {"workload": WORKLOAD, "poses": args.poses or "all", "poles": cfg["poles"],
+                       "systems_per_gpu": B,
                        "spheres_per_system": 2 * cfg["n_sph"],
                        "parallelism": "replicas: %d rank(s) x %d independent systems" % (world, B),
                        "l2": "no flush: inputs larger than L2 (120 IMats x 6.5 MB = 778 MB)"},
@@ -386,6 +390,7 @@ def main():
     ap.add_argument("--cpu-sample-its", type=int, default=6000,
                     help="largest inner-iteration count of a pose in the CPU sample")
     ap.add_argument("--cpu-limit", type=int, default=60, help="seconds before a sample pose is abandoned")
+    ap.add_argument("--poses", default="", help="comma-separated subset of the sweep's poses (small cases)")
     ap.add_argument("--traffic-per-launch", type=float, default=None,
                     help="DRAM bytes per launch measured by ncu (scaled from a small capture)")
     args = ap.parse_args()
