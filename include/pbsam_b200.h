@@ -133,6 +133,16 @@ int pbsam_system_last_kernel_ms(const pbsam_system *sys, double *ms);
  * imats receives n_sph * p^4 doubles, the content of imat.sp<k>.out.bin. */
 int pbsam_imat_build(pbsam_context *ctx, int n_sph, const double *centres, const double *radii, int n_points,
                      double *imats);
+/* No counterpart in the reference.  Same result as pbsam_imat_build, for callers
+ * that cannot allocate device memory (their own pool allocator owns the device, or
+ * their footprint must stay fixed after load): the work buffers are one fixed
+ * device array of about 3.2 MB that the library holds on every device it is used
+ * on.  Limits: pole order <= 16, at most 256 spheres overlapping any one sphere;
+ * larger cases return PBSAM_E_BADARG.  The first call on a device looks up the
+ * array's address; make it before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race, so callers serialise them. */
+int pbsam_imat_build_static(pbsam_context *ctx, int n_sph, const double *centres, const double *radii, int n_points,
+                            double *imats);
 /* Self-polarization of one molecule type: replaces CMolecule::polarize_self
  * (src/molecule.cpp:1898-1979) as run by `pbsam spol` (src/selfp_makemat.cpp:37-118).
  * The type's own F/H inputs are ignored.  Outputs are rounded as the reference

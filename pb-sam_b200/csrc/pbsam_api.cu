@@ -864,3 +864,6 @@ extern "C" int pbsam_system_phase_ms(const pbsam_system *s, double *ms)
   for (int i = 0; i < s->B * 8; i++) ms[i] *= 1e-6;
   return PBSAM_OK;
 }
+
+// fixed-buffer variant of the IMat builder (uses the helpers above)
+#include "pbsam_static_imat.cu"

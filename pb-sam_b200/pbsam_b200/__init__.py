@@ -61,6 +61,7 @@ SIGNATURES = {
     "pbsam_system_last_kernel_ms": (ctypes.c_int, [_P, _DP]),
     "pbsam_system_phase_ms": (ctypes.c_int, [_P, _DP]),
     "pbsam_imat_build": (ctypes.c_int, [_P, ctypes.c_int, _DP, _DP, ctypes.c_int, _DP]),
+    "pbsam_imat_build_static": (ctypes.c_int, [_P, ctypes.c_int, _DP, _DP, ctypes.c_int, _DP]),
     "pbsam_selfpol": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _IP]),
     "pbsam_last_error": (ctypes.c_char_p, []),
 }
