@@ -134,7 +134,7 @@ def run_ours(args):
     cfg = dict(workload.SWEEP_P30)
     t0 = time.time()
     specs, prep_t, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds)
-    ctx, types = workload.open_context(cfg, specs, device=local)
+    ctx, types = workload.open_context(cfg, specs, device=local, cluster_size=args.cluster_size)
     mols = workload.molecules(cfg)
     pos, quat, _ = workload.poses(cfg, mols, rank=rank)
     if args.poses:
@@ -211,7 +211,8 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "poses": args.poses or "all", "poles": cfg["poles"],
                        "systems_per_gpu": B,
                        "spheres_per_system": 2 * cfg["n_sph"],
-                       "parallelism": "replicas: %d rank(s) x %d independent systems" % (world, B),
+                       "parallelism": "replicas: %d rank(s) x %d independent systems, %d CTAs per system" % (
+                           world, B, int(stats[0, 5])),
                        "l2": "no flush: inputs larger than L2 (120 IMats x 6.5 MB = 778 MB)"},
             "e2e": {"value": units / (e2e_max * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": int(hp.nbytes + hq.nbytes),
@@ -390,6 +391,7 @@ def main():
     ap.add_argument("--cpu-sample-its", type=int, default=6000,
                     help="largest inner-iteration count of a pose in the CPU sample")
     ap.add_argument("--cpu-limit", type=int, default=60, help="seconds before a sample pose is abandoned")
+    ap.add_argument("--cluster-size", type=int, default=0, help="CTAs per system (0: automatic)")
     ap.add_argument("--poses", default="", help="comma-separated subset of the sweep's poses (small cases)")
     ap.add_argument("--traffic-per-launch", type=float, default=None,
                     help="DRAM bytes per launch measured by ncu (scaled from a small capture)")

@@ -49,6 +49,9 @@ typedef struct pbsam_params {
   double intra_cutoff;    /* intra near-list cutoff, src/BDnam.cpp:82 (30) */
   double min_sep_numeric; /* MINSEPDIST, src/molecule.h:22 (5) */
   int num_points_x;       /* NUM_POINTS_X cap on surface points, src/molecule.cpp:64 (10000) */
+  int cluster_size;       /* CTAs (one thread-block cluster) working on each system: 0 = the largest
+                             of 8, 4, 2 that keeps a whole batch resident at once; 1..8 forces it.
+                             No reference counterpart (a B200 launch parameter). */
 } pbsam_params;
 
 typedef struct pbsam_context pbsam_context;
@@ -107,7 +110,8 @@ int pbsam_system_compute_energy(pbsam_system *sys, double *energy, int on_device
 
 /* Counters of the last force evaluation, 8 ints per system: [0] sweeps,
  * [1] inner F/H iterations, [2] inner solves, [3] gradient solves,
- * [4] 1 if the polarization sweeps hit max_pol_rounds. */
+ * [4] 1 if the polarization sweeps hit max_pol_rounds, [5] CTAs that worked on
+ * the system. */
 int pbsam_system_stats(const pbsam_system *sys, int *stats);
 
 /* CUDA stream the system's work is queued on (cudaStream_t as void*); the

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <fstream>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "pbsam_b200.h"
@@ -150,6 +151,7 @@ struct pbsam_system {
   cudaStream_t stream = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
+  int crew = 1;            // CTAs (one cluster) per system in the force kernel
 };
 
 extern "C" void pbsam_params_default(pbsam_params *p)
@@ -158,6 +160,7 @@ extern "C" void pbsam_params_default(pbsam_params *p)
   p->max_polar_dev = 1e-2; p->solve_tol = 1e-8; p->solve_max_ct = 100; p->max_pol_rounds = 1000;
   p->inter_cutoff = 10; p->interact_cutoff = 100; p->intra_cutoff = 30; p->min_sep_numeric = 5;
   p->num_points_x = 10000;
+  p->cluster_size = 0;
 }
 
 static double kappa_of(const pbsam_params &p)
@@ -171,6 +174,8 @@ extern "C" int pbsam_context_create(const pbsam_params *prm, int device, pbsam_c
 {
   if (!prm || !out) return fail(PBSAM_E_BADARG, "null argument");
   if (prm->poles < 1 || prm->poles > 32) return fail(PBSAM_E_BADARG, "poles must be in [1, 32]");
+  if (prm->cluster_size < 0 || prm->cluster_size > 8)
+    return fail(PBSAM_E_BADARG, "cluster_size must be 0 (automatic) or 1..8");
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
   if (device < 0 || device >= ndev) return fail(PBSAM_E_BADARG, "no such CUDA device");
@@ -432,6 +437,52 @@ static int dput(std::vector<void *> &bufs, const T **p, const std::vector<T> &h)
 }
 #define TRY(x) do { int r_ = (x); if (r_) return r_; } while (0)
 
+// Launch n_sys crews of C CTAs (a thread-block cluster per system when C > 1).
+template <class... Exp, class... Act>
+static cudaError_t launch_crews(void (*kern)(Exp...), int n_sys, int C, size_t smem, cudaStream_t st, Act &&...args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(n_sys * C));
+  cfg.blockDim = dim3(PBSAM_TEAM);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  if (C > 1) {
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+  }
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Act>(args)...);
+}
+
+// CTAs per system: the requested size, or the largest of 8, 4, 2 at which all
+// n_sys crews are resident at once (cluster occupancy), else 1.
+template <class K>
+static int pick_crew(K kern, int n_sys, size_t smem, int requested)
+{
+  if (requested > 0) return requested;
+  for (int C : {8, 4, 2}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(n_sys * C));
+    cfg.blockDim = dim3(PBSAM_TEAM);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, (const void *)kern, &cfg) == cudaSuccess && n >= n_sys) return C;
+    cudaGetLastError();
+  }
+  return 1;
+}
+
 // opt every team kernel into the dynamic shared memory it needs
 static int set_smem_attrs(int NP)
 {
@@ -628,6 +679,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   p.min_sep_numeric = c->prm.min_sep_numeric; p.idiel = c->prm.idiel; p.sdiel = c->prm.sdiel;
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);
+  s->crew = pick_crew(pbsam_forces_kernel, B, team_smem_bytes(NP), c->prm.cluster_size);
   c->live_systems++;
   *out = s;
   return pbsam_system_reset(s);
@@ -680,7 +732,7 @@ extern "C" int pbsam_system_compute_forces(pbsam_system *s, double *force, doubl
   if (!s) return fail(PBSAM_E_BADARG, "null system");
   CK(cudaSetDevice(s->ctx->device));
   CK(cudaEventRecord(s->ev0, s->stream));
-  pbsam_forces_kernel<<<s->B, PBSAM_TEAM, team_smem_bytes(s->ctx->prm.poles), s->stream>>>(s->c);
+  CK(launch_crews(pbsam_forces_kernel, s->B, s->crew, team_smem_bytes(s->ctx->prm.poles), s->stream, s->c));
   CK(cudaGetLastError());
   CK(cudaEventRecord(s->ev1, s->stream));
   const size_t n = (size_t)s->B * s->nmol * 3;
@@ -838,8 +890,11 @@ extern "C" int pbsam_selfpol(pbsam_context *c, int type_id, int max_rounds, doub
   TRY(pbsam_system_create(c, 1, 1, mt, &s));
   int *drounds = nullptr;
   if (cudaMalloc(&drounds, sizeof(int)) != cudaSuccess) { pbsam_system_destroy(s); return fail(PBSAM_E_NOMEM, "rounds"); }
-  pbsam_selfpol_kernel<<<1, PBSAM_TEAM, team_smem_bytes(c->prm.poles), s->stream>>>(s->c, c->tv.Eass, max_rounds, drounds);
-  cudaError_t e = cudaGetLastError();
+  const size_t sp_smem = team_smem_bytes(c->prm.poles);
+  const int sp_crew = pick_crew(pbsam_selfpol_kernel, 1, sp_smem, c->prm.cluster_size);
+  cudaError_t e = launch_crews(pbsam_selfpol_kernel, 1, sp_crew, sp_smem, s->stream, s->c, (const double *)c->tv.Eass,
+                               max_rounds, drounds);
+  if (e == cudaSuccess) e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   const int ns = c->types[type_id].ns, NP2 = c->prm.poles * c->prm.poles;
   std::vector<double> F((size_t)ns * NP2), H((size_t)ns * NP2);

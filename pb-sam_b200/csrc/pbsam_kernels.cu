@@ -9,9 +9,11 @@
 // loop is bounded by the reference's own iteration caps; no thread ever waits
 // on another team.
 #include <cstdio>
+#include <cooperative_groups.h>
 #include "pbsam_types.cuh"
 
 namespace pbsam {
+namespace cg = cooperative_groups;
 
 #define PBSAM_TEAM 512
 
@@ -514,8 +516,11 @@ __device__ __forceinline__ void radial_factors(const Tab &T, double rho, double 
 
 template <int NC>
 __device__ void numeric_expand2(const Team &tm, const Tab &T, const Scr &sc, const double *pts, int N,
-                                const double *shift, double scale, NumSet A, NumSet B)
+                                const double *shift, double scale, NumSet A, NumSet B, int part_rank = 0,
+                                int part_size = 1, double *part = nullptr)
 {
+  // part != nullptr: this CTA takes tiles part_rank, part_rank + part_size, ... and
+  // writes its partial sums to part[(set * NC + k) * NP2 + c] instead of the outputs
   const int NP = T.NP, NP2 = NP * NP;
   const bool useB = B.w != nullptr;
   const int P = (useB && B.P > A.P) ? B.P : A.P, P2 = P * P;
@@ -539,7 +544,7 @@ __device__ void numeric_expand2(const Team &tm, const Tab &T, const Scr &sc, con
     for (int k = 0; k < NC; k++) { accA[j][k] = 0.0; accB[j][k] = 0.0; }
   }
   const int npair = (P + 1) / 2;
-  for (int h0 = 0; h0 < N; h0 += TP) {
+  for (int h0 = part_rank * TP; h0 < N; h0 += part_size * TP) {
     const int nt = (N - h0 < TP) ? N - h0 : TP;
     // per (point, set): weights, validity, radial factors; set A also the angles
     for (int u = tm.rank; u < 2 * nt; u += tm.size) {
@@ -622,8 +627,10 @@ __device__ void numeric_expand2(const Team &tm, const Tab &T, const Scr &sc, con
     if (c < NP2)
 #pragma unroll
       for (int k = 0; k < NC; k++) {
-        A.out[(size_t)k * NP2 + c] = (c < PA2) ? accA[j][k] : 0.0;
-        if (useB) B.out[(size_t)k * NP2 + c] = (c < PB2) ? accB[j][k] : 0.0;
+        double *oa = part ? part + (size_t)k * NP2 : A.out + (size_t)k * NP2;
+        double *ob = part ? part + (size_t)(NC + k) * NP2 : (useB ? B.out + (size_t)k * NP2 : nullptr);
+        oa[c] = (c < PA2) ? accA[j][k] : 0.0;
+        if (useB) ob[c] = (c < PB2) ? accB[j][k] : 0.0;
       }
   }
   tm.sync();
@@ -694,13 +701,13 @@ __device__ void surface_q(const Team &tm, const Tab &T, const double *pts, int N
 // blocks per step, so 128 bytes per lane are in flight; the D operands share every
 // loaded IMat element.  The row sums are reduced across the warp in a fixed order.
 template <int D>
-__device__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const double *x, int NP2, double *Y,
-                             const double *scale)
+__device__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const double *x, int NP2, int r_begin, int r_end,
+                             double *Y, const double *scale)
 {
   const int lane = tm.rank & 31, warp = tm.rank >> 5, nw = tm.size >> 5;
   const int NV = ld >> 1;
   const double2 *x2 = (const double2 *)x;
-  for (int r0 = warp * 4; r0 < NP2; r0 += nw * 4) {
+  for (int r0 = r_begin + warp * 4; r0 < r_end; r0 += nw * 4) {
     const double2 *rp[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -749,7 +756,7 @@ __device__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const do
       }
     if (lane < 4) {
       const int i = r0 + lane;
-      if (i < NP2) {
+      if (i < r_end) {
         int n = (int)sqrt((double)i);
         while (n * n > i) n--;
         while ((n + 1) * (n + 1) <= i) n++;
@@ -764,10 +771,123 @@ __device__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const do
 }
 
 __device__ __forceinline__ void imat_apply(const Team &tm, const double *IMT, int ld, const double *x, int NP2, int D,
-                                           double *Y, const double *scale)
+                                           int r_begin, int r_end, double *Y, const double *scale)
 {
-  if (D == 1) imat_apply_t<1>(tm, IMT, ld, x, NP2, Y, scale);
-  else imat_apply_t<3>(tm, IMT, ld, x, NP2, Y, scale);
+  if (D == 1) imat_apply_t<1>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
+  else imat_apply_t<3>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
+}
+
+// ------------------------------------------------------------------ crews (thread-block clusters)
+// A system may own a cluster of CTAs (a crew).  CTA 0 (the leader) runs the whole
+// evaluation; the others (helpers) take a share of the IMat rows of every matvec.
+// Protocol, all on cluster barriers (no flags, no spinning): the leader publishes
+// a command in its shared memory next to the operands and arrives; every CTA
+// applies its rows, writing them to the global output; a second barrier makes the
+// rows visible to the leader.  The exit command is followed by one last barrier so
+// no helper reads the leader's shared memory after it has gone.
+struct CrewCmd {
+  int op;                 // 0: exit, 1: matvec, 2: numeric expansion
+  int D, NP2, ld;         // matvec
+  const double *IMT;
+  double *Y;
+  const double *scale;
+  int NC, N;              // numeric expansion
+  const double *pts;
+  double shift[3], nscale;
+  NumSet A, B;
+};
+struct Crew {
+  int rank, size;         // CTA rank in the cluster, CTAs per system
+  CrewCmd *cmd;           // this CTA's command block (helpers read the leader's)
+};
+
+__device__ __forceinline__ void crew_rows(int NP2, int rank, int size, int &r0, int &r1)
+{
+  const int per = ((NP2 + size - 1) / size + 3) & ~3;
+  r0 = rank * per;
+  r1 = r0 + per;
+  if (r0 > NP2) r0 = NP2;
+  if (r1 > NP2) r1 = NP2;
+}
+
+__device__ void crew_imat_apply(const Team &tm, const Crew &cw, const double *IMT, int ld, const double *x, int NP2,
+                                int D, double *Y, const double *scale)
+{
+  if (cw.size == 1) { imat_apply(tm, IMT, ld, x, NP2, D, 0, NP2, Y, scale); return; }
+  cg::cluster_group cl = cg::this_cluster();
+  if (tm.rank == 0) {
+    cw.cmd->op = 1; cw.cmd->D = D; cw.cmd->NP2 = NP2; cw.cmd->ld = ld;
+    cw.cmd->IMT = IMT; cw.cmd->Y = Y; cw.cmd->scale = scale;
+  }
+  cl.sync();                    // command and operands visible to the crew
+  int r0, r1;
+  crew_rows(NP2, 0, cw.size, r0, r1);
+  imat_apply(tm, IMT, ld, x, NP2, D, r0, r1, Y, scale);
+  cl.sync();                    // every CTA's rows written
+}
+
+// Numeric expansion (numeric_expand2) shared by the crew: each CTA sums a share of
+// the point tiles into its shared memory, the leader adds the partials in rank order.
+template <int NC>
+__device__ void crew_numeric_expand2(const Team &tm, const Crew &cw, const Tab &T, const Scr &sc, const double *pts,
+                                     int N, const double *shift, double scale, NumSet A, NumSet B)
+{
+  if (cw.size == 1) { numeric_expand2<NC>(tm, T, sc, pts, N, shift, scale, A, B); return; }
+  cg::cluster_group cl = cg::this_cluster();
+  if (tm.rank == 0) {
+    CrewCmd &c = *cw.cmd;
+    c.op = 2; c.NC = NC; c.N = N; c.pts = pts; c.nscale = scale; c.A = A; c.B = B;
+    c.shift[0] = shift[0]; c.shift[1] = shift[1]; c.shift[2] = shift[2];
+  }
+  cl.sync();
+  numeric_expand2<NC>(tm, T, sc, pts, N, shift, scale, A, B, 0, cw.size, sc.tile);
+  cl.sync();                    // every CTA's partial sums are in its shared memory
+  const double *parts[8];
+  for (int q = 0; q < cw.size && q < 8; q++) parts[q] = cl.map_shared_rank(sc.tile, q);
+  const int NP2 = T.NP * T.NP, nsets = B.w ? 2 : 1;
+  for (int u = tm.rank; u < nsets * NC * NP2; u += tm.size) {
+    double v = 0.0;
+    for (int q = 0; q < cw.size && q < 8; q++) v += parts[q][u];
+    const int set = u / (NC * NP2);
+    (set ? B.out : A.out)[u - set * NC * NP2] = v;
+  }
+  tm.sync();
+}
+
+// helper CTAs: serve the leader's commands until it sends the exit command
+__device__ void crew_serve(const Team &tm, const Crew &cw, const Tab &T, const Scr &sc)
+{
+  cg::cluster_group cl = cg::this_cluster();
+  const CrewCmd *lead = cl.map_shared_rank(cw.cmd, 0);
+  const double2 *lxs = (const double2 *)cl.map_shared_rank(sc.xs, 0);
+  for (;;) {
+    cl.sync();
+    const CrewCmd c = *lead;
+    if (c.op == 1) {
+      for (int i = tm.rank; i < c.D * (c.ld >> 1); i += tm.size) ((double2 *)sc.xs)[i] = lxs[i];
+      tm.sync();
+      int r0, r1;
+      crew_rows(c.NP2, cw.rank, cw.size, r0, r1);
+      imat_apply(tm, c.IMT, c.ld, sc.xs, c.NP2, c.D, r0, r1, c.Y, c.scale);
+    } else if (c.op == 2) {
+      if (c.NC == 1)
+        numeric_expand2<1>(tm, T, sc, c.pts, c.N, c.shift, c.nscale, c.A, c.B, cw.rank, cw.size, sc.tile);
+      else
+        numeric_expand2<3>(tm, T, sc, c.pts, c.N, c.shift, c.nscale, c.A, c.B, cw.rank, cw.size, sc.tile);
+    } else break;
+    cl.sync();
+  }
+  cl.sync();                    // the leader may leave once every helper has read the exit
+}
+
+// leader: release the helpers at the end of the evaluation
+__device__ void crew_finish(const Team &tm, const Crew &cw)
+{
+  if (cw.size == 1) return;
+  cg::cluster_group cl = cg::this_cluster();
+  if (tm.rank == 0) cw.cmd->op = 0;
+  cl.sync();
+  cl.sync();
 }
 
 // ------------------------------------------------------------------ F/H inner solve
@@ -775,7 +895,8 @@ __device__ __forceinline__ void imat_apply(const Team &tm, const double *IMT, in
 // (CSolExpCenter::solveFH, src/expcenter.cpp:1079-1370) for D = 1 (F, H) or
 // D = 3 (x, y, z gradients).  F and H (D*NP2) are updated in place; returns the
 // deviation of H from its value on entry (computeDev2).
-__device__ double solve_fh(const Team &tm, const Tab &T, const TypeView &tv, const SolveParams &prm, const Scr &sc,
+__device__ double solve_fh(const Team &tm, const Crew &cw, const Tab &T, const TypeView &tv, const SolveParams &prm,
+                           const Scr &sc,
                            int ts, int D, double *F, double *H, const double *LF, const double *LH, double *red,
                            int *stats)
 {
@@ -816,7 +937,7 @@ __device__ double solve_fh(const Team &tm, const Tab &T, const TypeView &tv, con
       fx[(k / NP2) * ld + kk] = fbase[k] + cst[CST_H1 * NP + n] * H[k] + cst[CST_F1 * NP + n] * F[k];
     }
     tm.sync();
-    imat_apply(tm, IM, ld, sc.xs, NP2, D, F, T.CONST3);
+    crew_imat_apply(tm, cw, IM, ld, sc.xs, NP2, D, F, T.CONST3);
     tm.sync();
     for (int k = tm.rank; k < len; k += tm.size) {
       const int kk = k % NP2;
@@ -826,7 +947,7 @@ __device__ double solve_fh(const Team &tm, const Tab &T, const TypeView &tv, con
       hx[(k / NP2) * ld + kk] = hbase[k] + cst[CST_H2 * NP + n] * H[k] + cst[CST_F2 * NP + n] * F[k];
     }
     tm.sync();
-    imat_apply(tm, IM, ld, sc.xs, NP2, D, H, cst + CST_INVH * NP);
+    crew_imat_apply(tm, cw, IM, ld, sc.xs, NP2, D, H, cst + CST_INVH * NP);
     tm.sync();
     // computeDev over complex entries (d, n, m)
     double part = 0.0;
@@ -882,6 +1003,7 @@ __device__ double solve_fh(const Team &tm, const Tab &T, const TypeView &tv, con
 struct Sys {
   const Ctx *c;
   int b, NP, NP2, S;
+  Crew cw;
   Scr sc;
   double *red;
   double *tph;
@@ -983,7 +1105,7 @@ __device__ double solve_surface(const Team &tm, const Sys &y, int s, bool rotH)
   const int ts = y.ts(s);
   PhaseClock pc{y.tph, 0};
   pc.start(tm);
-  double dv = solve_fh(tm, T, y.c->tv, y.c->prm, y.sc, ts, 1, y.F(s), y.H(s), y.LFS(s), y.LHS(s), y.red, y.stats());
+  double dv = solve_fh(tm, y.cw, T, y.c->tv, y.c->prm, y.sc, ts, 1, y.F(s), y.H(s), y.LFS(s), y.LHS(s), y.red, y.stats());
   pc.stop(tm, PH_SOLVE);
   pc.start(tm);
   if (rotH) {
@@ -1057,8 +1179,8 @@ __device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s)
       pair_apply_multi(tm, T, y.sc, X, V, false);
       pc.stop(tm, PH_INTRA);
     } else {
-      numeric_expand2<1>(tm, T, y.sc, y.spx(s2), y.npts(s2), P, y.rad(s), NumSet{y.qF(s2), true, false, pF, a},
-                         NumSet{y.qH(s2), true, true, pH, bq});
+      crew_numeric_expand2<1>(tm, y.cw, T, y.sc, y.spx(s2), y.npts(s2), P, y.rad(s),
+                              NumSet{y.qF(s2), true, false, pF, a}, NumSet{y.qH(s2), true, true, pH, bq});
       pc.stop(tm, PH_NUMERIC);
     }
     for (int t = tm.rank; t < y.NP2; t += tm.size) { y.LFS(s)[t] += a[t]; y.LHS(s)[t] += bq[t]; }
@@ -1174,8 +1296,8 @@ __device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int
       pair_apply_multi(tm, T, y.sc, X, V, true);
     } else {
       double *tmpH = y.sc.G(6);
-      numeric_expand2<3>(tm, T, y.sc, y.spx(sm), y.npts(sm), P, y.rad(s), NumSet{y.gFp(sm), true, false, pF, tmpG},
-                         NumSet{y.gHp(sm), true, true, pH, tmpH});
+      crew_numeric_expand2<3>(tm, y.cw, T, y.sc, y.spx(sm), y.npts(sm), P, y.rad(s),
+                              NumSet{y.gFp(sm), true, false, pF, tmpG}, NumSet{y.gHp(sm), true, true, pH, tmpH});
       add_vec_into(tm, LGF, tmpG, 3 * NP2);
       add_vec_into(tm, LGH2, tmpH, 3 * NP2);
     }
@@ -1185,7 +1307,7 @@ __device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int
   double *gF = y.gw(bv.gFw, key), *gHk = y.gw(bv.gHw, key);
   PhaseClock pc{y.tph, 0};
   pc.start(tm);
-  const double dv = solve_fh(tm, T, y.c->tv, y.c->prm, y.sc, ts, 3, gF, gHk, LGF, LGH, y.red, y.stats());
+  const double dv = solve_fh(tm, y.cw, T, y.c->tv, y.c->prm, y.sc, ts, 3, gF, gHk, LGF, LGH, y.red, y.stats());
   pc.stop(tm, PH_SOLVE);
   for (int cc = 0; cc < 3; cc++) rot_apply_xi(tm, mr, gHk + cc * NP2, y.gw(bv.gHrotw, key) + cc * NP2, y.NP, true, y.NP);
   tm.sync();
@@ -1225,16 +1347,13 @@ __device__ double inprod_ml(const double *M, double mscale, const double *L, dou
 }
 
 // ------------------------------------------------------------------ the force kernel
-__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
+// One system (the crew leader's part): CMolecule::computeForces.
+__device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b, void *dsm, double *red)
 {
-  extern __shared__ double2 dsm[];
-  __shared__ double red[PBSAM_TEAM];
-  const Team tm{(int)threadIdx.x, (int)blockDim.x};
   const BatchView &bv = c.bv;
-  const int b = blockIdx.x;
-  if (b >= bv.B) return;
   Sys y;
   y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = bv.S;
+  y.cw = cw;
   y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP, dsm);
   y.red = red;
   y.tph = bv.tphase + (size_t)b * 8;
@@ -1244,6 +1363,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
   if (tm.rank == 0) {
     for (int k = 0; k < 8; k++) st[k] = 0;
     for (int k = 0; k < 8; k++) y.tph[k] = 0.0;
+    st[5] = cw.size;
     bv.status[b] = PBSAM_STATUS_OK;
   }
   total.start(tm);
@@ -1519,6 +1639,25 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
   total.stop(tm, PH_TOTAL);
 }
 
+// Grid: n_systems crews of cluster-size CTAs (a plain launch is a crew of one).
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
+{
+  extern __shared__ double2 dsm[];
+  __shared__ double red[PBSAM_TEAM];
+  __shared__ CrewCmd cmd;
+  const Team tm{(int)threadIdx.x, (int)blockDim.x};
+  cg::cluster_group cl = cg::this_cluster();
+  const Crew cw{(int)cl.block_rank(), (int)cl.num_blocks(), &cmd};
+  const int b = blockIdx.x / cw.size;
+  if (b >= c.bv.B) return;                 // whole crews only: the grid is n_systems * size
+  if (cw.rank != 0) {
+    crew_serve(tm, cw, c.T, make_scr(c.bv.scr + (size_t)b * c.bv.scr_stride, c.T.NP, dsm));
+    return;
+  }
+  forces_body(tm, c, cw, b, dsm, red);
+  crew_finish(tm, cw);
+}
+
 // interaction energy with the reference's convention (unrotated centres and
 // molecule-frame H, src/moldynamics.cpp:358-386, src/molecule.cpp:1850-1890)
 __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c)
@@ -1531,6 +1670,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c)
   if (b >= bv.B) return;
   Sys y;
   y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = bv.S;
+  y.cw = Crew{0, 1, nullptr};
   y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP, dsm);
   y.red = red;
   y.tph = nullptr;

@@ -108,17 +108,13 @@ __global__ void imat_assemble_kernel(Tab T, const double *G, const double *Gs, i
 // polarize_self (src/molecule.cpp:1898-1979) for a system of one molecule, starting
 // from F = 0 and H = the multipole expansion of the charges assigned to each
 // sphere (src/expcenter.cpp:88-103, 541-545, 576-587).
-__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_selfpol_kernel(Ctx c, const double *Eass, int max_rounds,
-                                                                  int *rounds_out)
+__device__ void selfpol_body(const Team &tm, const Ctx &c, const Crew &cw, int b, void *dsm, double *red,
+                             const double *Eass, int max_rounds, int *rounds_out)
 {
-  extern __shared__ double2 dsm[];
-  __shared__ double red[PBSAM_TEAM];
-  const Team tm{(int)threadIdx.x, (int)blockDim.x};
   const BatchView &bv = c.bv;
-  const int b = blockIdx.x;
-  if (b >= bv.B) return;
   Sys y;
   y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = bv.S;
+  y.cw = cw;
   y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP, dsm);
   y.red = red;
   y.tph = bv.tphase + (size_t)b * PH_N;
@@ -165,6 +161,26 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_selfpol_kernel(Ctx c, const 
     ct++;
   }
   if (tm.rank == 0) rounds_out[b] = ct;
+}
+
+// Grid: one crew of cluster-size CTAs per system (a plain launch is a crew of one).
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_selfpol_kernel(Ctx c, const double *Eass, int max_rounds,
+                                                                  int *rounds_out)
+{
+  extern __shared__ double2 dsm[];
+  __shared__ double red[PBSAM_TEAM];
+  __shared__ CrewCmd cmd;
+  const Team tm{(int)threadIdx.x, (int)blockDim.x};
+  cg::cluster_group cl = cg::this_cluster();
+  const Crew cw{(int)cl.block_rank(), (int)cl.num_blocks(), &cmd};
+  const int b = blockIdx.x / cw.size;
+  if (b >= c.bv.B) return;
+  if (cw.rank != 0) {
+    crew_serve(tm, cw, c.T, make_scr(c.bv.scr + (size_t)b * c.bv.scr_stride, c.T.NP, dsm));
+    return;
+  }
+  selfpol_body(tm, c, cw, b, dsm, red, Eass, max_rounds, rounds_out);
+  crew_finish(tm, cw);
 }
 
 }  // namespace pbsam
