@@ -226,7 +226,9 @@ def run_ours(args):
             "systems_ok": int(np.sum(status == 0)),
             "inner_iterations_per_step": int(np.sum(stats[:, 1])),
             "slowest_system_phase_ms": dict(zip(
-                ["solve", "surface", "numeric", "intra", "LS", "DTA", "grad_reexp", "total"],
+                ["solve", "surface", "numeric", "intra", "LS", "DTA", "grad_reexp", "total", "grad_surface",
+                 "setup", "grad_book", "forces", "grad_reexp_inter", "grad_reexp_analytic", "grad_reexp_numeric",
+                 "solve_matvec"],
                 [round(float(x), 1) for x in phases[int(np.argmax(phases[:, 7]))]])),
             "prep_s": round(prep_s, 1), "prep": prep_t,
         }

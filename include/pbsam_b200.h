@@ -118,12 +118,16 @@ int pbsam_system_stats(const pbsam_system *sys, int *stats);
  * calls above synchronise it before returning host results. */
 int pbsam_system_set_stream(pbsam_system *sys, void *stream);
 
-/* Device time per phase of the last force evaluation (or self-polarization), 8
+/* Device time per phase of the last force evaluation (or self-polarization), 16
  * doubles per system in ms: [0] F/H solves, [1] surface charges, [2] numeric
  * near-field re-expansions, [3] analytic intra re-expansions, [4] inter-molecular
  * LS re-expansions, [5] gradient re-expansions of H (DTA), [6] re-expansions of
  * the gradient solves (inter and intra, before each gradient F/H solve), [7] whole
- * evaluation.  [0]-[6] do not overlap; [7] includes everything. */
+ * evaluation, [8] gradient surface charges and rotation of the gradient H,
+ * [9] set-up (pair lists, molecule rotations), [10] gradient-phase bookkeeping,
+ * [11] force and torque sums; sub-phases: [12]-[14] the inter, intra analytic and
+ * intra numeric parts of [6], [15] the IMat products within [0].  The phases
+ * [0]-[6] and [8]-[11] do not overlap; [7] includes everything. */
 int pbsam_system_phase_ms(const pbsam_system *sys, double *ms);
 
 /* Device time in milliseconds of the last force-kernel launch (CUDA events). */

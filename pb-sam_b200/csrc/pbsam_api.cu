@@ -661,11 +661,13 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   chk(dalloc(Bf, &bv.molR, (size_t)B * n_mol * rot_off(2 * NP - 1)));
   chk(dalloc(Bf, &bv.molRS, B * n_mol * 16));
   chk(dalloc(Bf, &bv.sep, B * S * S));
+  s->crew = pick_crew(pbsam_forces_kernel, B, team_smem_bytes(NP), c->prm.cluster_size);
+  bv.crew = s->crew;
   bv.scr_stride = scr_doubles(NP, S);
-  chk(dalloc(Bf, &bv.scr, (size_t)B * bv.scr_stride));
+  chk(dalloc(Bf, &bv.scr, (size_t)B * s->crew * bv.scr_stride));
   chk(dalloc(Bf, &bv.force, B * n_mol * 3)); chk(dalloc(Bf, &bv.torque, B * n_mol * 3));
   chk(dalloc(Bf, &bv.energy, B)); chk(dalloc(Bf, &bv.status, B)); chk(dalloc(Bf, &bv.stats, B * 8));
-  chk(dalloc(Bf, &bv.tphase, B * 8));
+  chk(dalloc(Bf, &bv.tphase, B * PH_N));
   if (r) {
     for (void *p : Bf) cudaFree(p);
     delete s;
@@ -679,7 +681,6 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   p.min_sep_numeric = c->prm.min_sep_numeric; p.idiel = c->prm.idiel; p.sdiel = c->prm.sdiel;
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);
-  s->crew = pick_crew(pbsam_forces_kernel, B, team_smem_bytes(NP), c->prm.cluster_size);
   c->live_systems++;
   *out = s;
   return pbsam_system_reset(s);
@@ -890,10 +891,8 @@ extern "C" int pbsam_selfpol(pbsam_context *c, int type_id, int max_rounds, doub
   TRY(pbsam_system_create(c, 1, 1, mt, &s));
   int *drounds = nullptr;
   if (cudaMalloc(&drounds, sizeof(int)) != cudaSuccess) { pbsam_system_destroy(s); return fail(PBSAM_E_NOMEM, "rounds"); }
-  const size_t sp_smem = team_smem_bytes(c->prm.poles);
-  const int sp_crew = pick_crew(pbsam_selfpol_kernel, 1, sp_smem, c->prm.cluster_size);
-  cudaError_t e = launch_crews(pbsam_selfpol_kernel, 1, sp_crew, sp_smem, s->stream, s->c, (const double *)c->tv.Eass,
-                               max_rounds, drounds);
+  cudaError_t e = launch_crews(pbsam_selfpol_kernel, 1, s->crew, team_smem_bytes(c->prm.poles), s->stream, s->c,
+                               (const double *)c->tv.Eass, max_rounds, drounds);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   const int ns = c->types[type_id].ns, NP2 = c->prm.poles * c->prm.poles;
@@ -915,8 +914,8 @@ extern "C" int pbsam_system_phase_ms(const pbsam_system *s, double *ms)
 {
   if (!s || !ms) return fail(PBSAM_E_BADARG, "null argument");
   CK(cudaSetDevice(s->ctx->device));
-  CK(cudaMemcpy(ms, s->c.bv.tphase, (size_t)s->B * 8 * sizeof(double), cudaMemcpyDeviceToHost));
-  for (int i = 0; i < s->B * 8; i++) ms[i] *= 1e-6;
+  CK(cudaMemcpy(ms, s->c.bv.tphase, (size_t)s->B * PH_N * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < s->B * PH_N; i++) ms[i] *= 1e-6;
   return PBSAM_OK;
 }
 

@@ -115,8 +115,15 @@ __device__ Scr make_scr(double *base, int NP, void *smem)
   return s;
 }
 
+// scratch block of CTA `rank` of system b's crew
+__device__ __forceinline__ double *scr_of(const BatchView &bv, int b, int rank)
+{
+  return bv.scr + ((size_t)b * bv.crew + rank) * bv.scr_stride;
+}
+
 // ------------------------------------------------------------------ phase timers
-enum { PH_SOLVE = 0, PH_SURF, PH_NUMERIC, PH_INTRA, PH_LS, PH_DTA, PH_GRX, PH_TOTAL, PH_N };
+enum { PH_SOLVE = 0, PH_SURF, PH_NUMERIC, PH_INTRA, PH_LS, PH_DTA, PH_GRX, PH_TOTAL, PH_GSURF, PH_SETUP, PH_GBOOK,
+       PH_FORCE, PH_GX_INTER, PH_GX_ANALYTIC, PH_GX_NUMERIC, PH_MATVEC, PH_N = 16 };
 __device__ __forceinline__ unsigned long long gtimer()
 {
   unsigned long long t;
@@ -393,7 +400,7 @@ __device__ void trans_apply_multi(const Team &tm, const PairXf &X, const double 
   }
 }
 
-__device__ void pair_apply_multi(const Team &tm, const Tab &T, const Scr &sc, const PairXf &X, const MultiVec &V,
+__device__ __noinline__ void pair_apply_multi(const Team &tm, const Tab &T, const Scr &sc, const PairXf &X, const MultiVec &V,
                                  bool accumulate)
 {
   int pv[PBSAM_MV];
@@ -515,7 +522,7 @@ __device__ __forceinline__ void radial_factors(const Tab &T, double rho, double 
 }
 
 template <int NC>
-__device__ void numeric_expand2(const Team &tm, const Tab &T, const Scr &sc, const double *pts, int N,
+__device__ __noinline__ void numeric_expand2(const Team &tm, const Tab &T, const Scr &sc, const double *pts, int N,
                                 const double *shift, double scale, NumSet A, NumSet B, int part_rank = 0,
                                 int part_size = 1, double *part = nullptr)
 {
@@ -647,49 +654,73 @@ __device__ void numeric_expand(const Team &tm, const Tab &T, const Scr &sc, cons
 
 // ------------------------------------------------------------------ surface charges
 // q[h] = dA * sum_n (2 sum_{m>0} E(n,m) Y(n,m) c_n + E(n,0) Y(n,0) c_n) at each
-// exposed point (computeExposedSurfaceChargesFH, src/expcenter.cpp:1419-1440);
-// returns sum |q| over the points.  NC expansions E (stride NP2) share the
-// points and the per-degree factors c; q is written as q[NC*h + k].
+// exposed point (computeExposedSurfaceChargesFH, src/expcenter.cpp:1419-1440),
+// with sum |q| over the points.  Two sets share the points (the F and H expansions
+// of a sphere, or their gradients): set 1 from E1 with per-degree factors c1 into
+// q1, set 2 (optional, E2 != nullptr) from E2/c2 into q2; NC expansions per set
+// (stride NP2), q written as q[NC*h + k].  The weights (m > 0 ? 2 : 1) * c_n * E
+// are staged in shared memory; this CTA takes points rank*team + t, strided by
+// size*team, and its |q| sums are reduced over the team into tot1 / tot2.
 template <int NC>
-__device__ void surface_q(const Team &tm, const Tab &T, const double *pts, int N, double dA, const double *E,
-                          const double *cdeg, double *q, double *tot, double *red)
+__device__ __noinline__ void surface_q2(const Team &tm, const Tab &T, const Scr &sc, const double *pts, int N, double dA,
+                           const double *E1, const double *c1, double *q1, const double *E2, const double *c2,
+                           double *q2, int rank, int size, double *tot1, double *tot2, double *red)
 {
   const int NP = T.NP, NP2 = NP * NP;
-  double ta[NC];
-  for (int k = 0; k < NC; k++) ta[k] = 0.0;
-  for (int h = tm.rank; h < N; h += tm.size) {
+  const bool two = E2 != nullptr;
+  double *W = sc.tile;
+  for (int u = tm.rank; u < (two ? 2 : 1) * NC * NP2; u += tm.size) {
+    const int set = u / (NC * NP2), r = u - set * NC * NP2, c = r % NP2;
+    int n = (int)sqrt((double)c);
+    while (n * n > c) n--;
+    while ((n + 1) * (n + 1) <= c) n++;
+    const double *E = set ? E2 : E1;
+    const double *cd = set ? c2 : c1;
+    W[u] = ((c - n * n > 0) ? 2.0 : 1.0) * (cd[n] * E[r]);
+  }
+  tm.sync();
+  double ta1[NC], ta2[NC];
+#pragma unroll
+  for (int k = 0; k < NC; k++) { ta1[k] = 0.0; ta2[k] = 0.0; }
+  for (int h = rank * tm.size + tm.rank; h < N; h += size * tm.size) {
     const Sph s = cart2sph(pts[3 * h], pts[3 * h + 1], pts[3 * h + 2]);
     double st, ct;
     sincos(s.theta, &st, &ct);
-    double sn[NC][32], t0[NC][32];
-    for (int k = 0; k < NC; k++)
-      for (int n = 0; n < NP; n++) { sn[k][n] = 0.0; t0[k][n] = 0.0; }
+    double a1[NC], a2[NC];
+#pragma unroll
+    for (int k = 0; k < NC; k++) { a1[k] = 0.0; a2[k] = 0.0; }
     for (int m = 0; m < NP; m++) {
       sh_column(T, ct, st, s.phi, m, NP, [&](int n, double re, double im) {
-        const double c = cdeg[n];
+        const int i0 = IDX(n) + (m ? 2 * m - 1 : 0);
+#pragma unroll
         for (int k = 0; k < NC; k++) {
-          const double *Ek = E + (size_t)k * NP2 + IDX(n);
-          if (m == 0) t0[k][n] = Ek[0] * (re * c);
-          else {
-            sn[k][n] += Ek[2 * m - 1] * (re * c);
-            sn[k][n] += Ek[2 * m] * (im * c);
+          const double *w = W + (size_t)k * NP2 + i0;
+          a1[k] += (m ? w[0] * re + w[1] * im : w[0] * re);
+          if (two) {
+            const double *w2 = W + (size_t)(NC + k) * NP2 + i0;
+            a2[k] += (m ? w2[0] * re + w2[1] * im : w2[0] * re);
           }
         }
       });
     }
+#pragma unroll
     for (int k = 0; k < NC; k++) {
-      double sum = 0.0;
-      for (int n = 0; n < NP; n++) {
-        double v = sn[k][n] * 2.0;
-        v += t0[k][n];
-        sum += v;
+      const double v1 = a1[k] * dA;
+      q1[NC * h + k] = v1;
+      ta1[k] += fabs(v1);
+      if (two) {
+        const double v2 = a2[k] * dA;
+        q2[NC * h + k] = v2;
+        ta2[k] += fabs(v2);
       }
-      const double qq = sum * dA;
-      q[NC * h + k] = qq;
-      ta[k] += fabs(qq);
     }
   }
-  for (int k = 0; k < NC; k++) tot[k] = team_sum(tm, ta[k], red);
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    tot1[k] = team_sum(tm, ta1[k], red);
+    const double t2 = two ? team_sum(tm, ta2[k], red) : 0.0;
+    if (tot2) tot2[k] = t2;
+  }
 }
 
 // ------------------------------------------------------------------ IMat product
@@ -701,7 +732,7 @@ __device__ void surface_q(const Team &tm, const Tab &T, const double *pts, int N
 // blocks per step, so 128 bytes per lane are in flight; the D operands share every
 // loaded IMat element.  The row sums are reduced across the warp in a fixed order.
 template <int D>
-__device__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const double *x, int NP2, int r_begin, int r_end,
+__device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const double *x, int NP2, int r_begin, int r_end,
                              double *Y, const double *scale)
 {
   const int lane = tm.rank & 31, warp = tm.rank >> 5, nw = tm.size >> 5;
@@ -795,6 +826,11 @@ struct CrewCmd {
   const double *pts;
   double shift[3], nscale;
   NumSet A, B;
+  int s, self, filter_mol, use_ipol, use_iact;   // gradient re-expansion list (DTA)
+  double *acc;
+  const double *E1, *c1, *E2, *c2;               // surface charges
+  double *q1, *q2, dA;
+  double ptot[6];         // a helper's |q| sums (read by the leader)
 };
 struct Crew {
   int rank, size;         // CTA rank in the cluster, CTAs per system
@@ -854,30 +890,39 @@ __device__ void crew_numeric_expand2(const Team &tm, const Crew &cw, const Tab &
   tm.sync();
 }
 
-// helper CTAs: serve the leader's commands until it sends the exit command
-__device__ void crew_serve(const Team &tm, const Crew &cw, const Tab &T, const Scr &sc)
+// Surface charges (surface_q2) shared by the crew: points split over the CTAs,
+// |q| sums added in rank order.
+template <int NC>
+__device__ void crew_surface_q2(const Team &tm, const Crew &cw, const Tab &T, const Scr &sc, double *red,
+                                const double *pts, int N, double dA, const double *E1, const double *c1, double *q1,
+                                double *tot1, const double *E2, const double *c2, double *q2, double *tot2)
 {
-  cg::cluster_group cl = cg::this_cluster();
-  const CrewCmd *lead = cl.map_shared_rank(cw.cmd, 0);
-  const double2 *lxs = (const double2 *)cl.map_shared_rank(sc.xs, 0);
-  for (;;) {
-    cl.sync();
-    const CrewCmd c = *lead;
-    if (c.op == 1) {
-      for (int i = tm.rank; i < c.D * (c.ld >> 1); i += tm.size) ((double2 *)sc.xs)[i] = lxs[i];
-      tm.sync();
-      int r0, r1;
-      crew_rows(c.NP2, cw.rank, cw.size, r0, r1);
-      imat_apply(tm, c.IMT, c.ld, sc.xs, c.NP2, c.D, r0, r1, c.Y, c.scale);
-    } else if (c.op == 2) {
-      if (c.NC == 1)
-        numeric_expand2<1>(tm, T, sc, c.pts, c.N, c.shift, c.nscale, c.A, c.B, cw.rank, cw.size, sc.tile);
-      else
-        numeric_expand2<3>(tm, T, sc, c.pts, c.N, c.shift, c.nscale, c.A, c.B, cw.rank, cw.size, sc.tile);
-    } else break;
-    cl.sync();
+  if (cw.size == 1) {
+    surface_q2<NC>(tm, T, sc, pts, N, dA, E1, c1, q1, E2, c2, q2, 0, 1, tot1, tot2, red);
+    return;
   }
-  cl.sync();                    // the leader may leave once every helper has read the exit
+  cg::cluster_group cl = cg::this_cluster();
+  if (tm.rank == 0) {
+    CrewCmd &c = *cw.cmd;
+    c.op = 5; c.NC = NC; c.pts = pts; c.N = N; c.dA = dA;
+    c.E1 = E1; c.c1 = c1; c.q1 = q1; c.E2 = E2; c.c2 = c2; c.q2 = q2;
+  }
+  cl.sync();
+  double t1[NC], t2[NC];
+  surface_q2<NC>(tm, T, sc, pts, N, dA, E1, c1, q1, E2, c2, q2, 0, cw.size, t1, t2, red);
+  cl.sync();                    // helpers' charges written, their sums in their command blocks
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    double a = t1[k], b = t2[k];
+    for (int q = 1; q < cw.size; q++) {
+      const CrewCmd *r = cl.map_shared_rank(cw.cmd, q);
+      a += r->ptot[k];
+      b += r->ptot[3 + k];
+    }
+    tot1[k] = a;
+    if (tot2) tot2[k] = b;
+  }
+  tm.sync();
 }
 
 // leader: release the helpers at the end of the evaluation
@@ -895,8 +940,8 @@ __device__ void crew_finish(const Team &tm, const Crew &cw)
 // (CSolExpCenter::solveFH, src/expcenter.cpp:1079-1370) for D = 1 (F, H) or
 // D = 3 (x, y, z gradients).  F and H (D*NP2) are updated in place; returns the
 // deviation of H from its value on entry (computeDev2).
-__device__ double solve_fh(const Team &tm, const Crew &cw, const Tab &T, const TypeView &tv, const SolveParams &prm,
-                           const Scr &sc,
+__device__ double solve_fh(const Team &tm, const Crew &cw, double *tph, const Tab &T, const TypeView &tv,
+                           const SolveParams &prm, const Scr &sc,
                            int ts, int D, double *F, double *H, const double *LF, const double *LH, double *red,
                            int *stats)
 {
@@ -937,6 +982,8 @@ __device__ double solve_fh(const Team &tm, const Crew &cw, const Tab &T, const T
       fx[(k / NP2) * ld + kk] = fbase[k] + cst[CST_H1 * NP + n] * H[k] + cst[CST_F1 * NP + n] * F[k];
     }
     tm.sync();
+    PhaseClock mv{tph, 0};
+    mv.start(tm);
     crew_imat_apply(tm, cw, IM, ld, sc.xs, NP2, D, F, T.CONST3);
     tm.sync();
     for (int k = tm.rank; k < len; k += tm.size) {
@@ -948,6 +995,7 @@ __device__ double solve_fh(const Team &tm, const Crew &cw, const Tab &T, const T
     }
     tm.sync();
     crew_imat_apply(tm, cw, IM, ld, sc.xs, NP2, D, H, cst + CST_INVH * NP);
+    mv.stop(tm, PH_MATVEC);
     tm.sync();
     // computeDev over complex entries (d, n, m)
     double part = 0.0;
@@ -1105,7 +1153,7 @@ __device__ double solve_surface(const Team &tm, const Sys &y, int s, bool rotH)
   const int ts = y.ts(s);
   PhaseClock pc{y.tph, 0};
   pc.start(tm);
-  double dv = solve_fh(tm, y.cw, T, y.c->tv, y.c->prm, y.sc, ts, 1, y.F(s), y.H(s), y.LFS(s), y.LHS(s), y.red, y.stats());
+  double dv = solve_fh(tm, y.cw, y.tph, T, y.c->tv, y.c->prm, y.sc, ts, 1, y.F(s), y.H(s), y.LFS(s), y.LHS(s), y.red, y.stats());
   pc.stop(tm, PH_SOLVE);
   pc.start(tm);
   if (rotH) {
@@ -1114,10 +1162,10 @@ __device__ double solve_surface(const Team &tm, const Sys &y, int s, bool rotH)
   }
   const double *cst = y.c->tv.cst + (size_t)ts * CST_N * y.NP;
   const double dA = 4 * PB_PI / double(y.c->tv.nspx[ts]);
-  double tot[1];
-  surface_q<1>(tm, T, y.spx(s), y.npts(s), dA, y.F(s), T.CONST2, y.qF(s), tot, y.red);
-  double tF = tot[0];
-  surface_q<1>(tm, T, y.spx(s), y.npts(s), dA, y.H(s), cst + CST_CHGH * y.NP, y.qH(s), tot, y.red);
+  double totF[1], tot[1];
+  crew_surface_q2<1>(tm, y.cw, T, y.sc, y.red, y.spx(s), y.npts(s), dA, y.F(s), T.CONST2, y.qF(s), totF, y.H(s),
+                     cst + CST_CHGH * y.NP, y.qH(s), tot);
+  double tF = totF[0];
   pc.stop(tm, PH_SURF);
   if (tm.rank == 0) {
     y.c->bv.tF[y.sc1(s)] = tF;
@@ -1200,11 +1248,9 @@ __device__ double recompute(const Team &tm, const Sys &y, int s)             // 
 }
 
 // gradient re-expansion of neighbour m's rotated H into sphere s, accumulated in acc (3*NP2)
-__device__ void grad_xform_from(const Team &tm, const Sys &y, int s, int sm, bool self, double *acc)
+__device__ __noinline__ void grad_xform_from(const Team &tm, const Sys &y, int s, int sm, bool self, double *acc)
 {
   const Tab &T = y.c->T;
-  PhaseClock pc{y.tph, 0};
-  pc.start(tm);
   double ci[3], cm[3];
   y.cen_lab(s, ci);
   y.cen_lab(sm, cm);
@@ -1217,6 +1263,62 @@ __device__ void grad_xform_from(const Team &tm, const Sys &y, int s, int sm, boo
   double *G = y.sc.G(0);
   pair_apply_grad(tm, T, y.sc, X, self ? y.HselfRot(sm) : y.Hrot(sm), G);
   add_vec_into(tm, acc, G, 3 * y.NP2);
+}
+
+// This CTA's share of a list of gradient re-expansions into sphere s: the
+// neighbours of s's polarization list (use_ipol) then of its interaction list
+// (use_iact), optionally only those of molecule filter_mol; entries rank,
+// rank + size, ... are summed into part (3 * NP2, zeroed here).
+__device__ void dta_share(const Team &tm, const Sys &y, int s, bool self, int filter_mol, bool use_ipol, bool use_iact,
+                          int rank, int size, double *part)
+{
+  tzero(tm, part, 3 * y.NP2);
+  tm.sync();
+  const int n1 = use_ipol ? y.nipol(s) : 0, n2 = use_iact ? y.niact(s) : 0;
+  for (int e = rank; e < n1 + n2; e += size) {
+    const int sm = e < n1 ? y.ipol(s)[e] : y.iact(s)[e - n1];
+    if (filter_mol >= 0 && y.mol(sm) != filter_mol) continue;
+    grad_xform_from(tm, y, s, sm, self, part);
+  }
+}
+
+// acc (3 * NP2) += the gradient re-expansions of that list (prepareDTA /
+// prepareDTA_iself, src/molecule.cpp:1483-1628), shared by the crew: each CTA sums
+// its share in its own scratch, the leader adds the shares in rank order.
+__device__ void crew_dta(const Team &tm, const Sys &y, int s, bool self, int filter_mol, bool use_ipol, bool use_iact,
+                         double *acc)
+{
+  PhaseClock pc{y.tph, 0};
+  pc.start(tm);
+  const Crew &cw = y.cw;
+  if (cw.size == 1) {
+    const int n1 = use_ipol ? y.nipol(s) : 0, n2 = use_iact ? y.niact(s) : 0;
+    for (int e = 0; e < n1 + n2; e++) {
+      const int sm = e < n1 ? y.ipol(s)[e] : y.iact(s)[e - n1];
+      if (filter_mol >= 0 && y.mol(sm) != filter_mol) continue;
+      grad_xform_from(tm, y, s, sm, self, acc);
+    }
+    pc.stop(tm, PH_DTA);
+    return;
+  }
+  cg::cluster_group cl = cg::this_cluster();
+  if (tm.rank == 0) {
+    CrewCmd &c = *cw.cmd;
+    c.op = 3; c.s = s; c.self = self ? 1 : 0; c.filter_mol = filter_mol;
+    c.use_ipol = use_ipol ? 1 : 0; c.use_iact = use_iact ? 1 : 0; c.acc = acc;
+  }
+  cl.sync();
+  dta_share(tm, y, s, self, filter_mol, use_ipol, use_iact, 0, cw.size, y.sc.G(7));
+  cl.sync();                    // every CTA's share is in its scratch
+  const BatchView &bv = y.c->bv;
+  const int n = 3 * y.NP2;
+  const size_t off = (size_t)(y.sc.G(7) - scr_of(bv, y.b, 0));
+  for (int i = tm.rank; i < n; i += tm.size) {
+    double v = acc[i];
+    for (int q = 0; q < cw.size; q++) v += scr_of(bv, y.b, q)[off + i];
+    acc[i] = v;
+  }
+  tm.sync();
   pc.stop(tm, PH_DTA);
 }
 
@@ -1225,49 +1327,44 @@ __device__ void prepare_dta_iself(const Team &tm, const Sys &y, int s)     // sr
   double *acc = y.gLHN(s);
   tzero(tm, acc, 3 * y.NP2);
   tm.sync();
-  for (int e = 0; e < y.nipol(s); e++) grad_xform_from(tm, y, s, y.ipol(s)[e], true, acc);
-  for (int e = 0; e < y.niact(s); e++) grad_xform_from(tm, y, s, y.iact(s)[e], true, acc);
+  crew_dta(tm, y, s, true, -1, true, true, acc);
 }
 
-// one gradient recompute of sphere s w.r.t. molecule j (src/molecule.cpp:1680-1843)
-__device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int key)
+// This CTA's share of the analytic re-expansions that feed one gradient solve of
+// sphere s w.r.t. molecule j (reexpandGrad / reexpandIntraGrad, src/molecule.cpp:
+// 1681-1802).  kind 0: the rotated gradient H of the inter-molecular neighbours
+// into out0 (tGrot); kind 1: the gradient F and H of the intra list's analytic
+// pairs into out0 (LGF) and out1 (LGH2).  Entries counted in list order, this CTA
+// taking every size-th from rank; contributions are added to the outputs.
+__device__ __noinline__ void grad_share(const Team &tm, const Sys &y, int s, int j, int kind, int rank, int size, double *out0,
+                           double *out1)
 {
   const Tab &T = y.c->T;
   const BatchView &bv = y.c->bv;
   const int NP2 = y.NP2, i = y.mol(s), ts = y.ts(s);
-  double *tGrot = y.sc.G(1), *LGH = y.sc.G(2), *LGF = y.sc.G(3), *LGH2 = y.sc.G(4), *tmpG = y.sc.G(5);
-  double *tL = y.sc.E(7);
-  PhaseClock gx{y.tph, 0};
-  gx.start(tm);
-  tcopy(tm, tGrot, y.gw(bv.tGw, key), 3 * NP2);
-  tm.sync();
-  double ci[3];
-  y.cen_lab(s, ci);
-  for (int e = 0; e < y.nipol(s); e++) {
-    const int sm = y.ipol(s)[e];
-    if (i != j && y.mol(sm) != j) continue;
-    double cm[3];
-    y.cen_lab(sm, cm);
-    const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
-    const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
-    const int p = compute_order(y.NP, rho, bv.maxgH[y.sc1(sm)], y.rad(sm));
-    PairXf X;
-    prep_pair(tm, T, y.sc, P, p, 0, y.rad(sm), y.rad(s), false, X);
-    const double *src = y.gw(bv.gHrotw, bv.gkey[y.sc1(sm)]);
-    MultiVec V;
-    V.n = 3;
-    for (int cc = 0; cc < 3; cc++) { V.in[cc] = src + cc * NP2; V.out[cc] = tGrot + cc * NP2; V.useF[cc] = false; }
-    pair_apply_multi(tm, T, y.sc, X, V, true);
+  int cnt = 0;
+  if (kind == 0) {
+    double ci[3];
+    y.cen_lab(s, ci);
+    for (int e = 0; e < y.nipol(s); e++) {
+      const int sm = y.ipol(s)[e];
+      if (i != j && y.mol(sm) != j) continue;
+      if ((cnt++ % size) != rank) continue;
+      double cm[3];
+      y.cen_lab(sm, cm);
+      const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+      const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+      const int p = compute_order(y.NP, rho, bv.maxgH[y.sc1(sm)], y.rad(sm));
+      PairXf X;
+      prep_pair(tm, T, y.sc, P, p, 0, y.rad(sm), y.rad(s), false, X);
+      const double *src = y.gw(bv.gHrotw, bv.gkey[y.sc1(sm)]);
+      MultiVec V;
+      V.n = 3;
+      for (int cc = 0; cc < 3; cc++) { V.in[cc] = src + cc * NP2; V.out[cc] = out0 + cc * NP2; V.useF[cc] = false; }
+      pair_apply_multi(tm, T, y.sc, X, V, true);
+    }
+    return;
   }
-  const RotState mr = y.molrot(i);
-  for (int cc = 0; cc < 3; cc++) rot_apply_xi(tm, mr, tGrot + cc * NP2, LGH + cc * NP2, y.NP, false, y.NP);
-  tm.sync();
-  if (j == i) { tcopy(tm, y.gLHN(s), LGH, 3 * NP2); tm.sync(); }
-  tzero(tm, LGF, 3 * NP2);
-  tzero(tm, LGH2, 3 * NP2);
-  tm.sync();
-  // intra list of the gradient: molecule j's polarized spheres (i == j) or
-  // i's spheres polarized by j (i != j)
   const int nlist = (i == j) ? bv.intraPol_n[(size_t)y.b * bv.nmol + j] : bv.interMol_n[(size_t)y.b * bv.nmol + j];
   const int *lst = (i == j) ? bv.intraPol + ((size_t)y.b * bv.nmol + j) * y.S : bv.interMol + ((size_t)y.b * bv.nmol + j) * y.S;
   const double *cis = y.cen(s);
@@ -1280,43 +1377,120 @@ __device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int
     const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
     const double rm = y.rad(sm);
     const double sep = rho - y.rad(s) - rm;
+    if (!(sep > 0 && !(sep < y.c->prm.min_sep_numeric))) continue;
+    if ((cnt++ % size) != rank) continue;
     const int pF = compute_order(y.NP, rho, bv.maxgF[y.sc1(sm)], rm);
     const int pH = compute_order(y.NP, rho, bv.maxgH[y.sc1(sm)], rm);
-    if (sep > 0 && !(sep < y.c->prm.min_sep_numeric)) {
-      PairXf X;
-      table_pair(tm, T, y.c->tv, y.sc, intra_pair(y.c->tv, ts, s - bv.mol_off[i], sm - bv.mol_off[i]), pH, pF, rm,
-                 y.rad(s), X);
-      const int km = bv.gkey[y.sc1(sm)];
-      MultiVec V;
-      V.n = 6;
-      for (int cc = 0; cc < 3; cc++) {
-        V.in[cc] = y.gw(bv.gFw, km) + cc * NP2; V.out[cc] = LGF + cc * NP2; V.useF[cc] = true;
-        V.in[3 + cc] = y.gw(bv.gHw, km) + cc * NP2; V.out[3 + cc] = LGH2 + cc * NP2; V.useF[3 + cc] = false;
-      }
-      pair_apply_multi(tm, T, y.sc, X, V, true);
-    } else {
-      double *tmpH = y.sc.G(6);
-      crew_numeric_expand2<3>(tm, y.cw, T, y.sc, y.spx(sm), y.npts(sm), P, y.rad(s),
-                              NumSet{y.gFp(sm), true, false, pF, tmpG}, NumSet{y.gHp(sm), true, true, pH, tmpH});
-      add_vec_into(tm, LGF, tmpG, 3 * NP2);
-      add_vec_into(tm, LGH2, tmpH, 3 * NP2);
+    PairXf X;
+    table_pair(tm, T, y.c->tv, y.sc, intra_pair(y.c->tv, ts, s - bv.mol_off[i], sm - bv.mol_off[i]), pH, pF, rm,
+               y.rad(s), X);
+    const int km = bv.gkey[y.sc1(sm)];
+    MultiVec V;
+    V.n = 6;
+    for (int cc = 0; cc < 3; cc++) {
+      V.in[cc] = y.gw(bv.gFw, km) + cc * NP2; V.out[cc] = out0 + cc * NP2; V.useF[cc] = true;
+      V.in[3 + cc] = y.gw(bv.gHw, km) + cc * NP2; V.out[3 + cc] = out1 + cc * NP2; V.useF[3 + cc] = false;
+    }
+    pair_apply_multi(tm, T, y.sc, X, V, true);
+  }
+}
+
+// grad_share over the whole crew: the leader adds its share straight into the
+// outputs, each helper into zeroed buffers of its own scratch, which the leader
+// then adds in rank order.
+__device__ void crew_grad(const Team &tm, const Sys &y, int s, int j, int kind, double *out0, double *out1)
+{
+  const Crew &cw = y.cw;
+  if (cw.size == 1) { grad_share(tm, y, s, j, kind, 0, 1, out0, out1); return; }
+  cg::cluster_group cl = cg::this_cluster();
+  if (tm.rank == 0) {
+    CrewCmd &c = *cw.cmd;
+    c.op = 4; c.s = s; c.filter_mol = j; c.self = kind;
+  }
+  cl.sync();
+  grad_share(tm, y, s, j, kind, 0, cw.size, out0, out1);
+  cl.sync();                    // helpers' shares are in their scratch
+  const BatchView &bv = y.c->bv;
+  const int n = 3 * y.NP2;
+  const size_t o5 = (size_t)(y.sc.G(5) - scr_of(bv, y.b, 0)), o6 = (size_t)(y.sc.G(6) - scr_of(bv, y.b, 0));
+  for (int i = tm.rank; i < n; i += tm.size) {
+    double v = out0[i];
+    for (int q = 1; q < cw.size; q++) v += scr_of(bv, y.b, q)[o5 + i];
+    out0[i] = v;
+    if (kind == 1) {
+      double w = out1[i];
+      for (int q = 1; q < cw.size; q++) w += scr_of(bv, y.b, q)[o6 + i];
+      out1[i] = w;
     }
   }
+  tm.sync();
+}
+
+// one gradient recompute of sphere s w.r.t. molecule j (src/molecule.cpp:1680-1843)
+__device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int key)
+{
+  const Tab &T = y.c->T;
+  const BatchView &bv = y.c->bv;
+  const int NP2 = y.NP2, i = y.mol(s), ts = y.ts(s);
+  double *tGrot = y.sc.G(1), *LGH = y.sc.G(2), *LGF = y.sc.G(3), *LGH2 = y.sc.G(4), *tmpG = y.sc.G(5);
+  PhaseClock gx{y.tph, 0};
+  gx.start(tm);
+  tcopy(tm, tGrot, y.gw(bv.tGw, key), 3 * NP2);
+  tm.sync();
+  PhaseClock sub{y.tph, 0};
+  sub.start(tm);
+  crew_grad(tm, y, s, j, 0, tGrot, nullptr);
+  sub.stop(tm, PH_GX_INTER);
+  const RotState mr = y.molrot(i);
+  for (int cc = 0; cc < 3; cc++) rot_apply_xi(tm, mr, tGrot + cc * NP2, LGH + cc * NP2, y.NP, false, y.NP);
+  tm.sync();
+  if (j == i) { tcopy(tm, y.gLHN(s), LGH, 3 * NP2); tm.sync(); }
+  tzero(tm, LGF, 3 * NP2);
+  tzero(tm, LGH2, 3 * NP2);
+  tm.sync();
+  // analytic pairs of the intra list shared by the crew, then the numeric ones
+  sub.start(tm);
+  crew_grad(tm, y, s, j, 1, LGF, LGH2);
+  sub.stop(tm, PH_GX_ANALYTIC);
+  sub.start(tm);
+  const int nlist = (i == j) ? bv.intraPol_n[(size_t)y.b * bv.nmol + j] : bv.interMol_n[(size_t)y.b * bv.nmol + j];
+  const int *lst = (i == j) ? bv.intraPol + ((size_t)y.b * bv.nmol + j) * y.S : bv.interMol + ((size_t)y.b * bv.nmol + j) * y.S;
+  const double *cis = y.cen(s);
+  for (int e = 0; e < nlist; e++) {
+    const int sm = lst[e];
+    if (i != j && y.mol(sm) != i) continue;
+    if (sm == s) continue;
+    const double *cms = y.cen(sm);
+    const double P[3] = {cis[0] - cms[0], cis[1] - cms[1], cis[2] - cms[2]};
+    const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+    const double rm = y.rad(sm);
+    const double sep = rho - y.rad(s) - rm;
+    if (sep > 0 && !(sep < y.c->prm.min_sep_numeric)) continue;
+    const int pF = compute_order(y.NP, rho, bv.maxgF[y.sc1(sm)], rm);
+    const int pH = compute_order(y.NP, rho, bv.maxgH[y.sc1(sm)], rm);
+    double *tmpH = y.sc.G(6);
+    crew_numeric_expand2<3>(tm, y.cw, T, y.sc, y.spx(sm), y.npts(sm), P, y.rad(s),
+                            NumSet{y.gFp(sm), true, false, pF, tmpG}, NumSet{y.gHp(sm), true, true, pH, tmpH});
+    add_vec_into(tm, LGF, tmpG, 3 * NP2);
+    add_vec_into(tm, LGH2, tmpH, 3 * NP2);
+  }
+  sub.stop(tm, PH_GX_NUMERIC);
   add_vec_into(tm, LGH, LGH2, 3 * NP2);
   gx.stop(tm, PH_GRX);
   double *gF = y.gw(bv.gFw, key), *gHk = y.gw(bv.gHw, key);
   PhaseClock pc{y.tph, 0};
   pc.start(tm);
-  const double dv = solve_fh(tm, y.cw, T, y.c->tv, y.c->prm, y.sc, ts, 3, gF, gHk, LGF, LGH, y.red, y.stats());
+  const double dv = solve_fh(tm, y.cw, y.tph, T, y.c->tv, y.c->prm, y.sc, ts, 3, gF, gHk, LGF, LGH, y.red, y.stats());
   pc.stop(tm, PH_SOLVE);
+  pc.start(tm);
   for (int cc = 0; cc < 3; cc++) rot_apply_xi(tm, mr, gHk + cc * NP2, y.gw(bv.gHrotw, key) + cc * NP2, y.NP, true, y.NP);
   tm.sync();
   // exposed gradient charges (src/expcenter.cpp:1377-1412)
   const double *cst = y.c->tv.cst + (size_t)ts * CST_N * y.NP;
   const double dA = 4 * PB_PI / double(y.c->tv.nspx[ts]);
   double totF[3], totH[3];
-  surface_q<3>(tm, T, y.spx(s), y.npts(s), dA, gF, T.CONST2, y.gFp(s), totF, y.red);
-  surface_q<3>(tm, T, y.spx(s), y.npts(s), dA, gHk, cst + CST_CHGH * y.NP, y.gHp(s), totH, y.red);
+  crew_surface_q2<3>(tm, y.cw, T, y.sc, y.red, y.spx(s), y.npts(s), dA, gF, T.CONST2, y.gFp(s), totF, gHk,
+                     cst + CST_CHGH * y.NP, y.gHp(s), totH);
   if (tm.rank == 0) {
     double mf = totF[0] > totF[1] ? totF[0] : totF[1];
     if (totF[2] > mf) mf = totF[2];
@@ -1328,6 +1502,7 @@ __device__ double recompute_grad(const Team &tm, const Sys &y, int s, int j, int
     y.stats()[3] += 1;
   }
   tm.sync();
+  pc.stop(tm, PH_GSURF);
   return dv;
 }
 
@@ -1347,6 +1522,61 @@ __device__ double inprod_ml(const double *M, double mscale, const double *L, dou
 }
 
 // ------------------------------------------------------------------ the force kernel
+// helper CTAs: serve the leader's commands until it sends the exit command.  y is
+// the helper's view of the system (its own scratch, no phase clocks).
+__device__ void crew_serve(const Team &tm, const Sys &y)
+{
+  const Crew &cw = y.cw;
+  const Tab &T = y.c->T;
+  const Scr &sc = y.sc;
+  cg::cluster_group cl = cg::this_cluster();
+  const CrewCmd *lead = cl.map_shared_rank(cw.cmd, 0);
+  const double2 *lxs = (const double2 *)cl.map_shared_rank(sc.xs, 0);
+  for (;;) {
+    cl.sync();
+    const CrewCmd c = *lead;
+    if (c.op == 1) {
+      for (int i = tm.rank; i < c.D * (c.ld >> 1); i += tm.size) ((double2 *)sc.xs)[i] = lxs[i];
+      tm.sync();
+      int r0, r1;
+      crew_rows(c.NP2, cw.rank, cw.size, r0, r1);
+      imat_apply(tm, c.IMT, c.ld, sc.xs, c.NP2, c.D, r0, r1, c.Y, c.scale);
+    } else if (c.op == 2) {
+      if (c.NC == 1)
+        numeric_expand2<1>(tm, T, sc, c.pts, c.N, c.shift, c.nscale, c.A, c.B, cw.rank, cw.size, sc.tile);
+      else
+        numeric_expand2<3>(tm, T, sc, c.pts, c.N, c.shift, c.nscale, c.A, c.B, cw.rank, cw.size, sc.tile);
+    } else if (c.op == 3) {
+      dta_share(tm, y, c.s, c.self != 0, c.filter_mol, c.use_ipol != 0, c.use_iact != 0, cw.rank, cw.size, sc.G(7));
+    } else if (c.op == 4) {
+      tzero(tm, sc.G(5), 3 * y.NP2);
+      if (c.self == 1) tzero(tm, sc.G(6), 3 * y.NP2);
+      tm.sync();
+      grad_share(tm, y, c.s, c.filter_mol, c.self, cw.rank, cw.size, sc.G(5), sc.G(6));
+    } else if (c.op == 5) {
+      double t1[3], t2[3];
+      if (c.NC == 1) surface_q2<1>(tm, T, sc, c.pts, c.N, c.dA, c.E1, c.c1, c.q1, c.E2, c.c2, c.q2, cw.rank, cw.size, t1, t2, y.red);
+      else surface_q2<3>(tm, T, sc, c.pts, c.N, c.dA, c.E1, c.c1, c.q1, c.E2, c.c2, c.q2, cw.rank, cw.size, t1, t2, y.red);
+      if (tm.rank == 0)
+        for (int k = 0; k < c.NC; k++) { cw.cmd->ptot[k] = t1[k]; cw.cmd->ptot[3 + k] = t2[k]; }
+    } else break;
+    cl.sync();
+  }
+  cl.sync();                    // the leader may leave once every helper has read the exit
+}
+
+// a helper CTA's view of system b: its own scratch block, no phase clocks
+__device__ Sys helper_sys(const Ctx &c, const Crew &cw, int b, void *dsm, double *red)
+{
+  Sys y;
+  y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = c.bv.S;
+  y.cw = cw;
+  y.sc = make_scr(scr_of(c.bv, b, cw.rank), y.NP, dsm);
+  y.red = red;
+  y.tph = nullptr;
+  return y;
+}
+
 // One system (the crew leader's part): CMolecule::computeForces.
 __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b, void *dsm, double *red)
 {
@@ -1354,19 +1584,21 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
   Sys y;
   y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = bv.S;
   y.cw = cw;
-  y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP, dsm);
+  y.sc = make_scr(scr_of(bv, b, 0), y.NP, dsm);
   y.red = red;
-  y.tph = bv.tphase + (size_t)b * 8;
+  y.tph = bv.tphase + (size_t)b * PH_N;
   const int S = bv.S, nmol = bv.nmol, NP2 = y.NP2;
   int *st = y.stats();
   PhaseClock total{y.tph, 0};
   if (tm.rank == 0) {
     for (int k = 0; k < 8; k++) st[k] = 0;
-    for (int k = 0; k < 8; k++) y.tph[k] = 0.0;
+    for (int k = 0; k < PH_N; k++) y.tph[k] = 0.0;
     st[5] = cw.size;
     bv.status[b] = PBSAM_STATUS_OK;
   }
   total.start(tm);
+  PhaseClock setup{y.tph, 0};
+  setup.start(tm);
   for (int t = tm.rank; t < nmol * 3; t += tm.size) {
     bv.force[(size_t)b * nmol * 3 + t] = 0.0;
     bv.torque[(size_t)b * nmol * 3 + t] = 0.0;
@@ -1479,6 +1711,7 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
       tm.sync();
     }
   }
+  setup.stop(tm, PH_SETUP);
   // ---- first round from self values
   double dev = 0.0, MAXDEV = 0.0;
   int mtotal = 0;
@@ -1540,6 +1773,8 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
     const double itj = 1.0 / double(jsize);
     const int *inter = bv.interMol + ((size_t)b * nmol + j) * S;
     const int *intra = bv.intraPol + ((size_t)b * nmol + j) * S;
+    PhaseClock book{y.tph, 0};
+    book.start(tm);
     for (int s = tm.rank; s < S; s += tm.size) bv.gkey[y.sc1(s)] = -1;
     tm.sync();
     for (int k = tm.rank; k < jsize; k += tm.size) bv.gkey[y.sc1(k < ni ? inter[k] : intra[k - ni])] = k;
@@ -1550,20 +1785,13 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
       tzero(tm, y.gw(bv.tGw, k), 3 * NP2);
     }
     tm.sync();
+    book.stop(tm, PH_GBOOK);
     // prepareDTA (src/molecule.cpp:1483-1571)
     for (int k = 0; k < jsize; k++) {
       const int s = k < ni ? inter[k] : intra[k - ni];
       double *acc = y.gw(bv.tGw, k);
-      if (k < ni) {
-        for (int e = 0; e < y.nipol(s); e++) {
-          const int sm = y.ipol(s)[e];
-          if (y.mol(sm) != j) continue;
-          grad_xform_from(tm, y, s, sm, false, acc);
-        }
-      } else {
-        for (int e = 0; e < y.nipol(s); e++) grad_xform_from(tm, y, s, y.ipol(s)[e], false, acc);
-        for (int e = 0; e < y.niact(s); e++) grad_xform_from(tm, y, s, y.iact(s)[e], false, acc);
-      }
+      if (k < ni) crew_dta(tm, y, s, false, j, true, false, acc);
+      else crew_dta(tm, y, s, false, -1, true, true, acc);
     }
     double *dg = bv.dgrad + (size_t)b * S;
     double dv = 0.0;
@@ -1595,6 +1823,8 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
     for (int h = 0; h < nact; h++) prepare_dta_iself(tm, y, bv.intraAct[((size_t)b * nmol + j) * S + h]);
   }
   tm.sync();
+  PhaseClock fclk{y.tph, 0};
+  fclk.start(tm);
   // ---- forces and torques (src/moldynamics.cpp:524-550, src/expcenter.cpp:123-149)
   double *fk = y.sc.misc;   // [S][3]
   for (int s = tm.rank; s < S; s += tm.size) {
@@ -1636,6 +1866,7 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
     qrot(qn, Tq, bv.torque + ((size_t)b * nmol + i) * 3);
   }
   tm.sync();
+  fclk.stop(tm, PH_FORCE);
   total.stop(tm, PH_TOTAL);
 }
 
@@ -1651,7 +1882,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
   const int b = blockIdx.x / cw.size;
   if (b >= c.bv.B) return;                 // whole crews only: the grid is n_systems * size
   if (cw.rank != 0) {
-    crew_serve(tm, cw, c.T, make_scr(c.bv.scr + (size_t)b * c.bv.scr_stride, c.T.NP, dsm));
+    crew_serve(tm, helper_sys(c, cw, b, dsm, red));
     return;
   }
   forces_body(tm, c, cw, b, dsm, red);
@@ -1671,7 +1902,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c)
   Sys y;
   y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = bv.S;
   y.cw = Crew{0, 1, nullptr};
-  y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP, dsm);
+  y.sc = make_scr(scr_of(bv, b, 0), y.NP, dsm);
   y.red = red;
   y.tph = nullptr;
   const Tab &T = c.T;
@@ -1791,10 +2022,10 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup1_kernel(Ctx c, double 
   const double *pts = tv.spx + 3 * (size_t)tv.spx_off[ts];
   const int npt = tv.spx_off[ts + 1] - tv.spx_off[ts];
   const double dA = 4.0 * PB_PI / double(tv.nspx[ts]);
-  double tot[1];
-  surface_q<1>(tm, T, pts, npt, dA, tv.Fself + (size_t)ts * NP2, T.CONST2, tv.qFself + tv.spx_off[ts], tot, red);
-  const double tF = tot[0];
-  surface_q<1>(tm, T, pts, npt, dA, tv.Hself + (size_t)ts * NP2, cst + CST_CHGH * NP, tv.qHself + tv.spx_off[ts], tot, red);
+  double totF[1], tot[1];
+  surface_q2<1>(tm, T, sc, pts, npt, dA, tv.Fself + (size_t)ts * NP2, T.CONST2, tv.qFself + tv.spx_off[ts],
+                tv.Hself + (size_t)ts * NP2, cst + CST_CHGH * NP, tv.qHself + tv.spx_off[ts], 0, 1, totF, tot, red);
+  const double tF = totF[0];
   if (tm.rank == 0) { tv.tFself[ts] = tF; tv.tHself[ts] = tot[0]; }
   // fixed charges split into inside (multipole) / outside (local) sets, scaled by 1/eps_in
   const int q0 = tv.chg_off[t], nq = tv.chg_off[t + 1] - q0;

@@ -115,7 +115,7 @@ __device__ void selfpol_body(const Team &tm, const Ctx &c, const Crew &cw, int b
   Sys y;
   y.c = &c; y.b = b; y.NP = c.T.NP; y.NP2 = y.NP * y.NP; y.S = bv.S;
   y.cw = cw;
-  y.sc = make_scr(bv.scr + (size_t)b * bv.scr_stride, y.NP, dsm);
+  y.sc = make_scr(scr_of(bv, b, 0), y.NP, dsm);
   y.red = red;
   y.tph = bv.tphase + (size_t)b * PH_N;
   const Tab &T = c.T;
@@ -135,7 +135,8 @@ __device__ void selfpol_body(const Team &tm, const Ctx &c, const Crew &cw, int b
     const double *cst = c.tv.cst + (size_t)ts * CST_N * y.NP;
     const double dA = 4 * PB_PI / double(c.tv.nspx[ts]);
     double tot[1];
-    surface_q<1>(tm, T, y.spx(s), y.npts(s), dA, y.H(s), cst + CST_CHGH * y.NP, y.qH(s), tot, y.red);
+    crew_surface_q2<1>(tm, y.cw, T, y.sc, y.red, y.spx(s), y.npts(s), dA, y.H(s), cst + CST_CHGH * y.NP, y.qH(s), tot,
+                       nullptr, nullptr, nullptr, nullptr);
     if (tm.rank == 0) { bv.tH[y.sc1(s)] = tot[0]; bv.tF[y.sc1(s)] = 0.0; bv.dev[y.sc1(s)] = 0.0; }
     tm.sync();
   }
@@ -176,7 +177,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_selfpol_kernel(Ctx c, const 
   const int b = blockIdx.x / cw.size;
   if (b >= c.bv.B) return;
   if (cw.rank != 0) {
-    crew_serve(tm, cw, c.T, make_scr(c.bv.scr + (size_t)b * c.bv.scr_stride, c.T.NP, dsm));
+    crew_serve(tm, helper_sys(c, cw, b, dsm, red));
     return;
   }
   selfpol_body(tm, c, cw, b, dsm, red, Eass, max_rounds, rounds_out);

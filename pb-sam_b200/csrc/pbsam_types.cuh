@@ -81,8 +81,9 @@ struct BatchView {
   double2 *molR;             // [B][nmol][rot entries at NP]
   double *molRS;             // [B][nmol][8] rotation state scalars
   double *sep;               // [B][S][S] sphere-sphere surface gaps
-  double *scr;               // [B][scr_stride]
+  double *scr;               // [B][crew][scr_stride]: one scratch block per CTA
   long long scr_stride;
+  int crew;                  // CTAs per system
   double *force, *torque, *energy;  // [B][nmol][3], [B][nmol][3], [B]
   int *status;               // [B]
   int *stats;                // [B][8]: sweeps, inner iterations, solves, grad solves, ...

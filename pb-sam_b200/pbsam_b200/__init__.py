@@ -217,9 +217,11 @@ class Molecules:
         return s
 
     def phase_ms(self):
-        """Device ms per phase of the last evaluation: solve, surface charges, numeric,
-        analytic intra, inter LS, gradient DTA, gradient-solve re-expansions, total."""
-        m = np.zeros((self.n_systems, 8))
+        """Device ms per phase of the last evaluation (16 per system): solve, surface
+        charges, numeric, analytic intra, inter LS, gradient DTA, gradient-solve
+        re-expansions, total, gradient surface charges, set-up, gradient bookkeeping,
+        forces; sub-phases: gradient inter, intra analytic, intra numeric, IMat products."""
+        m = np.zeros((self.n_systems, 16))
         _check(lib().pbsam_system_phase_ms(self.handle, _dptr(m)))
         return m
 
