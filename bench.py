@@ -24,6 +24,7 @@ import subprocess
 import sys
 import tempfile
 import time
+from collections import Counter
 
 import numpy as np
 
@@ -211,8 +212,8 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "poses": args.poses or "all", "poles": cfg["poles"],
                        "systems_per_gpu": B,
                        "spheres_per_system": 2 * cfg["n_sph"],
-                       "parallelism": "replicas: %d rank(s) x %d independent systems, %d CTAs per system" % (
-                           world, B, int(stats[0, 5])),
+                       "parallelism": "replicas: %d rank(s) x %d independent systems; CTAs per system %s" % (
+                           world, B, dict(sorted(Counter(int(x) for x in stats[:, 5]).items()))),
                        "l2": "no flush: inputs larger than L2 (120 IMats x 6.5 MB = 778 MB)"},
             "e2e": {"value": units / (e2e_max * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": int(hp.nbytes + hq.nbytes),
@@ -393,7 +394,8 @@ def main():
     ap.add_argument("--cpu-sample-its", type=int, default=6000,
                     help="largest inner-iteration count of a pose in the CPU sample")
     ap.add_argument("--cpu-limit", type=int, default=60, help="seconds before a sample pose is abandoned")
-    ap.add_argument("--cluster-size", type=int, default=0, help="CTAs per system (0: automatic)")
+    ap.add_argument("--cluster-size", type=int, default=-1,
+                    help="CTAs per system (0: automatic, -1: adaptive from the previous step's costs)")
     ap.add_argument("--poses", default="", help="comma-separated subset of the sweep's poses (small cases)")
     ap.add_argument("--traffic-per-launch", type=float, default=None,
                     help="DRAM bytes per launch measured by ncu (scaled from a small capture)")

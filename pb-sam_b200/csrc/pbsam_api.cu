@@ -8,6 +8,7 @@
 #include <cstring>
 #include <fstream>
 #include <string>
+#include <algorithm>
 #include <utility>
 #include <vector>
 
@@ -152,7 +153,37 @@ struct pbsam_system {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
   int crew = 1;            // CTAs (one cluster) per system in the force kernel
+  // adaptive crews (cluster_size == -1): systems grouped by the cost of their last
+  // evaluation, one launch per crew size on side streams
+  bool adaptive = false;
+  int *h_stats = nullptr, *h_list = nullptr, *d_list = nullptr;   // pinned host / device
+  cudaEvent_t ev_stats = nullptr, ev_fork = nullptr, ev_join[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaStream_t gs[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool stats_pending = false;
+  std::vector<int> gsize, gcount;    // per launch: crew size, systems (lists concatenated in d_list)
 };
+
+// Crew sizes from the last evaluation's inner-iteration counts: every system starts
+// with one CTA, the one with the largest cost per CTA doubles (up to 8) while the
+// crews fit in the SMs.  Returns per system its crew size.
+static std::vector<int> plan_crews(const int *its, int B, int n_sm)
+{
+  std::vector<int> C(B, 1);
+  int total = B;
+  for (;;) {
+    int best = -1;
+    double bc = -1.0;
+    for (int b = 0; b < B; b++) {
+      if (C[b] >= 8) continue;
+      const double v = (its[b] + 1.0) / C[b];
+      if (v > bc) { bc = v; best = b; }
+    }
+    if (best < 0 || total + C[best] > n_sm) break;
+    total += C[best];
+    C[best] *= 2;
+  }
+  return C;
+}
 
 extern "C" void pbsam_params_default(pbsam_params *p)
 {
@@ -174,8 +205,8 @@ extern "C" int pbsam_context_create(const pbsam_params *prm, int device, pbsam_c
 {
   if (!prm || !out) return fail(PBSAM_E_BADARG, "null argument");
   if (prm->poles < 1 || prm->poles > 32) return fail(PBSAM_E_BADARG, "poles must be in [1, 32]");
-  if (prm->cluster_size < 0 || prm->cluster_size > 8)
-    return fail(PBSAM_E_BADARG, "cluster_size must be 0 (automatic) or 1..8");
+  if (prm->cluster_size < -1 || prm->cluster_size > 8)
+    return fail(PBSAM_E_BADARG, "cluster_size must be -1 (adaptive), 0 (automatic) or 1..8");
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
   if (device < 0 || device >= ndev) return fail(PBSAM_E_BADARG, "no such CUDA device");
@@ -550,7 +581,8 @@ static int finalize_types(pbsam_context *c)
   TRY(dput(B, &tv.rad, rad)); TRY(dput(B, &tv.spx_off, spx_off)); TRY(dput(B, &tv.spx, spx));
   TRY(dput(B, &tv.nspx, nspx)); TRY(dput(B, &tv.Fself, Fs)); TRY(dput(B, &tv.Hself, Hs));
   TRY(dput(B, &tv.hself_scale, hsc)); TRY(dput(B, &tv.near_off, near_off)); TRY(dput(B, &tv.near, near));
-  TRY(dput(B, &tv.imat, imat)); TRY(dput(B, &tv.chg_off, chg_off)); TRY(dput(B, &tv.chg_pos, chg_pos));
+  TRY(dput(B, &tv.imat, imat));
+  TRY(dput(B, &tv.chg_off, chg_off)); TRY(dput(B, &tv.chg_pos, chg_pos));
   TRY(dput(B, &tv.chg, chg));
   TRY(dput(B, &tv.chg_lab, chg_lab));
   TRY(dput(B, &tv.pair_off, pair_off));
@@ -661,10 +693,12 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   chk(dalloc(Bf, &bv.molR, (size_t)B * n_mol * rot_off(2 * NP - 1)));
   chk(dalloc(Bf, &bv.molRS, B * n_mol * 16));
   chk(dalloc(Bf, &bv.sep, B * S * S));
-  s->crew = pick_crew(pbsam_forces_kernel, B, team_smem_bytes(NP), c->prm.cluster_size);
-  bv.crew = s->crew;
+  s->adaptive = c->prm.cluster_size < 0;
+  s->crew = pick_crew(pbsam_forces_kernel, B, team_smem_bytes(NP), s->adaptive ? 0 : c->prm.cluster_size);
+  bv.crew = s->adaptive ? 8 : s->crew;       // scratch blocks per system: the largest crew it may get
   bv.scr_stride = scr_doubles(NP, S);
-  chk(dalloc(Bf, &bv.scr, (size_t)B * s->crew * bv.scr_stride));
+  chk(dalloc(Bf, &bv.scr, (size_t)B * bv.crew * bv.scr_stride));
+  if (s->adaptive) chk(dalloc(Bf, &s->d_list, B));
   chk(dalloc(Bf, &bv.force, B * n_mol * 3)); chk(dalloc(Bf, &bv.torque, B * n_mol * 3));
   chk(dalloc(Bf, &bv.energy, B)); chk(dalloc(Bf, &bv.status, B)); chk(dalloc(Bf, &bv.stats, B * 8));
   chk(dalloc(Bf, &bv.tphase, B * PH_N));
@@ -681,7 +715,22 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   p.min_sep_numeric = c->prm.min_sep_numeric; p.idiel = c->prm.idiel; p.sdiel = c->prm.sdiel;
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);
+  if (s->adaptive) {
+    if (cudaMallocHost(&s->h_stats, (size_t)B * 8 * sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&s->h_list, (size_t)B * sizeof(int)) != cudaSuccess)
+      r = fail(PBSAM_E_NOMEM, "pinned host buffers");
+    cudaEventCreateWithFlags(&s->ev_stats, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
+    for (int g = 0; g < 4; g++) {
+      cudaEventCreateWithFlags(&s->ev_join[g], cudaEventDisableTiming);
+      cudaStreamCreateWithFlags(&s->gs[g], cudaStreamNonBlocking);
+    }
+  }
   c->live_systems++;
+  if (r) {
+    pbsam_system_destroy(s);
+    return r;
+  }
   *out = s;
   return pbsam_system_reset(s);
 }
@@ -704,6 +753,16 @@ extern "C" int pbsam_system_destroy(pbsam_system *s)
   for (void *p : s->bufs) cudaFree(p);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->adaptive) {
+    for (int g = 0; g < 4; g++) {
+      if (s->gs[g]) { cudaStreamSynchronize(s->gs[g]); cudaStreamDestroy(s->gs[g]); }
+      if (s->ev_join[g]) cudaEventDestroy(s->ev_join[g]);
+    }
+    if (s->ev_stats) cudaEventDestroy(s->ev_stats);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->h_stats) cudaFreeHost(s->h_stats);
+    if (s->h_list) cudaFreeHost(s->h_list);
+  }
   s->ctx->live_systems--;
   delete s;
   return PBSAM_OK;
@@ -732,10 +791,55 @@ extern "C" int pbsam_system_compute_forces(pbsam_system *s, double *force, doubl
 {
   if (!s) return fail(PBSAM_E_BADARG, "null system");
   CK(cudaSetDevice(s->ctx->device));
+  const size_t smem = team_smem_bytes(s->ctx->prm.poles);
+  if (s->adaptive && s->stats_pending && cudaEventQuery(s->ev_stats) == cudaSuccess) {
+    // regroup from the last evaluation's costs
+    s->stats_pending = false;
+    std::vector<int> its(s->B);
+    for (int b = 0; b < s->B; b++) its[b] = s->h_stats[8 * b + 1];
+    int n_sm = 0;
+    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, s->ctx->device));
+    const std::vector<int> C = plan_crews(its.data(), s->B, n_sm - n_sm / 16);
+    std::vector<int> gsize, gcount, list;
+    for (int size : {8, 4, 2, 1}) {
+      int cnt = 0;
+      for (int b = 0; b < s->B; b++)
+        if (C[b] == size) { list.push_back(b); cnt++; }
+      if (cnt) { gsize.push_back(size); gcount.push_back(cnt); }
+    }
+    bool same = (gsize == s->gsize && gcount == s->gcount);
+    for (int i = 0; same && i < s->B; i++) same = (s->h_list[i] == list[i]);
+    if (!same) {
+      CK(cudaStreamSynchronize(s->stream));      // the previous list upload has completed
+      for (int i = 0; i < s->B; i++) s->h_list[i] = list[i];
+      CK(cudaMemcpyAsync(s->d_list, s->h_list, s->B * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+      s->gsize = gsize;
+      s->gcount = gcount;
+    }
+  }
   CK(cudaEventRecord(s->ev0, s->stream));
-  CK(launch_crews(pbsam_forces_kernel, s->B, s->crew, team_smem_bytes(s->ctx->prm.poles), s->stream, s->c));
+  if (!s->adaptive || s->gsize.empty()) {
+    CK(launch_crews(pbsam_forces_kernel, s->B, s->crew, smem, s->stream, s->c, (const int *)nullptr));
+  } else {
+    // one launch per crew size on side streams, heaviest first, joined back
+    CK(cudaEventRecord(s->ev_fork, s->stream));
+    int off = 0;
+    for (size_t g = 0; g < s->gsize.size(); g++) {
+      CK(cudaStreamWaitEvent(s->gs[g], s->ev_fork, 0));
+      CK(launch_crews(pbsam_forces_kernel, s->gcount[g], s->gsize[g], smem, s->gs[g], s->c,
+                      (const int *)(s->d_list + off)));
+      CK(cudaEventRecord(s->ev_join[g], s->gs[g]));
+      off += s->gcount[g];
+    }
+    for (size_t g = 0; g < s->gsize.size(); g++) CK(cudaStreamWaitEvent(s->stream, s->ev_join[g], 0));
+  }
   CK(cudaGetLastError());
   CK(cudaEventRecord(s->ev1, s->stream));
+  if (s->adaptive && !s->stats_pending) {
+    CK(cudaMemcpyAsync(s->h_stats, s->c.bv.stats, (size_t)s->B * 8 * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaEventRecord(s->ev_stats, s->stream));
+    s->stats_pending = true;
+  }
   const size_t n = (size_t)s->B * s->nmol * 3;
   const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   if (force) CK(cudaMemcpyAsync(force, s->c.bv.force, n * sizeof(double), k, s->stream));

@@ -65,10 +65,17 @@ __host__ __device__ inline size_t imat_stride(int NP2) { return (size_t)NP2 * im
 // numeric-expansion tile: per point the P^2 harmonics, 2 x P radial factors,
 // 5 geometry words and 2 x 3 weights
 __host__ __device__ inline size_t tile_point_bytes(int NP) { return ((size_t)NP * NP + 2 * NP + 11) * sizeof(double); }
+// F/H solve state kept in shared memory: F, H, new H, F base, H base, H at entry
+// (3 operands each) and a degree table
+__host__ __device__ inline size_t solve_state_bytes(int NP)
+{
+  return 6 * 3 * (size_t)NP * NP * sizeof(double) + (size_t)NP * NP * sizeof(short) + 16;
+}
 __host__ __device__ inline size_t dyn_region_bytes(int NP)
 {
   const size_t NN = 2 * NP - 1;
   size_t lv = 2 * NN * NN * sizeof(double2);
+  if (solve_state_bytes(NP) > lv) lv = solve_state_bytes(NP);
   size_t tp = (160 * 1024) / tile_point_bytes(NP);
   if (tp > 32) tp = 32;
   if (tp < 1) tp = 1;
@@ -146,16 +153,16 @@ __device__ __forceinline__ void tzero(const Team &tm, double *dst, int n)
 __device__ __forceinline__ void tadd(const Team &tm, double *dst, const double *src, int n)
 { for (int i = tm.rank; i < n; i += tm.size) dst[i] += src[i]; }
 
-// deterministic tree sum (team size is a power of two)
+// deterministic team sum: xor butterfly within each warp, then the warp sums in order
 __device__ double team_sum(const Team &tm, double v, double *red)
 {
-  red[tm.rank] = v;
+  const int lane = tm.rank & 31, warp = tm.rank >> 5, nw = tm.size >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) red[warp] = v;
   tm.sync();
-  for (int s = tm.size / 2; s > 0; s >>= 1) {
-    if (tm.rank < s) red[tm.rank] += red[tm.rank + s];
-    tm.sync();
-  }
-  double r = red[0];
+  double r = 0.0;
+  for (int w = 0; w < nw; w++) r += red[w];
   tm.sync();
   return r;
 }
@@ -731,9 +738,9 @@ __device__ __noinline__ void surface_q2(const Team &tm, const Tab &T, const Scr 
 // time and its lanes stride the rows with 16-byte read-only loads, two column
 // blocks per step, so 128 bytes per lane are in flight; the D operands share every
 // loaded IMat element.  The row sums are reduced across the warp in a fixed order.
-template <int D>
-__device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const double *x, int NP2, int r_begin, int r_end,
-                             double *Y, const double *scale)
+template <int D, int U>
+__device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const double *x, int NP2,
+                                          int r_begin, int r_end, double *Y, const double *scale)
 {
   const int lane = tm.rank & 31, warp = tm.rank >> 5, nw = tm.size >> 5;
   const int NV = ld >> 1;
@@ -750,30 +757,23 @@ __device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int
     for (int j = 0; j < 4; j++)
 #pragma unroll
       for (int d = 0; d < D; d++) acc[j][d] = 0.0;
-    int k = lane;
-    for (; k + 32 < NV; k += 64) {
-      double2 a[4], b[4];
+    // U column blocks of 32 double2 per step: 4 * U 16-byte loads per lane in flight
+    for (int k0 = lane; k0 < NV; k0 += 32 * U) {
+      double2 a[U][4];
 #pragma unroll
-      for (int j = 0; j < 4; j++) { a[j] = __ldg(rp[j] + k); b[j] = __ldg(rp[j] + k + 32); }
+      for (int b = 0; b < U; b++)
 #pragma unroll
-      for (int d = 0; d < D; d++) {
-        const double2 u = x2[d * NV + k], v = x2[d * NV + k + 32];
+        for (int j = 0; j < 4; j++)
+          a[b][j] = (k0 + 32 * b < NV) ? __ldg(rp[j] + k0 + 32 * b) : make_double2(0.0, 0.0);
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          acc[j][d] += a[j].x * u.x + a[j].y * u.y;
-          acc[j][d] += b[j].x * v.x + b[j].y * v.y;
+      for (int b = 0; b < U; b++) {
+        if (k0 + 32 * b >= NV) break;
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          const double2 u = x2[d * NV + k0 + 32 * b];
+#pragma unroll
+          for (int j = 0; j < 4; j++) acc[j][d] += a[b][j].x * u.x + a[b][j].y * u.y;
         }
-      }
-    }
-    if (k < NV) {
-      double2 a[4];
-#pragma unroll
-      for (int j = 0; j < 4; j++) a[j] = __ldg(rp[j] + k);
-#pragma unroll
-      for (int d = 0; d < D; d++) {
-        const double2 u = x2[d * NV + k];
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[j][d] += a[j].x * u.x + a[j].y * u.y;
       }
     }
 #pragma unroll
@@ -804,8 +804,8 @@ __device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int
 __device__ __forceinline__ void imat_apply(const Team &tm, const double *IMT, int ld, const double *x, int NP2, int D,
                                            int r_begin, int r_end, double *Y, const double *scale)
 {
-  if (D == 1) imat_apply_t<1>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
-  else imat_apply_t<3>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
+  if (D == 1) imat_apply_t<1, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
+  else imat_apply_t<3, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
 }
 
 // ------------------------------------------------------------------ crews (thread-block clusters)
@@ -817,10 +817,10 @@ __device__ __forceinline__ void imat_apply(const Team &tm, const double *IMT, in
 // rows visible to the leader.  The exit command is followed by one last barrier so
 // no helper reads the leader's shared memory after it has gone.
 struct CrewCmd {
-  int op;                 // 0: exit, 1: matvec, 2: numeric expansion
-  int D, NP2, ld;         // matvec
-  const double *IMT;
-  double *Y;
+  int op;                 // 0: exit, 1: matvec, 2: numeric expansion, 3: DTA list, 4: gradient pairs, 5: surface charges
+  int D, NP2, ld;         // matvec: rows of IMT times the pushed operands into the leader's shared
+  const double *IMT;      // memory at offset yoff from its tile region
+  long long yoff;
   const double *scale;
   int NC, N;              // numeric expansion
   const double *pts;
@@ -834,8 +834,22 @@ struct CrewCmd {
 };
 struct Crew {
   int rank, size;         // CTA rank in the cluster, CTAs per system
-  CrewCmd *cmd;           // this CTA's command block (helpers read the leader's)
+  CrewCmd *cmd;           // this CTA's command block (the leader writes every CTA's copy)
 };
+
+// leader: write the command into every CTA's command block, one 8-byte word per
+// thread (every thread holds the same command; the cluster barrier that follows
+// publishes it)
+__device__ __forceinline__ void crew_post(const Team &tm, const Crew &cw, const CrewCmd &c)
+{
+  constexpr int NW = sizeof(CrewCmd) / sizeof(unsigned long long);
+  static_assert(sizeof(CrewCmd) % sizeof(unsigned long long) == 0, "command block size");
+  if (tm.rank >= NW * cw.size) return;
+  cg::cluster_group cl = cg::this_cluster();
+  const int q = tm.rank / NW, w = tm.rank % NW;
+  unsigned long long *dst = (unsigned long long *)cl.map_shared_rank(cw.cmd, q);
+  dst[w] = ((const unsigned long long *)&c)[w];
+}
 
 __device__ __forceinline__ void crew_rows(int NP2, int rank, int size, int &r0, int &r1)
 {
@@ -846,20 +860,27 @@ __device__ __forceinline__ void crew_rows(int NP2, int rank, int size, int &r0, 
   if (r1 > NP2) r1 = NP2;
 }
 
-__device__ void crew_imat_apply(const Team &tm, const Crew &cw, const double *IMT, int ld, const double *x, int NP2,
-                                int D, double *Y, const double *scale)
+// Y (the leader's shared memory) = scale[n] * IMat x for the crew: the operands were
+// pushed into every CTA's operand buffer; each CTA applies its share of the rows
+// and stores them straight into the leader's Y.
+__device__ void crew_imat_apply(const Team &tm, const Crew &cw, const Scr &sc, const double *IMT, int NP2, int D,
+                                double *Y, const double *scale)
 {
-  if (cw.size == 1) { imat_apply(tm, IMT, ld, x, NP2, D, 0, NP2, Y, scale); return; }
-  cg::cluster_group cl = cg::this_cluster();
-  if (tm.rank == 0) {
-    cw.cmd->op = 1; cw.cmd->D = D; cw.cmd->NP2 = NP2; cw.cmd->ld = ld;
-    cw.cmd->IMT = IMT; cw.cmd->Y = Y; cw.cmd->scale = scale;
+  if (cw.size == 1) {
+    tm.sync();
+    imat_apply(tm, IMT, sc.ld, sc.xs, NP2, D, 0, NP2, Y, scale);
+    tm.sync();
+    return;
   }
-  cl.sync();                    // command and operands visible to the crew
+  cg::cluster_group cl = cg::this_cluster();
+  CrewCmd c;
+  c.op = 1; c.D = D; c.NP2 = NP2; c.ld = sc.ld; c.IMT = IMT; c.yoff = (long long)(Y - sc.tile); c.scale = scale;
+  crew_post(tm, cw, c);
+  cl.sync();                    // operands and command visible to the crew
   int r0, r1;
   crew_rows(NP2, 0, cw.size, r0, r1);
-  imat_apply(tm, IMT, ld, x, NP2, D, r0, r1, Y, scale);
-  cl.sync();                    // every CTA's rows written
+  imat_apply(tm, IMT, sc.ld, sc.xs, NP2, D, r0, r1, Y, scale);
+  cl.sync();                    // every CTA's rows are in the leader's Y
 }
 
 // Numeric expansion (numeric_expand2) shared by the crew: each CTA sums a share of
@@ -870,10 +891,11 @@ __device__ void crew_numeric_expand2(const Team &tm, const Crew &cw, const Tab &
 {
   if (cw.size == 1) { numeric_expand2<NC>(tm, T, sc, pts, N, shift, scale, A, B); return; }
   cg::cluster_group cl = cg::this_cluster();
-  if (tm.rank == 0) {
-    CrewCmd &c = *cw.cmd;
+  {
+    CrewCmd c;
     c.op = 2; c.NC = NC; c.N = N; c.pts = pts; c.nscale = scale; c.A = A; c.B = B;
     c.shift[0] = shift[0]; c.shift[1] = shift[1]; c.shift[2] = shift[2];
+    crew_post(tm, cw, c);
   }
   cl.sync();
   numeric_expand2<NC>(tm, T, sc, pts, N, shift, scale, A, B, 0, cw.size, sc.tile);
@@ -902,10 +924,11 @@ __device__ void crew_surface_q2(const Team &tm, const Crew &cw, const Tab &T, co
     return;
   }
   cg::cluster_group cl = cg::this_cluster();
-  if (tm.rank == 0) {
-    CrewCmd &c = *cw.cmd;
+  {
+    CrewCmd c;
     c.op = 5; c.NC = NC; c.pts = pts; c.N = N; c.dA = dA;
     c.E1 = E1; c.c1 = c1; c.q1 = q1; c.E2 = E2; c.c2 = c2; c.q2 = q2;
+    crew_post(tm, cw, c);
   }
   cl.sync();
   double t1[NC], t2[NC];
@@ -930,7 +953,9 @@ __device__ void crew_finish(const Team &tm, const Crew &cw)
 {
   if (cw.size == 1) return;
   cg::cluster_group cl = cg::this_cluster();
-  if (tm.rank == 0) cw.cmd->op = 0;
+  CrewCmd c;
+  c.op = 0;
+  crew_post(tm, cw, c);
   cl.sync();
   cl.sync();
 }
@@ -948,56 +973,62 @@ __device__ double solve_fh(const Team &tm, const Crew &cw, double *tph, const Ta
   const int NP = T.NP, NP2 = NP * NP, len = D * NP2;
   const double *cst = tv.cst + (size_t)ts * CST_N * NP;
   const double *Dfix = tv.Dfix + (size_t)ts * NP2, *Vfix = tv.Vfix + (size_t)ts * NP2;
-  const double *IM = tv.imat + (size_t)ts * imat_stride(NP2);
+  const double *IMT = tv.imat + (size_t)ts * imat_stride(NP2);
   const int ld = sc.ld;
-  double *fbase = sc.sol, *hbase = sc.sol + len, *fx = sc.xs, *hx = sc.xs;
-  double *oldH = sc.sol + 4 * len, *outH = sc.sol + 5 * len;
+  // state in shared memory for the whole solve
+  double *sF = sc.tile, *sH = sF + len, *sHn = sH + len, *sFb = sHn + len, *sHb = sFb + len, *sOut = sHb + len;
+  short *deg = (short *)(sOut + len);
+  // operand buffers of every CTA of the crew (the leader's own first)
+  cg::cluster_group cl = cg::this_cluster();
+  double *ox[8];
+  const int nc = cw.size < 8 ? cw.size : 8;
+  for (int q = 0; q < nc; q++) ox[q] = (q == 0) ? sc.xs : cl.map_shared_rank(sc.xs, q);
+  for (int k = tm.rank; k < NP2; k += tm.size) {
+    int n = (int)sqrt((double)k);
+    while (n * n > k) n--;
+    while ((n + 1) * (n + 1) <= k) n++;
+    deg[k] = (short)n;
+  }
   // the operands' pad columns stay zero (the IMat pad column is zero too)
-  for (int d = tm.rank; d < D; d += tm.size)
-    for (int k = NP2; k < ld; k++) sc.xs[d * ld + k] = 0.0;
+  for (int u = tm.rank; u < D * (ld - NP2) * nc; u += tm.size) {
+    const int q = u / (D * (ld - NP2)), r = u % (D * (ld - NP2));
+    ox[q][(r / (ld - NP2)) * ld + NP2 + r % (ld - NP2)] = 0.0;
+  }
+  tm.sync();
   for (int k = tm.rank; k < len; k += tm.size) {
-    const int kk = k % NP2;
-    int n = (int)sqrt((double)kk);
-    while (n * n > kk) n--;
-    while ((n + 1) * (n + 1) <= kk) n++;
+    const int kk = k % NP2, n = deg[kk];
     if (D == 1) {
-      fbase[k] = Vfix[kk] + cst[CST_LH1 * NP + n] * LH[k] + cst[CST_LF1 * NP + n] * LF[k];
-      hbase[k] = Dfix[kk] + cst[CST_LH2 * NP + n] * LH[k] + cst[CST_LF2 * NP + n] * LF[k];
+      sFb[k] = Vfix[kk] + cst[CST_LH1 * NP + n] * LH[k] + cst[CST_LF1 * NP + n] * LF[k];
+      sHb[k] = Dfix[kk] + cst[CST_LH2 * NP + n] * LH[k] + cst[CST_LF2 * NP + n] * LF[k];
     } else {
-      fbase[k] = cst[CST_LH1 * NP + n] * LH[k] + cst[CST_LF1 * NP + n] * LF[k];
-      hbase[k] = cst[CST_LH2 * NP + n] * LH[k] + cst[CST_LF2 * NP + n] * LF[k];
+      sFb[k] = cst[CST_LH1 * NP + n] * LH[k] + cst[CST_LF1 * NP + n] * LF[k];
+      sHb[k] = cst[CST_LH2 * NP + n] * LH[k] + cst[CST_LF2 * NP + n] * LF[k];
     }
-    oldH[k] = H[k];
-    outH[k] = H[k];
+    const double h = H[k];
+    sF[k] = F[k];
+    sH[k] = h;
+    sOut[k] = h;
   }
   tm.sync();
   int ct = 0;
   double dev = 0.0;
+  PhaseClock mv{tph, 0};
   for (;;) {
-    for (int k = tm.rank; k < len; k += tm.size) {
-      const int kk = k % NP2;
-      int n = (int)sqrt((double)kk);
-      while (n * n > kk) n--;
-      while ((n + 1) * (n + 1) <= kk) n++;
-      fx[(k / NP2) * ld + kk] = fbase[k] + cst[CST_H1 * NP + n] * H[k] + cst[CST_F1 * NP + n] * F[k];
-    }
-    tm.sync();
-    PhaseClock mv{tph, 0};
     mv.start(tm);
-    crew_imat_apply(tm, cw, IM, ld, sc.xs, NP2, D, F, T.CONST3);
-    tm.sync();
     for (int k = tm.rank; k < len; k += tm.size) {
-      const int kk = k % NP2;
-      int n = (int)sqrt((double)kk);
-      while (n * n > kk) n--;
-      while ((n + 1) * (n + 1) <= kk) n++;
-      hx[(k / NP2) * ld + kk] = hbase[k] + cst[CST_H2 * NP + n] * H[k] + cst[CST_F2 * NP + n] * F[k];
+      const int kk = k % NP2, n = deg[kk];
+      const double v = sFb[k] + cst[CST_H1 * NP + n] * sH[k] + cst[CST_F1 * NP + n] * sF[k];
+      for (int q = 0; q < nc; q++) ox[q][(k / NP2) * ld + kk] = v;
     }
-    tm.sync();
-    crew_imat_apply(tm, cw, IM, ld, sc.xs, NP2, D, H, cst + CST_INVH * NP);
+    crew_imat_apply(tm, cw, sc, IMT, NP2, D, sF, T.CONST3);
+    for (int k = tm.rank; k < len; k += tm.size) {
+      const int kk = k % NP2, n = deg[kk];
+      const double v = sHb[k] + cst[CST_H2 * NP + n] * sH[k] + cst[CST_F2 * NP + n] * sF[k];
+      for (int q = 0; q < nc; q++) ox[q][(k / NP2) * ld + kk] = v;
+    }
+    crew_imat_apply(tm, cw, sc, IMT, NP2, D, sHn, cst + CST_INVH * NP);
     mv.stop(tm, PH_MATVEC);
-    tm.sync();
-    // computeDev over complex entries (d, n, m)
+    // computeDev over complex entries (d, n, m) of the old and new H
     double part = 0.0;
     const int ncx = D * NP * (NP + 1) / 2;
     for (int u = tm.rank; u < ncx; u += tm.size) {
@@ -1008,8 +1039,8 @@ __device__ double solve_fh(const Team &tm, const Crew &cw, double *tph, const Ta
       const int m = r - n * (n + 1) / 2;
       const int base = d * NP2 + IDX(n);
       double ar, ai = 0.0, br, bi = 0.0;
-      if (m == 0) { ar = oldH[base]; br = H[base]; }
-      else { ar = oldH[base + 2 * m - 1]; ai = oldH[base + 2 * m]; br = H[base + 2 * m - 1]; bi = H[base + 2 * m]; }
+      if (m == 0) { ar = sH[base]; br = sHn[base]; }
+      else { ar = sH[base + 2 * m - 1]; ai = sH[base + 2 * m]; br = sHn[base + 2 * m - 1]; bi = sHn[base + 2 * m]; }
       const double PL = 1e-30;
       double s;
       if (fabs(ar) < PL && fabs(ai) < PL) {
@@ -1025,20 +1056,19 @@ __device__ double solve_fh(const Team &tm, const Crew &cw, double *tph, const Ta
       part += s;
     }
     dev = team_sum(tm, part, red) / (4 * NP * NP);
-    for (int k = tm.rank; k < len; k += tm.size) oldH[k] = H[k];
-    tm.sync();
+    { double *t = sH; sH = sHn; sHn = t; }    // the new H is the current one
     ct++;
     if (!(dev > prm.solve_tol && ct < prm.solve_max_ct)) break;
   }
   if (tm.rank == 0 && stats) { stats[1] += ct; stats[2] += 1; }
-  // computeDev2 (outer deviation)
+  // results back to the system state; computeDev2 (outer deviation)
   double pd = 0.0, ps = 0.0;
   for (int u = tm.rank; u < len; u += tm.size) {
-    const int i = u % NP2;
-    int n = (int)sqrt((double)i);
-    while (n * n > i) n--;
+    F[u] = sF[u];
+    H[u] = sH[u];
+    const int i = u % NP2, n = deg[i];
     const int mm = i - n * n;
-    const double a = outH[u], b = H[u], df = a - b;
+    const double a = sOut[u], b = sH[u], df = a - b;
     const double w = (mm == 0) ? 1.0 : 2.0;
     pd += w * (df * df);
     ps += w * (a * a + b * b);
@@ -1302,10 +1332,11 @@ __device__ void crew_dta(const Team &tm, const Sys &y, int s, bool self, int fil
     return;
   }
   cg::cluster_group cl = cg::this_cluster();
-  if (tm.rank == 0) {
-    CrewCmd &c = *cw.cmd;
+  {
+    CrewCmd c;
     c.op = 3; c.s = s; c.self = self ? 1 : 0; c.filter_mol = filter_mol;
     c.use_ipol = use_ipol ? 1 : 0; c.use_iact = use_iact ? 1 : 0; c.acc = acc;
+    crew_post(tm, cw, c);
   }
   cl.sync();
   dta_share(tm, y, s, self, filter_mol, use_ipol, use_iact, 0, cw.size, y.sc.G(7));
@@ -1403,9 +1434,10 @@ __device__ void crew_grad(const Team &tm, const Sys &y, int s, int j, int kind, 
   const Crew &cw = y.cw;
   if (cw.size == 1) { grad_share(tm, y, s, j, kind, 0, 1, out0, out1); return; }
   cg::cluster_group cl = cg::this_cluster();
-  if (tm.rank == 0) {
-    CrewCmd &c = *cw.cmd;
+  {
+    CrewCmd c;
     c.op = 4; c.s = s; c.filter_mol = j; c.self = kind;
+    crew_post(tm, cw, c);
   }
   cl.sync();
   grad_share(tm, y, s, j, kind, 0, cw.size, out0, out1);
@@ -1530,17 +1562,14 @@ __device__ void crew_serve(const Team &tm, const Sys &y)
   const Tab &T = y.c->T;
   const Scr &sc = y.sc;
   cg::cluster_group cl = cg::this_cluster();
-  const CrewCmd *lead = cl.map_shared_rank(cw.cmd, 0);
-  const double2 *lxs = (const double2 *)cl.map_shared_rank(sc.xs, 0);
   for (;;) {
     cl.sync();
-    const CrewCmd c = *lead;
+    const CrewCmd c = *cw.cmd;    // posted by the leader before the barrier
     if (c.op == 1) {
-      for (int i = tm.rank; i < c.D * (c.ld >> 1); i += tm.size) ((double2 *)sc.xs)[i] = lxs[i];
-      tm.sync();
       int r0, r1;
       crew_rows(c.NP2, cw.rank, cw.size, r0, r1);
-      imat_apply(tm, c.IMT, c.ld, sc.xs, c.NP2, c.D, r0, r1, c.Y, c.scale);
+      double *Y = cl.map_shared_rank(sc.tile + c.yoff, 0);
+      imat_apply(tm, c.IMT, c.ld, sc.xs, c.NP2, c.D, r0, r1, Y, c.scale);
     } else if (c.op == 2) {
       if (c.NC == 1)
         numeric_expand2<1>(tm, T, sc, c.pts, c.N, c.shift, c.nscale, c.A, c.B, cw.rank, cw.size, sc.tile);
@@ -1870,8 +1899,9 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
   total.stop(tm, PH_TOTAL);
 }
 
-// Grid: n_systems crews of cluster-size CTAs (a plain launch is a crew of one).
-__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
+// Grid: crews of cluster-size CTAs (a plain launch is a crew of one), one per
+// system; crew k works on system list[k] (list == nullptr: system k).
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c, const int *list)
 {
   extern __shared__ double2 dsm[];
   __shared__ double red[PBSAM_TEAM];
@@ -1879,8 +1909,9 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c)
   const Team tm{(int)threadIdx.x, (int)blockDim.x};
   cg::cluster_group cl = cg::this_cluster();
   const Crew cw{(int)cl.block_rank(), (int)cl.num_blocks(), &cmd};
-  const int b = blockIdx.x / cw.size;
-  if (b >= c.bv.B) return;                 // whole crews only: the grid is n_systems * size
+  const int k = blockIdx.x / cw.size;
+  const int b = list ? list[k] : k;
+  if (b >= c.bv.B) return;                 // whole crews only: the grid is (systems in the list) * size
   if (cw.rank != 0) {
     crew_serve(tm, helper_sys(c, cw, b, dsm, red));
     return;
