@@ -218,7 +218,8 @@ def run_ours(args):
             "e2e": {"value": units / (e2e_max * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": int(hp.nbytes + hq.nbytes),
                     "d2h_bytes_per_step": int(f.nbytes + t.nbytes + st.nbytes)},
-            "gpu_launches": args.steps,
+            # one force-kernel launch per crew size in use (adaptive crews: up to 4) per step
+            "gpu_launches": args.steps * len(set(int(x) for x in stats[:, 5])),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind, "kernel": "pbsam_forces_kernel", "launch_ms": launch_ms,

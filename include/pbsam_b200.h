@@ -50,7 +50,7 @@ typedef struct pbsam_params {
   double min_sep_numeric; /* MINSEPDIST, src/molecule.h:22 (5) */
   int num_points_x;       /* NUM_POINTS_X cap on surface points, src/molecule.cpp:64 (10000) */
   int cluster_size;       /* CTAs (one thread-block cluster) working on each system: 0 = the largest
-                             of 8, 4, 2 that keeps a whole batch resident at once; 1..8 forces it;
+                             of 16, 8, 4, 2 that keeps a whole batch resident at once; 1..16 forces it;
                              -1 = adaptive: after each evaluation the systems are regrouped by its
                              inner-iteration counts, costlier systems getting larger clusters (the
                              rounding of the results may then differ between calls by ~1e-15).

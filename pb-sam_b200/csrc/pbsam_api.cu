@@ -157,14 +157,14 @@ struct pbsam_system {
   // evaluation, one launch per crew size on side streams
   bool adaptive = false;
   int *h_stats = nullptr, *h_list = nullptr, *d_list = nullptr;   // pinned host / device
-  cudaEvent_t ev_stats = nullptr, ev_fork = nullptr, ev_join[4] = {nullptr, nullptr, nullptr, nullptr};
-  cudaStream_t gs[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_stats = nullptr, ev_fork = nullptr, ev_join[5] = {};
+  cudaStream_t gs[5] = {};
   bool stats_pending = false;
   std::vector<int> gsize, gcount;    // per launch: crew size, systems (lists concatenated in d_list)
 };
 
 // Crew sizes from the last evaluation's inner-iteration counts: every system starts
-// with one CTA, the one with the largest cost per CTA doubles (up to 8) while the
+// with one CTA, the one with the largest cost per CTA doubles (up to 16) while the
 // crews fit in the SMs.  Returns per system its crew size.
 static std::vector<int> plan_crews(const int *its, int B, int n_sm)
 {
@@ -174,7 +174,7 @@ static std::vector<int> plan_crews(const int *its, int B, int n_sm)
     int best = -1;
     double bc = -1.0;
     for (int b = 0; b < B; b++) {
-      if (C[b] >= 8) continue;
+      if (C[b] >= PBSAM_MAX_CREW) continue;
       const double v = (its[b] + 1.0) / C[b];
       if (v > bc) { bc = v; best = b; }
     }
@@ -205,8 +205,8 @@ extern "C" int pbsam_context_create(const pbsam_params *prm, int device, pbsam_c
 {
   if (!prm || !out) return fail(PBSAM_E_BADARG, "null argument");
   if (prm->poles < 1 || prm->poles > 32) return fail(PBSAM_E_BADARG, "poles must be in [1, 32]");
-  if (prm->cluster_size < -1 || prm->cluster_size > 8)
-    return fail(PBSAM_E_BADARG, "cluster_size must be -1 (adaptive), 0 (automatic) or 1..8");
+  if (prm->cluster_size < -1 || prm->cluster_size > PBSAM_MAX_CREW)
+    return fail(PBSAM_E_BADARG, "cluster_size must be -1 (adaptive), 0 (automatic) or 1..16");
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
   if (device < 0 || device >= ndev) return fail(PBSAM_E_BADARG, "no such CUDA device");
@@ -489,13 +489,13 @@ static cudaError_t launch_crews(void (*kern)(Exp...), int n_sys, int C, size_t s
   return cudaLaunchKernelEx(&cfg, kern, std::forward<Act>(args)...);
 }
 
-// CTAs per system: the requested size, or the largest of 8, 4, 2 at which all
+// CTAs per system: the requested size, or the largest of 16, 8, 4, 2 at which all
 // n_sys crews are resident at once (cluster occupancy), else 1.
 template <class K>
 static int pick_crew(K kern, int n_sys, size_t smem, int requested)
 {
   if (requested > 0) return requested;
-  for (int C : {8, 4, 2}) {
+  for (int C : {16, 8, 4, 2}) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(n_sys * C));
     cfg.blockDim = dim3(PBSAM_TEAM);
@@ -519,6 +519,9 @@ static int set_smem_attrs(int NP)
 {
   const int smem = (int)team_smem_bytes(NP);
   CK(cudaFuncSetAttribute(pbsam_forces_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  // clusters of up to 16 CTAs (beyond the portable 8)
+  CK(cudaFuncSetAttribute(pbsam_forces_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  CK(cudaFuncSetAttribute(pbsam_selfpol_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   CK(cudaFuncSetAttribute(pbsam_energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   CK(cudaFuncSetAttribute(pbsam_setup1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   CK(cudaFuncSetAttribute(pbsam_setup2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -695,7 +698,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   chk(dalloc(Bf, &bv.sep, B * S * S));
   s->adaptive = c->prm.cluster_size < 0;
   s->crew = pick_crew(pbsam_forces_kernel, B, team_smem_bytes(NP), s->adaptive ? 0 : c->prm.cluster_size);
-  bv.crew = s->adaptive ? 8 : s->crew;       // scratch blocks per system: the largest crew it may get
+  bv.crew = s->adaptive ? PBSAM_MAX_CREW : s->crew;   // scratch blocks per system: the largest crew it may get
   bv.scr_stride = scr_doubles(NP, S);
   chk(dalloc(Bf, &bv.scr, (size_t)B * bv.crew * bv.scr_stride));
   if (s->adaptive) chk(dalloc(Bf, &s->d_list, B));
@@ -721,7 +724,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
       r = fail(PBSAM_E_NOMEM, "pinned host buffers");
     cudaEventCreateWithFlags(&s->ev_stats, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
-    for (int g = 0; g < 4; g++) {
+    for (int g = 0; g < 5; g++) {
       cudaEventCreateWithFlags(&s->ev_join[g], cudaEventDisableTiming);
       cudaStreamCreateWithFlags(&s->gs[g], cudaStreamNonBlocking);
     }
@@ -754,7 +757,7 @@ extern "C" int pbsam_system_destroy(pbsam_system *s)
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
   if (s->adaptive) {
-    for (int g = 0; g < 4; g++) {
+    for (int g = 0; g < 5; g++) {
       if (s->gs[g]) { cudaStreamSynchronize(s->gs[g]); cudaStreamDestroy(s->gs[g]); }
       if (s->ev_join[g]) cudaEventDestroy(s->ev_join[g]);
     }
@@ -801,7 +804,7 @@ extern "C" int pbsam_system_compute_forces(pbsam_system *s, double *force, doubl
     CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, s->ctx->device));
     const std::vector<int> C = plan_crews(its.data(), s->B, n_sm - n_sm / 16);
     std::vector<int> gsize, gcount, list;
-    for (int size : {8, 4, 2, 1}) {
+    for (int size : {16, 8, 4, 2, 1}) {
       int cnt = 0;
       for (int b = 0; b < s->B; b++)
         if (C[b] == size) { list.push_back(b); cnt++; }

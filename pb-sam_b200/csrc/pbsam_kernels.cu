@@ -16,6 +16,7 @@ namespace pbsam {
 namespace cg = cooperative_groups;
 
 #define PBSAM_TEAM 512
+#define PBSAM_MAX_CREW 16       // CTAs (one thread-block cluster) per system at most
 
 // ------------------------------------------------------------------ scratch
 struct Scr {
@@ -65,11 +66,11 @@ __host__ __device__ inline size_t imat_stride(int NP2) { return (size_t)NP2 * im
 // numeric-expansion tile: per point the P^2 harmonics, 2 x P radial factors,
 // 5 geometry words and 2 x 3 weights
 __host__ __device__ inline size_t tile_point_bytes(int NP) { return ((size_t)NP * NP + 2 * NP + 11) * sizeof(double); }
-// F/H solve state kept in shared memory: F, H, new H, F base, H base, H at entry
-// (3 operands each) and a degree table
+// F/H solve state kept in shared memory: F, H, new H, F base, H base (3 operands
+// each) and a degree table
 __host__ __device__ inline size_t solve_state_bytes(int NP)
 {
-  return 6 * 3 * (size_t)NP * NP * sizeof(double) + (size_t)NP * NP * sizeof(short) + 16;
+  return 5 * 3 * (size_t)NP * NP * sizeof(double) + (size_t)NP * NP * sizeof(short) + 16;
 }
 __host__ __device__ inline size_t dyn_region_bytes(int NP)
 {
@@ -818,10 +819,10 @@ __device__ __forceinline__ void imat_apply(const Team &tm, const double *IMT, in
 // no helper reads the leader's shared memory after it has gone.
 struct CrewCmd {
   int op;                 // 0: exit, 1: matvec, 2: numeric expansion, 3: DTA list, 4: gradient pairs, 5: surface charges
-  int D, NP2, ld;         // matvec: rows of IMT times the pushed operands into the leader's shared
-  const double *IMT;      // memory at offset yoff from its tile region
-  long long yoff;
-  const double *scale;
+  int D, ts;              // F/H solve of type sphere ts with D operands
+  double *F, *H;
+  const double *LF, *LH;
+  double *xg;             // the leader's exchange buffers (new F rows, new H rows)
   int NC, N;              // numeric expansion
   const double *pts;
   double shift[3], nscale;
@@ -844,11 +845,12 @@ __device__ __forceinline__ void crew_post(const Team &tm, const Crew &cw, const 
 {
   constexpr int NW = sizeof(CrewCmd) / sizeof(unsigned long long);
   static_assert(sizeof(CrewCmd) % sizeof(unsigned long long) == 0, "command block size");
-  if (tm.rank >= NW * cw.size) return;
   cg::cluster_group cl = cg::this_cluster();
-  const int q = tm.rank / NW, w = tm.rank % NW;
-  unsigned long long *dst = (unsigned long long *)cl.map_shared_rank(cw.cmd, q);
-  dst[w] = ((const unsigned long long *)&c)[w];
+  for (int t = tm.rank; t < NW * cw.size; t += tm.size) {
+    const int q = t / NW, w = t % NW;
+    unsigned long long *dst = (unsigned long long *)cl.map_shared_rank(cw.cmd, q);
+    dst[w] = ((const unsigned long long *)&c)[w];
+  }
 }
 
 __device__ __forceinline__ void crew_rows(int NP2, int rank, int size, int &r0, int &r1)
@@ -858,29 +860,6 @@ __device__ __forceinline__ void crew_rows(int NP2, int rank, int size, int &r0, 
   r1 = r0 + per;
   if (r0 > NP2) r0 = NP2;
   if (r1 > NP2) r1 = NP2;
-}
-
-// Y (the leader's shared memory) = scale[n] * IMat x for the crew: the operands were
-// pushed into every CTA's operand buffer; each CTA applies its share of the rows
-// and stores them straight into the leader's Y.
-__device__ void crew_imat_apply(const Team &tm, const Crew &cw, const Scr &sc, const double *IMT, int NP2, int D,
-                                double *Y, const double *scale)
-{
-  if (cw.size == 1) {
-    tm.sync();
-    imat_apply(tm, IMT, sc.ld, sc.xs, NP2, D, 0, NP2, Y, scale);
-    tm.sync();
-    return;
-  }
-  cg::cluster_group cl = cg::this_cluster();
-  CrewCmd c;
-  c.op = 1; c.D = D; c.NP2 = NP2; c.ld = sc.ld; c.IMT = IMT; c.yoff = (long long)(Y - sc.tile); c.scale = scale;
-  crew_post(tm, cw, c);
-  cl.sync();                    // operands and command visible to the crew
-  int r0, r1;
-  crew_rows(NP2, 0, cw.size, r0, r1);
-  imat_apply(tm, IMT, sc.ld, sc.xs, NP2, D, r0, r1, Y, scale);
-  cl.sync();                    // every CTA's rows are in the leader's Y
 }
 
 // Numeric expansion (numeric_expand2) shared by the crew: each CTA sums a share of
@@ -900,12 +879,12 @@ __device__ void crew_numeric_expand2(const Team &tm, const Crew &cw, const Tab &
   cl.sync();
   numeric_expand2<NC>(tm, T, sc, pts, N, shift, scale, A, B, 0, cw.size, sc.tile);
   cl.sync();                    // every CTA's partial sums are in its shared memory
-  const double *parts[8];
-  for (int q = 0; q < cw.size && q < 8; q++) parts[q] = cl.map_shared_rank(sc.tile, q);
+  const double *parts[PBSAM_MAX_CREW];
+  for (int q = 0; q < cw.size; q++) parts[q] = cl.map_shared_rank(sc.tile, q);
   const int NP2 = T.NP * T.NP, nsets = B.w ? 2 : 1;
   for (int u = tm.rank; u < nsets * NC * NP2; u += tm.size) {
     double v = 0.0;
-    for (int q = 0; q < cw.size && q < 8; q++) v += parts[q][u];
+    for (int q = 0; q < cw.size; q++) v += parts[q][u];
     const int set = u / (NC * NP2);
     (set ? B.out : A.out)[u - set * NC * NP2] = v;
   }
@@ -965,35 +944,37 @@ __device__ void crew_finish(const Team &tm, const Crew &cw)
 // (CSolExpCenter::solveFH, src/expcenter.cpp:1079-1370) for D = 1 (F, H) or
 // D = 3 (x, y, z gradients).  F and H (D*NP2) are updated in place; returns the
 // deviation of H from its value on entry (computeDev2).
-__device__ double solve_fh(const Team &tm, const Crew &cw, double *tph, const Tab &T, const TypeView &tv,
-                           const SolveParams &prm, const Scr &sc,
-                           int ts, int D, double *F, double *H, const double *LF, const double *LH, double *red,
-                           int *stats)
+// The F/H inner solve, run by every CTA of the crew on a full copy of the state in
+// its shared memory: each CTA forms the operands itself and applies its share of
+// the IMat rows, writing them to the exchange buffer xg in global memory (L2); after
+// one cluster barrier per matvec every CTA reads the whole new F (H) back.  The new
+// F and the new H have separate exchange buffers, and every CTA takes the same
+// stopping decision from identical data.  Returns computeDev2 on the leader (rank
+// 0), which writes F and H back to the system state.
+__device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double *tph, const Tab &T,
+                                          const TypeView &tv, const SolveParams &prm, const Scr &sc, double *xg,
+                                          int ts, int D, double *F, double *H, const double *LF, const double *LH,
+                                          double *red, int *stats)
 {
   const int NP = T.NP, NP2 = NP * NP, len = D * NP2;
   const double *cst = tv.cst + (size_t)ts * CST_N * NP;
   const double *Dfix = tv.Dfix + (size_t)ts * NP2, *Vfix = tv.Vfix + (size_t)ts * NP2;
   const double *IMT = tv.imat + (size_t)ts * imat_stride(NP2);
   const int ld = sc.ld;
-  // state in shared memory for the whole solve
-  double *sF = sc.tile, *sH = sF + len, *sHn = sH + len, *sFb = sHn + len, *sHb = sFb + len, *sOut = sHb + len;
-  short *deg = (short *)(sOut + len);
-  // operand buffers of every CTA of the crew (the leader's own first)
+  double *sF = sc.tile, *sH = sF + len, *sHn = sH + len, *sFb = sHn + len, *sHb = sFb + len;
+  short *deg = (short *)(sHb + len);
+  double *xgF = xg, *xgH = xg + 3 * NP2;     // exchange buffers (global, the leader's scratch)
+  double *sOut = xg + 6 * NP2;               // H at entry (leader only)
+  const bool lead = cw.rank == 0, crew = cw.size > 1;
   cg::cluster_group cl = cg::this_cluster();
-  double *ox[8];
-  const int nc = cw.size < 8 ? cw.size : 8;
-  for (int q = 0; q < nc; q++) ox[q] = (q == 0) ? sc.xs : cl.map_shared_rank(sc.xs, q);
   for (int k = tm.rank; k < NP2; k += tm.size) {
     int n = (int)sqrt((double)k);
     while (n * n > k) n--;
     while ((n + 1) * (n + 1) <= k) n++;
     deg[k] = (short)n;
   }
-  // the operands' pad columns stay zero (the IMat pad column is zero too)
-  for (int u = tm.rank; u < D * (ld - NP2) * nc; u += tm.size) {
-    const int q = u / (D * (ld - NP2)), r = u % (D * (ld - NP2));
-    ox[q][(r / (ld - NP2)) * ld + NP2 + r % (ld - NP2)] = 0.0;
-  }
+  for (int d = tm.rank; d < D; d += tm.size)
+    for (int k = NP2; k < ld; k++) sc.xs[d * ld + k] = 0.0;   // pad columns (the IMat's are zero too)
   tm.sync();
   for (int k = tm.rank; k < len; k += tm.size) {
     const int kk = k % NP2, n = deg[kk];
@@ -1007,9 +988,11 @@ __device__ double solve_fh(const Team &tm, const Crew &cw, double *tph, const Ta
     const double h = H[k];
     sF[k] = F[k];
     sH[k] = h;
-    sOut[k] = h;
+    if (lead) sOut[k] = h;
   }
   tm.sync();
+  int r0, r1;
+  crew_rows(NP2, cw.rank, cw.size, r0, r1);
   int ct = 0;
   double dev = 0.0;
   PhaseClock mv{tph, 0};
@@ -1017,16 +1000,30 @@ __device__ double solve_fh(const Team &tm, const Crew &cw, double *tph, const Ta
     mv.start(tm);
     for (int k = tm.rank; k < len; k += tm.size) {
       const int kk = k % NP2, n = deg[kk];
-      const double v = sFb[k] + cst[CST_H1 * NP + n] * sH[k] + cst[CST_F1 * NP + n] * sF[k];
-      for (int q = 0; q < nc; q++) ox[q][(k / NP2) * ld + kk] = v;
+      sc.xs[(k / NP2) * ld + kk] = sFb[k] + cst[CST_H1 * NP + n] * sH[k] + cst[CST_F1 * NP + n] * sF[k];
     }
-    crew_imat_apply(tm, cw, sc, IMT, NP2, D, sF, T.CONST3);
+    tm.sync();
+    if (crew) {
+      imat_apply(tm, IMT, ld, sc.xs, NP2, D, r0, r1, xgF, T.CONST3);
+      cl.sync();                // every CTA's rows of the new F are in L2
+      for (int k = tm.rank; k < len; k += tm.size) sF[k] = xgF[k];
+    } else {
+      imat_apply(tm, IMT, ld, sc.xs, NP2, D, 0, NP2, sF, T.CONST3);
+    }
+    tm.sync();
     for (int k = tm.rank; k < len; k += tm.size) {
       const int kk = k % NP2, n = deg[kk];
-      const double v = sHb[k] + cst[CST_H2 * NP + n] * sH[k] + cst[CST_F2 * NP + n] * sF[k];
-      for (int q = 0; q < nc; q++) ox[q][(k / NP2) * ld + kk] = v;
+      sc.xs[(k / NP2) * ld + kk] = sHb[k] + cst[CST_H2 * NP + n] * sH[k] + cst[CST_F2 * NP + n] * sF[k];
     }
-    crew_imat_apply(tm, cw, sc, IMT, NP2, D, sHn, cst + CST_INVH * NP);
+    tm.sync();
+    if (crew) {
+      imat_apply(tm, IMT, ld, sc.xs, NP2, D, r0, r1, xgH, cst + CST_INVH * NP);
+      cl.sync();
+      for (int k = tm.rank; k < len; k += tm.size) sHn[k] = xgH[k];
+    } else {
+      imat_apply(tm, IMT, ld, sc.xs, NP2, D, 0, NP2, sHn, cst + CST_INVH * NP);
+    }
+    tm.sync();
     mv.stop(tm, PH_MATVEC);
     // computeDev over complex entries (d, n, m) of the old and new H
     double part = 0.0;
@@ -1056,10 +1053,11 @@ __device__ double solve_fh(const Team &tm, const Crew &cw, double *tph, const Ta
       part += s;
     }
     dev = team_sum(tm, part, red) / (4 * NP * NP);
-    { double *t = sH; sH = sHn; sHn = t; }    // the new H is the current one
+    { double *t = sH; sH = sHn; sHn = t; }
     ct++;
     if (!(dev > prm.solve_tol && ct < prm.solve_max_ct)) break;
   }
+  if (!lead) return 0.0;
   if (tm.rank == 0 && stats) { stats[1] += ct; stats[2] += 1; }
   // results back to the system state; computeDev2 (outer deviation)
   double pd = 0.0, ps = 0.0;
@@ -1075,6 +1073,27 @@ __device__ double solve_fh(const Team &tm, const Crew &cw, double *tph, const Ta
   }
   const double td = team_sum(tm, pd, red), tsm = team_sum(tm, ps, red);
   return td / (4 * tsm) / double(D);
+}
+
+// Fixed-point solve of one sphere's surface-charge expansions
+// (CSolExpCenter::solveFH, src/expcenter.cpp:1079-1370) for D = 1 (F, H) or
+// D = 3 (x, y, z gradients), called by the leader: F and H (D*NP2) are updated in
+// place; returns the deviation of H from its value on entry (computeDev2).
+__device__ double solve_fh(const Team &tm, const Crew &cw, double *tph, const Tab &T, const TypeView &tv,
+                           const SolveParams &prm, const Scr &sc, int ts, int D, double *F, double *H,
+                           const double *LF, const double *LH, double *red, int *stats)
+{
+  if (cw.size == 1) return solve_core(tm, cw, tph, T, tv, prm, sc, sc.sol, ts, D, F, H, LF, LH, red, stats);
+  cg::cluster_group cl = cg::this_cluster();
+  {
+    CrewCmd c;
+    c.op = 1; c.D = D; c.ts = ts; c.F = F; c.H = H; c.LF = LF; c.LH = LH; c.xg = sc.sol;
+    crew_post(tm, cw, c);
+  }
+  cl.sync();
+  const double dv = solve_core(tm, cw, tph, T, tv, prm, sc, sc.sol, ts, D, F, H, LF, LH, red, stats);
+  cl.sync();                    // the crew has left the solve
+  return dv;
 }
 
 // ------------------------------------------------------------------ system state access
@@ -1566,10 +1585,7 @@ __device__ void crew_serve(const Team &tm, const Sys &y)
     cl.sync();
     const CrewCmd c = *cw.cmd;    // posted by the leader before the barrier
     if (c.op == 1) {
-      int r0, r1;
-      crew_rows(c.NP2, cw.rank, cw.size, r0, r1);
-      double *Y = cl.map_shared_rank(sc.tile + c.yoff, 0);
-      imat_apply(tm, c.IMT, c.ld, sc.xs, c.NP2, c.D, r0, r1, Y, c.scale);
+      solve_core(tm, cw, nullptr, T, y.c->tv, y.c->prm, sc, c.xg, c.ts, c.D, c.F, c.H, c.LF, c.LH, y.red, nullptr);
     } else if (c.op == 2) {
       if (c.NC == 1)
         numeric_expand2<1>(tm, T, sc, c.pts, c.N, c.shift, c.nscale, c.A, c.B, cw.rank, cw.size, sc.tile);
