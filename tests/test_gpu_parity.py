@@ -26,12 +26,12 @@ def poses(case):
     return json.load(open(os.path.join(golden_dir(case), "poses.json")))
 
 
-def make_ctx(case, tight=False):
+def make_ctx(case, tight=False, cluster_size=0):
     import pbsam_b200 as pb
     P = poses(case)
     tol = oracle.TIGHT_TOL if tight else oracle.DEFAULT_TOL
     ctx = pb.CSystem(poles=P["poles"], salt=P["salt"], idiel=P["idiel"], max_polar_dev=tol[0],
-                     solve_tol=tol[1], solve_max_ct=tol[2], max_pol_rounds=tol[3])
+                     solve_tol=tol[1], solve_max_ct=tol[2], max_pol_rounds=tol[3], cluster_size=cluster_size)
     d = golden_dir(case)
     ta = ctx.load_moltype(d + "/molA.pqr", d + "/imA", d + "/expA", "molA.0")
     tb = ctx.load_moltype(d + "/molB.pqr", d + "/imB", d + "/expB", "molB.0")
@@ -212,3 +212,37 @@ def test_overlap_and_single_molecule(ctx_default):
     f, t, st = one.compute_forces()
     assert np.all(st == 0) and np.all(f == 0) and np.all(t == 0)
     one.close()
+
+
+def test_cluster_sizes_agree():
+    """The CTAs working on a system (1, 2, 4, 8, 16, or adaptive regrouping between
+    calls) change only the rounding.  Three calls in a row on the same poses (each
+    system keeps its state between calls, as the reference's molecules do, so the
+    later calls differ from a fresh one): the first matches the reference, and every
+    size agrees with one CTA per system, call by call, to 1e-12."""
+    P = poses("cfg0")
+    frames = [p["frame"] for p in P["poses"]]
+    pos, quat = frame_arrays(frames)
+    refs = [oracle.parse(os.path.join(golden_dir("cfg0"), "ref_default", "pose%d.txt" % k))[0]
+            for k in range(len(frames))]
+    results = {}
+    for size in (1, 2, 4, 8, 16, -1):
+        ctx, types = make_ctx("cfg0", cluster_size=size)
+        mol = ctx.molecules(types, n_systems=len(frames))
+        for call in range(3):      # adaptive: the first call is uniform, the next ones regrouped
+            mol.set_poses(pos, quat)
+            f, t, st = mol.compute_forces()
+            assert np.all(st == 0)
+            if call == 0:
+                for k in range(len(frames)):
+                    assert rel(f[k], refs[k]["force"]) < TOL and rel(t[k], refs[k]["torque"]) < TOL, (size, k)
+            results.setdefault(size, []).append((f, t))
+            if size > 0:
+                assert np.all(mol.stats()[:, 5] == size)
+        mol.close()
+        ctx.close()
+    for size, runs in results.items():
+        for call, (f, t) in enumerate(runs):
+            f1, t1 = results[1][call]
+            for k in range(len(frames)):
+                assert rel(f[k], f1[k]) < 1e-12 and rel(t[k], t1[k]) < 1e-12, (size, call, k)
