@@ -236,12 +236,155 @@ def run_ours(args):
         }
         if args.cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(cfg, specs, pos, quat, stats, args)
+    sysb.close()
+    ctx.close()
+    if args.bd:
+        try:
+            bd = run_bd(args, local, rank, world, dist)
+        except Exception as e:   # the headline line stands without the BD leg
+            bd = {"error": "%s: %s" % (type(e).__name__, e), "gpu_launches": 0}
+        if out is not None:
+            out["bd"] = bd
+            out["gpu_launches"] += bd["gpu_launches"]
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    return out
+
+
+# ---------------------------------------------------------------- Brownian dynamics leg
+BD_METRIC = "BD steps/s (two-molecule bdnam trajectories, p=10)"
+BD_WORKLOAD = ("bdnam p=10: %d trajectories of 2 molecules x 35 spheres (r 3-6 A, 1200 charges, net +2/-2), start "
+               "50 A, escape 150 A, dt 0.02 ps at contact rising to 2 ps at a 30 A gap, Stokes-Einstein D, Philox "
+               "noise; a step = force evaluation (where c2c < 100 A) + Ermak-McCammon move, one CUDA graph")
+
+
+def run_bd(args, local, rank, world, dist):
+    """BD steps per second of a batch of independent two-molecule trajectories:
+    every step (a CUDA graph: time step and force mask, force kernel, move kernel)
+    of every trajectory counts as one unit."""
+    import torch
+    from pbsam_b200 import replicas, workload
+    cfg = dict(workload.BD_P10)
+    specs, prep_t, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds_p10)
+    ctx, types = workload.open_context(cfg, specs, device=local)
+    mols = workload.molecules(cfg)
+    B = args.bd_traj
+    pos, quat = workload.bd_start(cfg, mols, B, rank=rank)
+    ext = max(m.extent() for m in mols)
+    dtr, drot = workload.stokes_einstein(ext, cfg["viscosity"], cfg["temperature"])
+    sysb = ctx.molecules(types, n_systems=B)
+    stream = torch.cuda.current_stream()
+    sysb.set_stream(stream.cuda_stream)
+    sysb.set_poses(pos, quat)
+    sysb.bd_init([0.0, dtr], [drot, drot], mode=0, seed=1234 + rank, escape_dist=cfg["escape"],
+                 dt_min=cfg["dt_min"], dt_max=cfg["dt_max"], dt_ref=0.0,
+                 dt_div=cfg["dt_gap"] / (cfg["dt_max"] - cfg["dt_min"]))
+    sysb.bd_run(args.warmup)
+    torch.cuda.synchronize()
+    s0 = sysb.bd_state()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_id_for_smi(local)) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sysb.bd_run(args.bd_steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clocks = clk.summary()
+    s1 = sysb.bd_state()
+    ms_max = replicas.max_over_ranks(ms, dist if world > 1 else None)
+    units = int(np.sum(s1["steps"] - s0["steps"]))
+    fe = int(np.sum(s1["fevals"] - s0["fevals"]))
+    units_all = replicas.sum_over_ranks(units, dist if world > 1 else None)
+    # e2e: one step at a time through the public API with the poses, statuses and
+    # counters read back to the host after every step
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_e2e = max(1, args.bd_steps // 2)
+    torch.cuda.synchronize()
+    ee0.record(stream)
+    for _ in range(n_e2e):
+        sysb.bd_run(1)
+        st = sysb.bd_state()
+    ee1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = replicas.max_over_ranks(ee0.elapsed_time(ee1), dist if world > 1 else None)
+    e2e_units = replicas.sum_over_ranks(int(np.sum(st["steps"] - s1["steps"])), dist if world > 1 else None)
+    d2h = sum(int(v.nbytes) for v in st.values())
+    out = {"metric": BD_METRIC, "value": units_all / (ms_max * 1e-3), "unit": "BD steps/s",
+           "ms_per_step": ms_max / args.bd_steps, "steps": args.bd_steps, "warmup": args.warmup, "dtype": "f64",
+           "config": {"workload": BD_WORKLOAD % B, "trajectories_per_gpu": B, "dtr_A2_per_ps": dtr,
+                      "drot_rad2_per_ps": drot},
+           "force_evaluations_fraction": fe / max(units, 1),
+           "status_counts": {pb_status: int(np.sum(s1["status"] == k)) for k, pb_status in
+                             ((0, "running"), (1, "escaped"), (2, "stuck"), (4, "failed"))},
+           "e2e": {"value": e2e_units / (e2e_ms * 1e-3), "unit": "BD steps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": d2h, "note": "one step per call, state read back to the host each step"},
+           "gpu_launches": 3 * args.bd_steps, "clocks": clocks, "prep": prep_t}
+    if rank == 0 and args.cpu_baseline:
+        out["cpu_baseline"] = bd_cpu_baseline(cfg, specs, sysb, s1, fe / max(units, 1), args)
     sysb.close()
     ctx.close()
     return out
+
+
+def bd_cpu_baseline(cfg, specs, sysb, state, force_frac, args):
+    """The reference's computeForces (p = 10 build) on consecutive poses of sampled
+    trajectories: for each, the harness evaluates the pose before the last step
+    (untimed, it sets up the carried solver state as in a BD run) and then the pose
+    after it (timed), one single-threaded process per trajectory on all host cores.
+    BD steps/s = cores / (mean force time x fraction of steps with forces); the
+    move itself (a few hundred distance tests) is not counted."""
+    from pbsam_b200 import workload
+    if not os.path.exists(_ref_harness(cfg["poles"])):
+        return {"value": None, "unit": "BD steps/s", "cores": 0, "kind": "reference",
+                "sample": "reference binary not built"}
+    ncores = os.cpu_count() or 1
+    run = [b for b in range(len(state["status"])) if state["status"][b] == 0]
+    sel = run[:: max(1, len(run) // ncores)][:ncores]
+    sysb.bd_run(1)
+    after = sysb.bd_state()
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        files = workload.write_inputs(cfg, specs, td)
+        procs = []
+        for j in sel:
+            spec = os.path.join(td, "bd%d.txt" % j)
+            with open(spec, "w") as fh:
+                fh.write("salt %r\nidiel %r\ndump 0\nenergy 0\n" % (cfg["salt"], cfg["idiel"]))
+                for fl in files:
+                    fh.write("moltype %s %s %s %s\n" % fl)
+                for s in (state, after):
+                    fh.write("frame\n")
+                    for m in range(2):
+                        fh.write("mol %d %s %s\n" % (m, " ".join("%.17g" % v for v in s["pos"][j, m]),
+                                                     " ".join("%.17g" % v for v in s["quat"][j, m])))
+            env = dict(os.environ, OMP_NUM_THREADS="1")
+            procs.append((spec, subprocess.Popen([_ref_harness(cfg["poles"]), spec, spec + ".out"], env=env,
+                                                 stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)))
+        import oracle
+        t0 = time.time()
+        for spec, p in procs:
+            try:
+                p.wait(timeout=max(1.0, args.cpu_limit - (time.time() - t0)))
+            except subprocess.TimeoutExpired:
+                p.kill()
+                p.wait()
+                continue
+            if p.returncode == 0:
+                fr = oracle.parse(spec + ".out")
+                if len(fr) == 2 and fr[1]["ok"]:
+                    times.append(float(fr[1]["info"][0]))
+    if not times:
+        return {"value": None, "unit": "BD steps/s", "cores": ncores, "kind": "reference",
+                "sample": "no trajectory finished"}
+    t = float(np.mean(times))
+    return {"value": ncores / (t * max(force_frac, 1e-9)), "unit": "BD steps/s", "cores": ncores,
+            "kind": "reference",
+            "sample": "%d trajectories, the force call of one step each (mean %.3f s, 1 thread per process), scaled "
+                      "by the fraction of steps with forces (%.3f)" % (len(times), t, force_frac)}
 
 
 # ---------------------------------------------------------------- reference CPU leg
@@ -397,6 +540,10 @@ def main():
     ap.add_argument("--cpu-limit", type=int, default=60, help="seconds before a sample pose is abandoned")
     ap.add_argument("--cluster-size", type=int, default=-1,
                     help="CTAs per system (0: automatic, -1: adaptive from the previous step's costs)")
+    ap.add_argument("--bd", type=int, default=1, help="also time the Brownian-dynamics workload")
+    ap.add_argument("--bd-traj", type=int, default=1024, help="BD trajectories per GPU")
+    ap.add_argument("--bd-steps", type=int, default=20, help="timed BD steps")
+    ap.add_argument("--selfpol-rounds-p10", type=int, default=200)
     ap.add_argument("--poses", default="", help="comma-separated subset of the sweep's poses (small cases)")
     ap.add_argument("--traffic-per-launch", type=float, default=None,
                     help="DRAM bytes per launch measured by ncu (scaled from a small capture)")

@@ -136,6 +136,63 @@ int pbsam_system_phase_ms(const pbsam_system *sys, double *ms);
 /* Device time in milliseconds of the last force-kernel launch (CUDA events). */
 int pbsam_system_last_kernel_ms(const pbsam_system *sys, double *ms);
 
+/* Brownian dynamics on the force path: the Ermak-McCammon step of the reference's
+ * drivers, for every system of a batch (each system one trajectory).
+ *   PBSAM_BD_NAM   = CBDnam::run / makeMove / compute_dt (src/BDnam.cpp:166-417):
+ *                    two molecules, molecule 0 rotates in place, molecule 1
+ *                    translates and rotates; forces while the centre distance is
+ *                    below force_dist; PBSAM_BD_ESCAPED beyond escape_dist;
+ *                    PBSAM_BD_STUCK after max_tries rejected draws.
+ *   PBSAM_BD_MULTI = CBDmulti::propagate / makeMove / compute_dt / computeMinSepDist
+ *                    (src/BDmulti.cpp:396-566): every molecule moves in turn;
+ *                    forces while the minimum separation is below the context's
+ *                    interaction cutoff (no periodic box).
+ * Time step dt = min(dt_max, dt_min + max(0, d - dt_ref) / dt_div) ps, d the
+ * molecule gap (NAM) or the minimum separation (MULTI); drifts D*dt*fact_tr*F and
+ * Dr*dt*ikbt*coul_k*torque; noise N(0, 2*D*dt) per component from Philox4x64-10
+ * (key = seed, counter = (draw, system)) where the reference uses drand48.
+ * Docking (contact lists, PBSAM_BD_DOCKED) is not evaluated.  A force evaluation
+ * that finds overlapping spheres ends the trajectory with PBSAM_BD_FAILED, where the
+ * reference exits (src/BDnam.cpp:210-212). */
+#define PBSAM_BD_NAM 0
+#define PBSAM_BD_MULTI 1
+#define PBSAM_BD_RUNNING 0
+#define PBSAM_BD_ESCAPED 1
+#define PBSAM_BD_STUCK 2
+#define PBSAM_BD_DOCKED 3
+#define PBSAM_BD_FAILED 4
+
+typedef struct pbsam_bd_params {
+  int mode;              /* PBSAM_BD_NAM or PBSAM_BD_MULTI */
+  int max_tries;         /* draws per move before giving up (maxc = 500) */
+  double force_dist;     /* NAM: forces while centre distance < this (f_DIST = 100) */
+  double escape_dist;    /* NAM: escape radius (q_DIST = 500) */
+  double dt_min, dt_max, dt_ref, dt_div;   /* time-step schedule (2, none, 5 or 10, 15) */
+  double fact_tr;        /* FACT2 = 560.4586 */
+  double ikbt;           /* IKbT = 1/(kB*298.15) */
+  double coul_k;         /* COUL_K = 2.30708e-18 */
+  unsigned long long seed;
+  int use_graph;         /* 1: a step is replayed as one CUDA graph */
+} pbsam_bd_params;
+
+/* Reference values of the chosen driver (src/BDnam.h:10-25, src/BDmulti.cpp:13,
+ * src/BDnam.cpp:409-417). */
+void pbsam_bd_params_default(int mode, pbsam_bd_params *prm);
+/* Start a trajectory in every system from its current poses (set them first with
+ * pbsam_system_set_poses): dtr/drot[n_mol] translational (A^2/ps) and rotational
+ * (rad^2/ps) diffusion coefficients per molecule (the reference's m_Dtr, m_Dr1,
+ * m_Dr2, src/BDnam.cpp:145, src/BDmulti.cpp:204-205). */
+int pbsam_system_bd_init(pbsam_system *sys, const pbsam_bd_params *prm, const double *dtr, const double *drot);
+/* Queue n_steps steps of every running trajectory on the system's stream (the
+ * while loop of CBDnam::run, src/BDnam.cpp:196-243); returns without waiting.
+ * Trajectories that stopped (escaped, stuck, failed) are left as they are. */
+int pbsam_system_bd_run(pbsam_system *sys, int n_steps);
+/* Poses pos[n_systems*n_mol*3], quat[n_systems*n_mol*4], status[n_systems]
+ * (PBSAM_BD_*), steps taken, simulated time (ps) and force evaluations per
+ * trajectory.  Any pointer may be NULL. */
+int pbsam_system_bd_state(pbsam_system *sys, double *pos, double *quat, int *status, int *steps, double *time,
+                          int *fevals, int on_device);
+
 /* Molecule-type preparation (the reference's `pbsam mat` and `pbsam spol`).
  *
  * Surface-integral matrices of a molecule's spheres: replaces the CMolecule IMat

@@ -52,6 +52,59 @@ def write_spec(path, moltypes, frames, salt=0.05, idiel=4.0, poles=10, tol=DEFAU
                 fh.write("mol %d %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n" % tuple([t] + list(pos) + list(q)))
 
 
+BD_DEFAULT = dict(max_tries=500, force_dist=100.0, escape_dist=500.0, dt_min=2.0, dt_max=1e300, dt_ref=5.0,
+                  dt_div=15.0)
+
+
+def write_bd_spec(path, moltypes, frame, mode, n_steps, seed, system, dtr, drot, salt=0.05, idiel=4.0, poles=10,
+                  tol=DEFAULT_TOL, **bdp):
+    """Brownian dynamics from one frame's poses (the oracle's BD mode): n_steps steps of
+    trajectory `system` (the noise counter's system word) with the given seed."""
+    p = dict(BD_DEFAULT)
+    if mode == 1:
+        p["dt_ref"] = 10.0
+    p.update(bdp)
+    write_spec(path, moltypes, [frame], salt=salt, idiel=idiel, poles=poles, tol=tol, energy=0)
+    with open(path, "a") as fh:
+        fh.write("bd %d %d %d %d\n" % (mode, n_steps, seed, system))
+        fh.write("bdp %d %r %r %r %r %r %r\n" % (p["max_tries"], p["force_dist"], p["escape_dist"], p["dt_min"],
+                                                  p["dt_max"], p["dt_ref"], p["dt_div"]))
+        for a, b in zip(dtr, drot):
+            fh.write("bddiff %r %r\n" % (a, b))
+
+
+def run_bd_spec(spec, out):
+    """Returns per step dict(steps, status, fevals, time, pos[n,3], quat[n,4])."""
+    rc = liboracle().pbsam_oracle_run(spec.encode(), out.encode())
+    if rc != 0:
+        raise RuntimeError("oracle failed with status %d" % rc)
+    steps = []
+    with open(out) as fh:
+        for ln in fh:
+            t = ln.split()
+            if t and t[0] == "BDSTEP":
+                steps.append(dict(steps=int(t[1]), status=int(t[2]), fevals=int(t[3]), time=float(t[4]), pos={},
+                                  quat={}))
+            elif t and t[0] == "POSE":
+                v = [float(x) for x in t[2:]]
+                steps[-1]["pos"][int(t[1])] = v[:3]
+                steps[-1]["quat"][int(t[1])] = v[3:]
+    for s in steps:
+        n = len(s["pos"])
+        s["pos"] = np.array([s["pos"][i] for i in range(n)])
+        s["quat"] = np.array([s["quat"][i] for i in range(n)])
+    return steps
+
+
+def philox(counter, key):
+    """One Philox4x64-10 block of the oracle's noise generator."""
+    lib = liboracle()
+    c = (ctypes.c_ulonglong * 4)(*[int(x) for x in counter])
+    lib.pbsam_oracle_philox.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_ulonglong, ctypes.c_ulonglong]
+    lib.pbsam_oracle_philox(c, int(key[0]), int(key[1]))
+    return [int(x) for x in c]
+
+
 def run_spec(spec, out):
     rc = liboracle().pbsam_oracle_run(spec.encode(), out.encode())
     if rc != 0:

@@ -1757,6 +1757,213 @@ struct System {
       }
     return pot;
   }
+
+  // ---------------------------------------------------------------- Brownian dynamics
+  // The Ermak-McCammon step of the reference's drivers: CBDnam::run / makeMove /
+  // compute_dt (src/BDnam.cpp:166-417) and CBDmulti::propagate / makeMove /
+  // compute_dt / computeMinSepDist (src/BDmulti.cpp:396-566).  Noise: Philox4x64-10
+  // (Salmon et al., SC 2011), key (seed, 0), counter (draw, system, 0, 0), four
+  // uniforms ((x >> 11) + 0.5) 2^-53 and the Box-Muller transform give one random
+  // vector (the reference draws from drand48 with the polar method).
+  struct BD {
+    int mode = 0, max_tries = 500;
+    double force_dist = 100, escape_dist = 500, dt_min = 2, dt_max = 1e300, dt_ref = 5, dt_div = 15;
+    double fact_tr = 5.604586e2, ikbt = 1.0 / (1.3806503e-23 * 298.15), coul_k = 2.30708e-18;
+    unsigned long long seed = 0, ctr = 0;
+    int sys = 0, status = 0, steps = 0, fevals = 0;
+    double time = 0;
+    std::vector<double> dtr, drot;
+    std::vector<Quat> rot;
+  } bd;
+
+  static void philox(unsigned long long c[4], unsigned long long k0, unsigned long long k1)
+  {
+    const unsigned long long M0 = 0xD2E7470EE14C6C93ULL, M1 = 0xCA5A826395121157ULL;
+    const unsigned long long W0 = 0x9E3779B97F4A7C15ULL, W1 = 0xBB67AE8584CAA73BULL;
+    for (int r = 0; r < 10; r++) {
+      if (r) { k0 += W0; k1 += W1; }
+      unsigned __int128 p0 = (unsigned __int128)M0 * c[0], p1 = (unsigned __int128)M1 * c[2];
+      unsigned long long hi0 = (unsigned long long)(p0 >> 64), lo0 = (unsigned long long)p0;
+      unsigned long long hi1 = (unsigned long long)(p1 >> 64), lo1 = (unsigned long long)p1;
+      unsigned long long n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+      c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+    }
+  }
+  P3 rand_vec(double sd)   // CBDnam::getRandVec (src/BDnam.h:44-45)
+  {
+    unsigned long long c[4] = {bd.ctr++, (unsigned long long)bd.sys, 0ULL, 0ULL};
+    philox(c, bd.seed, 0ULL);
+    double u[4];
+    for (int i = 0; i < 4; i++) u[i] = ((double)(c[i] >> 11) + 0.5) * 0x1p-53;
+    const double r0 = sqrt(-2.0 * log(u[0])), r1 = sqrt(-2.0 * log(u[2]));
+    return sd * P3(r0 * cos(2.0 * M_PI * u[1]), r0 * sin(2.0 * M_PI * u[1]), r1 * cos(2.0 * M_PI * u[3]));
+  }
+  static Quat qraw(double w, const P3 &v) { Quat q; q.w = w; q.v = v; return q; }
+  static Quat qmul(const Quat &a, const Quat &b)   // a * b: b *= a (src/util.h:242-263)
+  {
+    return qraw(a.w * b.w - dot(a.v, b.v), (a.w * b.v + b.w * a.v) + cross(a.v, b.v));
+  }
+  static Quat axis_angle(const P3 &ax, double angle)   // CQuat(axis, angle), src/util.h:220-229
+  {
+    if (angle != 0.0 && ax.norm2() != 0.0) return Quat(cos(0.5 * angle), sin(0.5 * angle) * ((1.0 / ax.norm()) * ax));
+    return Quat();
+  }
+  double c2c(int i, int j) const { return (mols[i].rcen - mols[j].rcen).norm(); }
+  double mol_gap(int i, int j) const
+  {
+    return c2c(i, j) - types[mols[i].type].maxR - types[mols[j].type].maxR;
+  }
+  void rotate(int i, const Quat &dq)   // CMolecule::rotate (src/moldynamics.cpp:666-679)
+  {
+    Molecule &M = mols[i];
+    M.orient = qmul(dq, M.orient);
+    for (size_t k = 0; k < M.s.size(); k++) M.s[k].cenRot = qrot(M.orient, st(i, k).cen);
+  }
+  bool is_collided(int i) const   // src/moldynamics.cpp:167-193
+  {
+    for (size_t j = 0; j < mols.size(); j++) {
+      if ((int)j == i || mol_gap(i, j) > 0) continue;
+      for (size_t ki = 0; ki < mols[i].s.size(); ki++)
+        for (size_t kj = 0; kj < mols[j].s.size(); kj++) {
+          P3 d = ((mols[i].rcen + mols[i].s[ki].cenRot) - mols[j].rcen) - mols[j].s[kj].cenRot;
+          if ((d.norm() - st(i, ki).rad) - st(j, kj).rad < 0.0) return true;
+        }
+    }
+    return false;
+  }
+  bool will_rot_collide(int i, const Quat &dq) const   // src/moldynamics.cpp:43-85
+  {
+    const Quat Q = qmul(dq, mols[i].orient);
+    for (size_t j = 0; j < mols.size(); j++) {
+      if ((int)j == i || mol_gap(i, j) > 0) continue;
+      for (size_t ki = 0; ki < mols[i].s.size(); ki++) {
+        const P3 cki = mols[i].rcen + qrot(Q, st(i, ki).cen);
+        for (size_t kj = 0; kj < mols[j].s.size(); kj++) {
+          P3 d = (cki - mols[j].rcen) - mols[j].s[kj].cenRot;
+          if ((st(i, ki).rad + st(j, kj).rad) - d.norm() > 0.0) return true;
+        }
+      }
+    }
+    return false;
+  }
+  double bd_dt(double d) const
+  {
+    double dt = (d - bd.dt_ref > 0) ? bd.dt_min + (d - bd.dt_ref) / bd.dt_div : bd.dt_min;
+    return dt < bd.dt_max ? dt : bd.dt_max;
+  }
+  int translate_try(int i, const P3 &drift, double sd)
+  {
+    int c = 0;
+    bool done = false;
+    while (!done && c < bd.max_tries) {
+      c++;
+      const P3 old = mols[i].rcen;
+      mols[i].rcen = mols[i].rcen + (drift + rand_vec(sd));
+      if (is_collided(i)) mols[i].rcen = old;
+      else done = true;
+    }
+    return c;
+  }
+  int rotate_try(int i, const P3 &drift, double sd, Quat &last)
+  {
+    int c = 0;
+    bool done = false;
+    while (!done && c < bd.max_tries) {
+      c++;
+      const P3 o = drift + rand_vec(sd);
+      last = axis_angle(o, o.norm());
+      if (!will_rot_collide(i, last)) { rotate(i, last); done = true; }
+    }
+    return c;
+  }
+  // one step; returns false when a needed force evaluation failed
+  bool bd_step()
+  {
+    const int nmol = mols.size();
+    if (bd.status != 0) return true;
+    double dt, md = 0;
+    bool need;
+    if (bd.mode == 0) {
+      dt = bd_dt(mol_gap(0, 1));
+      need = c2c(0, 1) < bd.force_dist;
+    } else {
+      const double ic = prm.interact_cut;
+      const double maxd = bd.dt_ref > ic ? bd.dt_ref : ic, mind = bd.dt_ref > ic ? ic : bd.dt_ref;
+      double smin = 1e300, mmin = 1e300;
+      bool track = false;
+      for (int i = 0; i < nmol; i++)
+        for (int j = i + 1; j < nmol; j++) {
+          const double dm = mol_gap(i, j);
+          if (dm < maxd) {
+            track = true;
+            for (size_t ki = 0; ki < mols[i].s.size(); ki++)
+              for (size_t kj = 0; kj < mols[j].s.size(); kj++) {
+                P3 d = ((mols[i].rcen + mols[i].s[ki].cenRot) - mols[j].rcen) - mols[j].s[kj].cenRot;
+                const double g = (d.norm() - st(i, ki).rad) - st(j, kj).rad;
+                if (g < smin) smin = g;
+              }
+          } else if (dm < mmin) mmin = dm;
+        }
+      md = track ? (smin < mind ? mind : smin) : (mmin > 0 ? mmin : 0);
+      dt = bd_dt(md);
+      need = md < ic;
+    }
+    std::vector<P3> F(nmol), T(nmol);
+    if (need) {
+      bd.fevals++;
+      if (!compute_forces(F, T)) { bd.status = 4; return false; }
+    }
+    int status = 0;
+    if (bd.mode == 0) {
+      P3 dR, dO1, dO2;
+      if (need) {
+        dR = ((bd.dtr[1] * dt) * bd.fact_tr) * F[1];
+        dO1 = (((bd.drot[0] * dt) * bd.ikbt) * bd.coul_k) * T[0];
+        dO2 = (((bd.drot[1] * dt) * bd.ikbt) * bd.coul_k) * T[1];
+      }
+      const double bdist = c2c(0, 1);
+      const int ct = translate_try(1, dR, sqrt(2 * dt * bd.dtr[1]));
+      if (ct == bd.max_tries) status = 2;
+      else if (c2c(0, 1) > bd.escape_dist) status = 1;
+      if (status == 0) {
+        const double s1 = sqrt(2 * dt * bd.drot[0]), s2 = sqrt(2 * dt * bd.drot[1]);
+        const P3 o1 = dO1 + rand_vec(s1), o2 = dO2 + rand_vec(s2);
+        const Quat Q1 = axis_angle(o1, o1.norm()), Q2 = axis_angle(o2, o2.norm());
+        const double adist = c2c(0, 1);
+        if (adist > bd.force_dist) {
+          bd.rot[0] = qmul(Q1, bd.rot[0]);
+          bd.rot[1] = qmul(Q2, bd.rot[1]);
+        } else if (bdist > bd.force_dist) {
+          rotate(0, bd.rot[0]);
+          rotate(1, bd.rot[1]);
+          bd.rot[0] = Quat(); bd.rot[1] = Quat();
+        } else {
+          for (int i = 0; i < 2 && status == 0; i++) {
+            Quat last;
+            if (rotate_try(i, i ? dO2 : dO1, i ? s2 : s1, last) == bd.max_tries) {
+              bd.rot[i] = qmul(last, bd.rot[i]);
+              status = 2;
+            }
+          }
+        }
+      }
+    } else {
+      for (int i = 0; i < nmol; i++) {
+        P3 dR, dO;
+        if (need) {
+          dR = ((bd.dtr[i] * dt) * bd.fact_tr) * F[i];
+          dO = (((bd.drot[i] * dt) * bd.ikbt) * bd.coul_k) * T[i];
+        }
+        translate_try(i, dR, sqrt(2 * dt * bd.dtr[i]));
+        Quat last;
+        rotate_try(i, dO, sqrt(2 * dt * bd.drot[i]), last);
+      }
+    }
+    bd.status = status;
+    bd.steps++;
+    bd.time += dt;
+    return true;
+  }
 };
 
 }  // namespace orc
@@ -1774,6 +1981,10 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
   std::vector<std::vector<std::string> > types;
   struct PoseL { int type; double v[7]; };
   std::vector<std::vector<PoseL> > frames;
+  int bdmode = -1, bdsteps = 0, bdsys = 0;
+  unsigned long long bdseed = 0;
+  double bdp[7] = {500, 100, 500, 2, 1e300, 5, 15};   // max_tries, force, escape, dt_min, dt_max, dt_ref, dt_div
+  std::vector<double> bddtr, bddrot;
   std::string tok;
   while (in >> tok) {
     if (tok == "salt") in >> prm.salt;
@@ -1785,6 +1996,9 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
     else if (tok == "moltype") { std::vector<std::string> t(4); in >> t[0] >> t[1] >> t[2] >> t[3]; types.push_back(t); }
     else if (tok == "frame") frames.push_back(std::vector<PoseL>());
     else if (tok == "mol") { PoseL p; in >> p.type; for (int k = 0; k < 7; k++) in >> p.v[k]; frames.back().push_back(p); }
+    else if (tok == "bd") in >> bdmode >> bdsteps >> bdseed >> bdsys;
+    else if (tok == "bdp") in >> bdp[0] >> bdp[1] >> bdp[2] >> bdp[3] >> bdp[4] >> bdp[5] >> bdp[6];
+    else if (tok == "bddiff") { double a, b; in >> a >> b; bddtr.push_back(a); bddrot.push_back(b); }
     else return 2;
   }
   System sys;
@@ -1800,6 +2014,31 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
   if (!out) return 2;
   fprintf(out, "KAPPA %.17e\n", kappa);
   for (auto &p : frames[0]) sys.add_molecule(p.type);
+  if (bdmode >= 0) {
+    // Brownian dynamics from the first frame's poses: one BDSTEP block per step
+    for (size_t i = 0; i < frames[0].size(); i++) {
+      const double *v = frames[0][i].v;
+      sys.set_pose(i, P3(v[0], v[1], v[2]), Quat(v[3], P3(v[4], v[5], v[6])));
+    }
+    System::BD &B = sys.bd;
+    B.mode = bdmode; B.seed = bdseed; B.sys = bdsys;
+    B.max_tries = (int)bdp[0]; B.force_dist = bdp[1]; B.escape_dist = bdp[2];
+    B.dt_min = bdp[3]; B.dt_max = bdp[4]; B.dt_ref = bdp[5]; B.dt_div = bdp[6];
+    B.dtr = bddtr; B.drot = bddrot;
+    B.rot.assign(sys.mols.size(), Quat());
+    if (bddtr.size() != sys.mols.size()) { fclose(out); return 2; }
+    for (int k = 0; k < bdsteps; k++) {
+      sys.bd_step();
+      fprintf(out, "BDSTEP %d %d %d %.17e\n", B.steps, B.status, B.fevals, B.time);
+      for (size_t i = 0; i < sys.mols.size(); i++) {
+        const Molecule &M = sys.mols[i];
+        fprintf(out, "POSE %d %.17e %.17e %.17e %.17e %.17e %.17e %.17e\n", (int)i, M.rcen.x, M.rcen.y, M.rcen.z,
+                M.orient.w, M.orient.v.x, M.orient.v.y, M.orient.v.z);
+      }
+    }
+    fclose(out);
+    return 0;
+  }
   for (size_t f = 0; f < frames.size(); f++) {
     for (size_t i = 0; i < frames[f].size(); i++) {
       const double *v = frames[f][i].v;
@@ -1831,4 +2070,11 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
   }
   fclose(out);
   return 0;
+}
+
+// one Philox4x64-10 block in place (pins the noise generator against an
+// independent implementation in the tests)
+extern "C" void pbsam_oracle_philox(unsigned long long *c, unsigned long long k0, unsigned long long k1)
+{
+  orc::System::philox(c, k0, k1);
 }

@@ -15,6 +15,7 @@
 #include "pbsam_b200.h"
 #include "pbsam_kernels.cu"
 #include "pbsam_setup.cu"
+#include "pbsam_bd.cu"
 
 using namespace pbsam;
 
@@ -161,7 +162,9 @@ struct pbsam_system {
   cudaStream_t gs[5] = {};
   bool stats_pending = false;
   std::vector<int> gsize, gcount;    // per launch: crew size, systems (lists concatenated in d_list)
+  struct BDHost *bd = nullptr;       // Brownian-dynamics state (pbsam_system_bd_init)
 };
+static void bd_free(pbsam_system *s);
 
 // Crew sizes from the last evaluation's inner-iteration counts: every system starts
 // with one CTA, the one with the largest cost per CTA doubles (up to 16) while the
@@ -675,6 +678,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   double *pos, *quat;
   chk(dalloc(Bf, &pos, B * n_mol * 3)); chk(dalloc(Bf, &quat, B * n_mol * 4));
   bv.pos = pos; bv.quat = quat;
+  bv.fmask = nullptr;
   chk(dalloc(Bf, &bv.F, B * S * NP2)); chk(dalloc(Bf, &bv.H, B * S * NP2)); chk(dalloc(Bf, &bv.Hrot, B * S * NP2));
   chk(dalloc(Bf, &bv.HselfRot, B * S * NP2)); chk(dalloc(Bf, &bv.LS, B * S * NP2));
   chk(dalloc(Bf, &bv.LFS, B * S * NP2)); chk(dalloc(Bf, &bv.LHS, B * S * NP2));
@@ -766,6 +770,7 @@ extern "C" int pbsam_system_destroy(pbsam_system *s)
     if (s->h_stats) cudaFreeHost(s->h_stats);
     if (s->h_list) cudaFreeHost(s->h_list);
   }
+  bd_free(s);
   s->ctx->live_systems--;
   delete s;
   return PBSAM_OK;
@@ -1025,6 +1030,9 @@ extern "C" int pbsam_system_phase_ms(const pbsam_system *s, double *ms)
   for (int i = 0; i < s->B * PH_N; i++) ms[i] *= 1e-6;
   return PBSAM_OK;
 }
+
+// Brownian dynamics on the force path (uses the helpers above)
+#include "pbsam_bd_host.cu"
 
 // fixed-buffer variant of the IMat builder (uses the helpers above)
 #include "pbsam_static_imat.cu"

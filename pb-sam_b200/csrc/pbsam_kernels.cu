@@ -1928,6 +1928,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c, const i
   const int k = blockIdx.x / cw.size;
   const int b = list ? list[k] : k;
   if (b >= c.bv.B) return;                 // whole crews only: the grid is (systems in the list) * size
+  if (c.bv.fmask && c.bv.fmask[b] == 0) return;   // the whole crew skips a masked system
   if (cw.rank != 0) {
     crew_serve(tm, helper_sys(c, cw, b, dsm, red));
     return;

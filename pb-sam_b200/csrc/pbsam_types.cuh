@@ -86,6 +86,8 @@ struct BatchView {
   int crew;                  // CTAs per system
   double *force, *torque, *energy;  // [B][nmol][3], [B][nmol][3], [B]
   int *status;               // [B]
+  const int *fmask;          // [B] or null: systems with fmask[b] == 0 are skipped by the
+                             // force kernel (Brownian dynamics steps without forces)
   int *stats;                // [B][8]: sweeps, inner iterations, solves, grad solves, ...
   double *tphase;            // [B][8] device time per phase (ns): solve, surface charges,
                              // numeric near field, analytic intra, inter LS, gradient DTA,

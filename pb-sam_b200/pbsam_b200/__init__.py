@@ -38,6 +38,19 @@ class pbsam_params(ctypes.Structure):
                 ("num_points_x", ctypes.c_int), ("cluster_size", ctypes.c_int)]
 
 
+PBSAM_BD_NAM = 0
+PBSAM_BD_MULTI = 1
+BD_STATUS = {0: "RUNNING", 1: "ESCAPED", 2: "STUCK", 3: "DOCKED", 4: "FAILED"}
+
+
+class pbsam_bd_params(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("max_tries", ctypes.c_int), ("force_dist", ctypes.c_double),
+                ("escape_dist", ctypes.c_double), ("dt_min", ctypes.c_double), ("dt_max", ctypes.c_double),
+                ("dt_ref", ctypes.c_double), ("dt_div", ctypes.c_double), ("fact_tr", ctypes.c_double),
+                ("ikbt", ctypes.c_double), ("coul_k", ctypes.c_double), ("seed", ctypes.c_ulonglong),
+                ("use_graph", ctypes.c_int)]
+
+
 # every entry point declared in include/pbsam_b200.h, with ctypes signatures
 _P = ctypes.c_void_p
 _DP = ctypes.POINTER(ctypes.c_double)
@@ -63,6 +76,10 @@ SIGNATURES = {
     "pbsam_imat_build": (ctypes.c_int, [_P, ctypes.c_int, _DP, _DP, ctypes.c_int, _DP]),
     "pbsam_imat_build_static": (ctypes.c_int, [_P, ctypes.c_int, _DP, _DP, ctypes.c_int, _DP]),
     "pbsam_selfpol": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _IP]),
+    "pbsam_bd_params_default": (None, [ctypes.c_int, ctypes.POINTER(pbsam_bd_params)]),
+    "pbsam_system_bd_init": (ctypes.c_int, [_P, ctypes.POINTER(pbsam_bd_params), _DP, _DP]),
+    "pbsam_system_bd_run": (ctypes.c_int, [_P, ctypes.c_int]),
+    "pbsam_system_bd_state": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, ctypes.c_int]),
     "pbsam_last_error": (ctypes.c_char_p, []),
 }
 
@@ -96,6 +113,15 @@ def _check(rc):
 def default_params(**kw):
     p = pbsam_params()
     lib().pbsam_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def bd_params(mode=PBSAM_BD_NAM, **kw):
+    """pbsam_bd_params with the reference driver's values, fields overridden by kw."""
+    p = pbsam_bd_params()
+    lib().pbsam_bd_params_default(mode, ctypes.byref(p))
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -232,6 +258,36 @@ class Molecules:
         m = ctypes.c_double()
         _check(lib().pbsam_system_last_kernel_ms(self.handle, ctypes.byref(m)))
         return m.value
+
+    # ---- Brownian dynamics (CBDnam::run / CBDmulti::propagate)
+    def bd_init(self, dtr, drot, mode=PBSAM_BD_NAM, seed=0, use_graph=True, **kw):
+        """Start one trajectory per system from the current poses.  dtr/drot: per-molecule
+        translational (A^2/ps) and rotational (rad^2/ps) diffusion coefficients; kw
+        overrides fields of pbsam_bd_params (max_tries, force_dist, escape_dist, dt_min,
+        dt_max, dt_ref, dt_div, ...)."""
+        p = bd_params(mode, seed=seed, use_graph=int(bool(use_graph)), **kw)
+        dtr = np.ascontiguousarray(dtr, dtype=np.float64)
+        drot = np.ascontiguousarray(drot, dtype=np.float64)
+        if dtr.shape != (self.n_mol,) or drot.shape != (self.n_mol,):
+            raise ValueError("one diffusion coefficient per molecule")
+        _check(lib().pbsam_system_bd_init(self.handle, ctypes.byref(p), _dptr(dtr), _dptr(drot)))
+        self.bd_params = p
+
+    def bd_run(self, n_steps):
+        """Queue n_steps steps of every running trajectory (asynchronous)."""
+        _check(lib().pbsam_system_bd_run(self.handle, int(n_steps)))
+
+    def bd_state(self):
+        """dict(pos[n_sys, n_mol, 3], quat[n_sys, n_mol, 4], status, steps, time, fevals)."""
+        pos = np.zeros((self.n_systems, self.n_mol, 3))
+        quat = np.zeros((self.n_systems, self.n_mol, 4))
+        st = np.zeros(self.n_systems, dtype=np.int32)
+        steps = np.zeros(self.n_systems, dtype=np.int32)
+        tm = np.zeros(self.n_systems)
+        fe = np.zeros(self.n_systems, dtype=np.int32)
+        _check(lib().pbsam_system_bd_state(self.handle, pos.ctypes.data, quat.ctypes.data, st.ctypes.data,
+                                           steps.ctypes.data, tm.ctypes.data, fe.ctypes.data, 0))
+        return dict(pos=pos, quat=quat, status=st, steps=steps, time=tm, fevals=fe)
 
     def close(self):
         if self.handle:

@@ -44,6 +44,18 @@ def max_over_ranks(value, dist=None):
     return float(t.item())
 
 
+def sum_over_ranks(value, dist=None):
+    """Sum of a count over all ranks (units processed by the whole job); identity without a process group."""
+    if dist is None or not dist.is_available() or not dist.is_initialized():
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64)
+    if dist.get_backend() == "nccl":
+        t = t.cuda()
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def gather_rows(local, dist=None):
     """Concatenate per-rank row blocks on every rank (results, not a data-path exchange)."""
     local = np.ascontiguousarray(local, dtype=np.float64)

@@ -25,6 +25,42 @@ SWEEP_P30 = dict(n_sph=60, r=(3.0, 8.0), n_q=2000, q_amp=0.8, nets=(4.0, -4.0), 
                  pose_seed=2103)
 SWEEP_P10 = dict(n_sph=8, r=(3.0, 6.0), n_q=300, q_amp=0.6, nets=(2.0, -2.0), poles=10, salt=0.05,
                  idiel=4.0, dists=[20.0 + 2 * k for k in range(11)], min_gap=1.0, seeds=(1, 2), pose_seed=7)
+# Brownian dynamics of two-molecule encounters at p = 10 (bdnam): one pair of
+# 35-sphere molecules (the mean of 10-60), charges as in the p = 10 case scaled to
+# the sphere count, trajectories started at a 50 A centre distance with random
+# orientations, escape at 150 A, time step 0.02 ps at contact rising linearly to 2 ps
+# at a 30 A gap, Stokes-Einstein diffusion constants at 298.15 K (water, 0.89 mPa s)
+# for a sphere of the molecule's extent.
+BD_P10 = dict(n_sph=35, r=(3.0, 6.0), n_q=1200, q_amp=0.6, nets=(2.0, -2.0), poles=10, salt=0.05, idiel=4.0,
+              seeds=(3101, 3102), pose_seed=3103, start=50.0, escape=150.0, dt_min=0.02, dt_max=2.0,
+              dt_gap=30.0, viscosity=0.89e-3, temperature=298.15, min_gap=1.0)
+
+
+def stokes_einstein(radius_A, viscosity=0.89e-3, temperature=298.15):
+    """(translational A^2/ps, rotational rad^2/ps) diffusion constants of a sphere."""
+    kT = 1.3806503e-23 * temperature
+    a = radius_A * 1e-10
+    dt = kT / (6 * np.pi * viscosity * a) * 1e20 / 1e12
+    dr = kT / (8 * np.pi * viscosity * a ** 3) / 1e12
+    return dt, dr
+
+
+def bd_start(cfg, mols, n_traj, rank=0):
+    """Start poses of n_traj two-molecule trajectories: molecule A at the origin,
+    molecule B at the start centre distance along a random axis (raised to the
+    minimum gap where spheres would overlap), random orientations."""
+    rng = np.random.default_rng(cfg["pose_seed"] + 7919 * rank)
+    a = (mols[0].centres, mols[0].radii)
+    b = (mols[1].centres, mols[1].radii)
+    pos, quat = [], []
+    for _ in range(n_traj):
+        qa, qb, ax = synth.random_quat(rng), synth.random_quat(rng), synth.random_axis(rng)
+        d = cfg["start"]
+        if synth.min_gap(a, np.zeros(3), qa, b, d * ax, qb) < cfg["min_gap"]:
+            d = synth.place_at_gap(a, qa, b, qb, ax, cfg["min_gap"])
+        pos.append([[0.0, 0.0, 0.0], list(d * ax)])
+        quat.append([list(qa), list(qb)])
+    return np.array(pos), np.array(quat)
 
 
 def molecules(cfg):

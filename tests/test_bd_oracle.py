@@ -1,0 +1,86 @@
+"""The oracle's Brownian-dynamics restatement (CBDnam / CBDmulti steps) on CPU.
+
+* its Philox4x64-10 blocks equal numpy's independent implementation
+  (numpy.random.Philox advances its counter before each block);
+* free diffusion beyond the force distance: per-step displacements are
+  N(0, 2 D dt) per component with the reference's time step 2 + (d - 5)/15 ps,
+  and no force evaluation is made (src/BDnam.cpp:196-222, 409-417);
+* escape beyond q_DIST ends the trajectory (src/BDnam.cpp:288);
+* a trajectory whose every move is rejected is STUCK (src/BDnam.cpp:287).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden_dir
+
+
+def test_philox_matches_numpy():
+    for ctr, key in (([1, 0, 0, 0], [0, 0]), ([5, 7, 9, 11], [123, 456]), ([2**64 - 1, 3, 0, 1], [2**63, 17])):
+        g = np.random.Philox(counter=np.array([(ctr[0] - 1) % 2**64] + ctr[1:], dtype=np.uint64),
+                             key=np.array(key, dtype=np.uint64))
+        if ctr[0] == 0:
+            continue
+        assert [int(x) for x in g.random_raw(4)] == oracle.philox(ctr, key)
+
+
+def _frame(p1, q1=(1, 0, 0, 0)):
+    return [(0, [0.0, 0.0, 0.0], [1.0, 0.0, 0.0, 0.0]), (1, list(p1), list(q1))]
+
+
+def _run(tmp_path, frame, n, mode=0, seed=7, system=0, dtr=(0.0, 0.03), drot=(4.5e-5, 4e-5), **kw):
+    case = golden_dir("tiny")
+    spec, out = os.path.join(tmp_path, "bd.txt"), os.path.join(tmp_path, "bd.out")
+    oracle.write_bd_spec(spec, oracle.golden_moltypes(case), frame, mode, n, seed, system, dtr, drot,
+                         salt=0.1, idiel=4.0, poles=6, **kw)
+    return oracle.run_bd_spec(spec, out)
+
+
+def test_free_diffusion_statistics(tmp_path):
+    n = 3000
+    steps = _run(str(tmp_path), _frame((300.0, 0.0, 0.0)), n, escape_dist=1e9)
+    pos = np.array([s["pos"][1] for s in steps])
+    assert all(s["fevals"] == 0 and s["status"] == 0 for s in steps)
+    prev = np.vstack([[300.0, 0.0, 0.0], pos[:-1]])
+    d = pos - prev
+    t = np.array([s["time"] for s in steps])
+    dt = np.diff(np.concatenate([[0.0], t]))
+    assert np.all(dt > 2.0)
+    z = d / np.sqrt(2 * 0.03 * dt)[:, None]
+    assert abs(z.mean()) < 4 / np.sqrt(z.size)
+    assert abs(z.var() - 1.0) < 0.06
+    # the time step follows the gap before the move: 2 + (gap - 5)/15
+    gap0 = 300.0 - (dt[0] - 2.0) * 15 - 5
+    c2c = np.linalg.norm(prev, axis=1)
+    np.testing.assert_allclose(dt, 2.0 + (c2c - gap0 - 5) / 15, rtol=1e-12)
+
+
+def test_escape(tmp_path):
+    steps = _run(str(tmp_path), _frame((140.0, 0.0, 0.0)), 400, escape_dist=150.0, dtr=(0.0, 0.5))
+    st = [s["status"] for s in steps]
+    assert 1 in st, "no escape"
+    k = st.index(1)
+    assert all(x == 1 for x in st[k:])
+    assert np.linalg.norm(steps[k]["pos"][1]) > 150.0
+    assert steps[-1]["steps"] == k + 1      # nothing moves after the escape
+
+
+def test_stuck_when_every_move_collides(tmp_path):
+    # molecule 1 placed on top of molecule 0: with one draw per move and a tiny
+    # diffusion constant every candidate position still overlaps
+    steps = _run(str(tmp_path), _frame((0.3, 0.0, 0.0)), 3, max_tries=1, dtr=(0.0, 1e-8), force_dist=0.0)
+    assert steps[0]["status"] == 2 and steps[-1]["steps"] == 1
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_same_seed_same_trajectory_other_system_differs(tmp_path, mode):
+    fr = _frame((60.0, 10.0, -5.0))
+    a = _run(str(tmp_path), fr, 5, mode=mode, system=0, force_dist=0.0, dtr=(0.03, 0.03))
+    b = _run(str(tmp_path), fr, 5, mode=mode, system=0, force_dist=0.0, dtr=(0.03, 0.03))
+    c = _run(str(tmp_path), fr, 5, mode=mode, system=1, force_dist=0.0, dtr=(0.03, 0.03))
+    assert np.array_equal(a[-1]["pos"], b[-1]["pos"]) and np.array_equal(a[-1]["quat"], b[-1]["quat"])
+    assert not np.allclose(a[-1]["pos"], c[-1]["pos"])
+    if mode == 0:
+        assert np.array_equal(a[-1]["pos"][0], [0, 0, 0])   # NAM: molecule 0 never translates

@@ -1,0 +1,109 @@
+"""Brownian dynamics through the C ABI (pbsam_system_bd_*) against the oracle.
+
+The GPU steps (time step and force mask, the force kernel, the move kernel with
+its rejection loops) and the oracle's restatement of CBDnam::run / makeMove and
+CBDmulti::propagate / makeMove draw the same Philox noise, so each trajectory
+is compared step by step: positions within 1e-9 A + 1e-9 relative, quaternion
+components within 1e-9, statuses, step and force-evaluation counts exactly.
+The forces inside a step agree to the 1e-8 relative bar of the force tests.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden_dir
+
+pytestmark = pytest.mark.gpu
+DTR = (0.0, 0.03)          # the reference's m_Dtr (src/BDnam.cpp:145), molecule 0 never translates
+DROT = (4.5e-5, 4e-5)      # m_Dr1, m_Dr2
+
+
+def tiny_ctx(cluster_size=0):
+    import pbsam_b200 as pb
+    P = json.load(open(os.path.join(golden_dir("tiny"), "poses.json")))
+    ctx = pb.CSystem(poles=P["poles"], salt=P["salt"], idiel=P["idiel"], cluster_size=cluster_size)
+    d = golden_dir("tiny")
+    ta = ctx.load_moltype(d + "/molA.pqr", d + "/imA", d + "/expA", "molA.0")
+    tb = ctx.load_moltype(d + "/molB.pqr", d + "/imB", d + "/expB", "molB.0")
+    return ctx, [ta, tb], P
+
+
+def oracle_traj(tmp_path, frame, mode, n, seed, system, dtr, drot, P, **kw):
+    spec, out = os.path.join(tmp_path, "bd%d.txt" % system), os.path.join(tmp_path, "bd%d.out" % system)
+    oracle.write_bd_spec(spec, oracle.golden_moltypes(golden_dir("tiny")), frame, mode, n, seed, system, dtr, drot,
+                         salt=P["salt"], idiel=P["idiel"], poles=P["poles"], **kw)
+    return oracle.run_bd_spec(spec, out)
+
+
+def check_step(g, b, o):
+    assert g["status"][b] == o["status"]
+    assert g["steps"][b] == o["steps"]
+    assert g["fevals"][b] == o["fevals"]
+    assert abs(g["time"][b] - o["time"]) <= 1e-12 * abs(o["time"])
+    np.testing.assert_allclose(g["pos"][b], o["pos"], rtol=1e-9, atol=1e-9)
+    np.testing.assert_allclose(g["quat"][b], o["quat"], rtol=0, atol=1e-9)
+
+
+def run_compare(tmp_path, mol_types, frame, mode, n, seed, dtr, drot, n_sys=2, use_graph=True, **kw):
+    ctx, types, P = tiny_ctx()
+    mol = ctx.molecules([types[t] for t in mol_types], n_systems=n_sys)
+    pos = np.array([[m[1] for m in frame]] * n_sys)
+    quat = np.array([[m[2] for m in frame]] * n_sys)
+    mol.set_poses(pos, quat)
+    mol.bd_init(dtr, drot, mode=mode, seed=seed, use_graph=use_graph, **kw)
+    ref = [oracle_traj(str(tmp_path), frame, mode, n, seed, b, dtr, drot, P, **kw) for b in range(n_sys)]
+    states = []
+    for k in range(n):
+        mol.bd_run(1)
+        g = mol.bd_state()
+        states.append(g)
+        for b in range(n_sys):
+            check_step(g, b, ref[b][k])
+    mol.close()
+    ctx.close()
+    return states, ref
+
+
+def gap5_frame():
+    P = json.load(open(os.path.join(golden_dir("tiny"), "poses.json")))
+    fr = P["poses"][1]["frame"]
+    return [(m["type"], m["pos"], m["quat"]) for m in fr]
+
+
+def test_nam_close_range_vs_oracle(tmp_path):
+    states, ref = run_compare(tmp_path, [0, 1], gap5_frame(), 0, 8, 11, DTR, DROT)
+    assert ref[0][-1]["fevals"] == 8          # every step evaluated forces (inside f_DIST)
+    assert not np.allclose(states[-1]["pos"][0], states[-1]["pos"][1])
+
+
+def test_nam_graph_and_stream_launches_agree(tmp_path):
+    a, _ = run_compare(tmp_path, [0, 1], gap5_frame(), 0, 4, 5, DTR, DROT, use_graph=True)
+    b, _ = run_compare(tmp_path, [0, 1], gap5_frame(), 0, 4, 5, DTR, DROT, use_graph=False)
+    assert np.array_equal(a[-1]["pos"], b[-1]["pos"]) and np.array_equal(a[-1]["quat"], b[-1]["quat"])
+
+
+def test_nam_crossing_force_distance_vs_oracle(tmp_path):
+    # start just outside a small force distance: rotations are stored while far
+    # and applied on the step that brings the pair back inside
+    fr = gap5_frame()
+    far = np.array(fr[1][1]) * 1.6
+    frame = [fr[0], (fr[1][0], list(far), fr[1][2])]
+    run_compare(tmp_path, [0, 1], frame, 0, 12, 3, (0.0, 2.0), (4.5e-3, 4e-3), force_dist=float(np.linalg.norm(far)) - 0.5)
+
+
+def test_multi_three_molecules_vs_oracle(tmp_path):
+    fr = gap5_frame()
+    third = (0, list(-np.array(fr[1][1])), [0.5, 0.5, -0.5, 0.5])
+    run_compare(tmp_path, [0, 1, 0], fr + [third], 1, 6, 9, (0.03, 0.03, 0.03), (4.5e-5, 4e-5, 4.5e-5))
+
+
+def test_escape_and_stuck_vs_oracle(tmp_path):
+    fr = gap5_frame()
+    esc = [fr[0], (fr[1][0], [140.0, 0.0, 0.0], fr[1][2])]
+    s, ref = run_compare(tmp_path, [0, 1], esc, 0, 60, 2, (0.0, 0.5), DROT, escape_dist=150.0)
+    stuck = [fr[0], (fr[1][0], [0.3, 0.0, 0.0], fr[1][2])]
+    s2, ref2 = run_compare(tmp_path, [0, 1], stuck, 0, 2, 2, (0.0, 1e-8), DROT, max_tries=1, force_dist=0.0)
+    assert ref2[0][0]["status"] == 2 and s2[-1]["status"][0] == 2

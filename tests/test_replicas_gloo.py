@@ -36,18 +36,19 @@ def _worker(rank, world, port, out):
     rows = np.arange(lo, hi, dtype=np.float64)[:, None] * np.ones((1, 3))
     allrows = replicas.gather_rows(rows, dist)
     t = replicas.max_over_ranks(1.0 + r, dist)
+    u = replicas.sum_over_ranks(10.0 + r, dist)
     dist.barrier()
     if r == 0:
-        np.save(out, np.concatenate([allrows.ravel(), [t]]))
+        np.save(out, np.concatenate([allrows.ravel(), [u, t]]))
     dist.destroy_process_group()
 
 
-def test_two_rank_gather_and_max(tmp_path):
+def test_two_rank_gather_max_and_sum(tmp_path):
     import torch.multiprocessing as mp
     out = str(tmp_path / "res.npy")
     port = _free_port()
     mp.start_processes(_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
     res = np.load(out)
-    rows, t = res[:-1].reshape(-1, 3), res[-1]
+    rows, u, t = res[:-2].reshape(-1, 3), res[-2], res[-1]
     assert np.array_equal(rows[:, 0], np.arange(7))
-    assert t == 2.0
+    assert t == 2.0 and u == 21.0
