@@ -110,6 +110,13 @@ int pbsam_system_compute_forces(pbsam_system *sys, double *force, double *torque
 /* Replaces CMolecule::computeTotalIntEnergy (src/molecule.h:180,
  * src/moldynamics.cpp:358-386) on the state left by the last force evaluation. */
 int pbsam_system_compute_energy(pbsam_system *sys, double *energy, int on_device);
+/* The same interaction energy with the orientation taken into account: sphere
+ * centres at pos + q*cen and every H rotated to the lab frame by its molecule's
+ * orientation before the pair re-expansions, so the value is invariant under a
+ * rigid motion of the whole system.  Replaces interactCenters_LowMemory
+ * (src/molecule.cpp:1850-1890), which uses the unrotated centres and molecule-frame
+ * H, in the corrected form; the reference has no such call. */
+int pbsam_system_compute_energy_lab(pbsam_system *sys, double *energy, int on_device);
 
 /* Counters of the last force evaluation, 8 ints per system: [0] sweeps,
  * [1] inner F/H iterations, [2] inner solves, [3] gradient solves,

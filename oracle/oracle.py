@@ -130,6 +130,8 @@ def parse(path):
                 cur["torque"][int(t[1])] = [float(x) for x in t[2:5]]
             elif t[0] == "ENERGY":
                 cur["energy"] = float(t[1])
+            elif t[0] == "ENERGYLAB":
+                cur["energy_lab"] = float(t[1])
             elif t[0] == "KAPPA":
                 pass
             elif cur is not None:

@@ -1758,6 +1758,45 @@ struct System {
     return pot;
   }
 
+  // the same sum in the lab frame: centres rcen + q*cen and H rotated to the lab
+  // frame by the molecule's orientation (the corrected form of
+  // interactCenters_LowMemory, src/molecule.cpp:1850-1890)
+  double total_energy_lab()
+  {
+    const int nmol = mols.size();
+    std::vector<std::vector<vec> > Hl(nmol);
+    for (int i = 0; i < nmol; i++) {
+      Rot R;
+      R.reset_quat(T, mols[i].orient, NP);
+      Hl[i].resize(mols[i].s.size());
+      for (size_t k = 0; k < mols[i].s.size(); k++) R.rotate_xi(mols[i].s[k].H, Hl[i][k], NP, true);
+    }
+    double pot = 0.0;
+    for (int i = 0; i < nmol; i++)
+      for (int j = i + 1; j < nmol; j++) {
+        double e = 0.0;
+        for (size_t ki = 0; ki < mols[i].s.size(); ki++) {
+          const SphType &Si = st(i, ki);
+          const SphState &Zi = mols[i].s[ki];
+          vec Lki(1, 0.0);
+          for (size_t kj = 0; kj < mols[j].s.size(); kj++) {
+            const SphType &Sj = st(j, kj);
+            const SphState &Zj = mols[j].s[kj];
+            P3 P = (mols[i].rcen + qrot(mols[i].orient, Si.cen)) - (mols[j].rcen + qrot(mols[j].orient, Sj.cen));
+            double rho = P.norm();
+            int pi2j = compute_order(NP, rho, Zi.tH, Si.rad), pj2i = compute_order(NP, rho, Zj.tH, Sj.rad);
+            int minp = pi2j < pj2i ? pi2j : pj2i;
+            XForm X; X.reset(T, P, minp, Sj.rad, Si.rad, false);
+            vec tL; X.xformH(Hl[j][kj], tL);
+            add_into(Lki, tL);
+          }
+          e += inprod_ml(Hl[i][ki], Zi.hscale, Lki, Si.rad);
+        }
+        pot += e;
+      }
+    return pot;
+  }
+
   // ---------------------------------------------------------------- Brownian dynamics
   // The Ermak-McCammon step of the reference's drivers: CBDnam::run / makeMove /
   // compute_dt (src/BDnam.cpp:166-417) and CBDmulti::propagate / makeMove /
@@ -2053,6 +2092,7 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
       fprintf(out, "TORQUE %d %.17e %.17e %.17e\n", (int)i, torque[i].x, torque[i].y, torque[i].z);
     }
     if (energy) fprintf(out, "ENERGY %.17e\n", sys.total_energy());
+    if (energy > 1) fprintf(out, "ENERGYLAB %.17e\n", sys.total_energy_lab());
     if (dump)
       for (size_t i = 0; i < sys.mols.size(); i++)
         for (size_t ki = 0; ki < sys.mols[i].s.size(); ki++) {

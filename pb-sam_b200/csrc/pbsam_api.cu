@@ -688,6 +688,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   chk(dalloc(Bf, &bv.gFp, B * SP * 3)); chk(dalloc(Bf, &bv.gHp, B * SP * 3));
   chk(dalloc(Bf, &bv.gLHN, B * S * 3 * NP2)); chk(dalloc(Bf, &bv.gH, B * S * 3 * NP2));
   chk(dalloc(Bf, &bv.cenRot, B * S * 3));
+  chk(dalloc(Bf, &bv.Hlab, B * S * NP2));
   chk(dalloc(Bf, &bv.ipol, B * S * S)); chk(dalloc(Bf, &bv.ipol_n, B * S));
   chk(dalloc(Bf, &bv.iact, B * S * S)); chk(dalloc(Bf, &bv.iact_n, B * S));
   chk(dalloc(Bf, &bv.interMol, B * n_mol * S)); chk(dalloc(Bf, &bv.interMol_n, B * n_mol));
@@ -860,15 +861,25 @@ extern "C" int pbsam_system_compute_forces(pbsam_system *s, double *force, doubl
   return PBSAM_OK;
 }
 
-extern "C" int pbsam_system_compute_energy(pbsam_system *s, double *energy, int on_device)
+static int energy_launch(pbsam_system *s, double *energy, int on_device, int lab)
 {
   if (!s || !energy) return fail(PBSAM_E_BADARG, "null argument");
   CK(cudaSetDevice(s->ctx->device));
-  pbsam_energy_kernel<<<s->B, PBSAM_TEAM, team_smem_bytes(s->ctx->prm.poles), s->stream>>>(s->c);
+  pbsam_energy_kernel<<<s->B, PBSAM_TEAM, team_smem_bytes(s->ctx->prm.poles), s->stream>>>(s->c, lab);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(energy, s->c.bv.energy, s->B * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s->stream));
   if (!on_device) CK(cudaStreamSynchronize(s->stream));
   return PBSAM_OK;
+}
+
+extern "C" int pbsam_system_compute_energy(pbsam_system *s, double *energy, int on_device)
+{
+  return energy_launch(s, energy, on_device, 0);
+}
+
+extern "C" int pbsam_system_compute_energy_lab(pbsam_system *s, double *energy, int on_device)
+{
+  return energy_launch(s, energy, on_device, 1);
 }
 
 extern "C" int pbsam_system_stats(const pbsam_system *s, int *stats)

@@ -1937,9 +1937,15 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c, const i
   crew_finish(tm, cw);
 }
 
-// interaction energy with the reference's convention (unrotated centres and
-// molecule-frame H, src/moldynamics.cpp:358-386, src/molecule.cpp:1850-1890)
-__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c)
+// interaction energy on the state left by the last force evaluation.
+// lab == 0: the reference's convention (src/moldynamics.cpp:358-386,
+//   src/molecule.cpp:1850-1890): unrotated sphere centres and molecule-frame H, so
+//   the value ignores the molecules' orientations.
+// lab == 1: the same sum in the lab frame: sphere centres at pos + q*cen and every
+//   H rotated to the lab frame by its molecule's orientation (the rotation the
+//   solve applies to H before re-expanding it to other molecules); invariant under
+//   a rigid rotation or translation of the whole system.
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c, int lab)
 {
   extern __shared__ double2 dsm[];
   __shared__ double red[PBSAM_TEAM];
@@ -1954,8 +1960,30 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c)
   y.red = red;
   y.tph = nullptr;
   const Tab &T = c.T;
+  const int NP2 = y.NP2;
   double pot = 0.0;
   if (bv.status[b] == PBSAM_STATUS_OK) {
+    if (lab) {
+      // lab-frame centres and H of every sphere
+      for (int i = 0; i < bv.nmol; i++) {
+        const double *q = bv.quat + 4 * ((size_t)b * bv.nmol + i);
+        double qn[4];
+        const double in = 1.0 / sqrt((q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) + q[0] * q[0]);
+        qn[0] = q[0] * in; qn[1] = q[1] * in; qn[2] = q[2] * in; qn[3] = q[3] * in;
+        for (int s = bv.mol_off[i] + tm.rank; s < bv.mol_off[i + 1]; s += tm.size) qrot(qn, y.cen(s), y.cenRot(s));
+        double th, ph, xi;
+        quat_angles(qn, th, ph, xi);
+        RotState rs;
+        double2 *Rm = bv.molR + ((size_t)b * bv.nmol + i) * rot_off(2 * y.NP - 1);
+        rot_compute(tm, T, th, ph, xi, y.NP, false, rs, Rm, nullptr, y.sc.sh, y.sc.lvA, y.sc.lvB);
+        tm.sync();
+        for (int s = bv.mol_off[i]; s < bv.mol_off[i + 1]; s++) {
+          rot_apply_xi(tm, rs, y.H(s), bv.Hlab + ((size_t)b * bv.S + s) * NP2, y.NP, true, y.NP);
+          tm.sync();
+        }
+      }
+      tm.sync();
+    }
     for (int i = 0; i < bv.nmol; i++)
       for (int j = i + 1; j < bv.nmol; j++) {
         double e = 0.0;
@@ -1964,9 +1992,9 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c)
           double *Lki = y.sc.E(9), *tL = y.sc.E(10);
           tzero(tm, Lki, y.NP2);
           tm.sync();
-          const double *ci = y.cen(si);
+          const double *ci = lab ? y.cenRot(si) : y.cen(si);
           for (int sj = bv.mol_off[j]; sj < bv.mol_off[j + 1]; sj++) {
-            const double *cj = y.cen(sj);
+            const double *cj = lab ? y.cenRot(sj) : y.cen(sj);
             const double P[3] = {(pi[0] + ci[0]) - (pj[0] + cj[0]), (pi[1] + ci[1]) - (pj[1] + cj[1]),
                                  (pi[2] + ci[2]) - (pj[2] + cj[2])};
             const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
@@ -1975,10 +2003,11 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c)
             const int minp = pi2j < pj2i ? pi2j : pj2i;
             PairXf X;
             prep_pair(tm, T, y.sc, P, minp, 0, y.rad(sj), y.rad(si), false, X);
-            pair_apply(tm, T, y.sc, X, false, y.H(sj), tL);
+            pair_apply(tm, T, y.sc, X, false, lab ? bv.Hlab + ((size_t)b * bv.S + sj) * NP2 : y.H(sj), tL);
             add_vec_into(tm, Lki, tL, y.NP2);
           }
-          e += inprod_ml(y.H(si), bv.hscale[y.sc1(si)], Lki, y.rad(si), y.NP);
+          e += inprod_ml(lab ? bv.Hlab + ((size_t)b * bv.S + si) * NP2 : y.H(si), bv.hscale[y.sc1(si)], Lki,
+                         y.rad(si), y.NP);
           tm.sync();
         }
         pot += e;

@@ -71,6 +71,7 @@ struct BatchView {
   double *gFp, *gHp;         // [B][SP][3]
   double *gLHN, *gH;         // [B][S][3][NP2]
   double *cenRot;            // [B][S][3]
+  double *Hlab;              // [B][S][NP2] H rotated to the lab frame (lab-frame energy)
   int *ipol, *ipol_n, *iact, *iact_n;        // [B][S][S], [B][S]
   int *interMol, *interMol_n;                // [B][nmol][S], [B][nmol]
   int *intraPol, *intraPol_n, *intraAct, *intraAct_n;

@@ -69,6 +69,7 @@ SIGNATURES = {
     "pbsam_system_set_poses": (ctypes.c_int, [_P, _P, _P, ctypes.c_int]),
     "pbsam_system_compute_forces": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int]),
     "pbsam_system_compute_energy": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "pbsam_system_compute_energy_lab": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "pbsam_system_stats": (ctypes.c_int, [_P, _IP]),
     "pbsam_system_set_stream": (ctypes.c_int, [_P, _P]),
     "pbsam_system_last_kernel_ms": (ctypes.c_int, [_P, _DP]),
@@ -232,9 +233,13 @@ class Molecules:
     def compute_forces_device(self, force_ptr, torque_ptr, status_ptr):
         _check(lib().pbsam_system_compute_forces(self.handle, force_ptr, torque_ptr, status_ptr, 1))
 
-    def compute_energy(self):
+    def compute_energy(self, lab=False):
+        """Interaction energy per system on the last force evaluation's state: the
+        reference's convention (computeTotalIntEnergy: unrotated centres and H), or
+        with lab=True the orientation-correct lab-frame form."""
         e = np.zeros(self.n_systems)
-        _check(lib().pbsam_system_compute_energy(self.handle, e.ctypes.data, 0))
+        f = lib().pbsam_system_compute_energy_lab if lab else lib().pbsam_system_compute_energy
+        _check(f(self.handle, e.ctypes.data, 0))
         return e
 
     def stats(self):
