@@ -175,13 +175,15 @@ def test_singular_rotations_vs_oracle(ctx_default, tmp_path):
     cb = B[0] - B[0].mean(axis=0)
     ident = [1.0, 0.0, 0.0, 0.0]
     flip = [0.0, 1.0, 0.0, 0.0]       # rotation by pi about x
-    # B placed so that sphere 0 of B sits straight above sphere 0 of A at a 3 A gap
+    # B placed so that sphere 0 of B sits straight above sphere 0 of A, raised in
+    # 0.5 A steps from a 3 A gap until no two spheres are closer than 1 A
     zoff = A[1][0] + B[1][0] + 3.0
-    posb = list(ca[0] - cb[0] + np.array([0.0, 0.0, zoff]))
+    while True:
+        posb = list(ca[0] - cb[0] + np.array([0.0, 0.0, zoff]))
+        if synth.min_gap((A[0], A[1]), np.zeros(3), ident, (B[0], B[1]), np.array(posb), ident) > 1.0:
+            break
+        zoff += 0.5
     frames = [[dict(type=0, pos=[0, 0, 0], quat=ident), dict(type=1, pos=posb, quat=ident)]]
-    gmin = synth.min_gap((A[0], A[1]), np.zeros(3), ident, (B[0], B[1]), np.array(posb), ident)
-    if gmin <= 0.2:
-        pytest.skip("constructed pose overlaps")
     frames.append([dict(type=0, pos=[0, 0, 0], quat=flip),
                    dict(type=1, pos=list(40.0 * np.array([0.0, 0.0, 1.0])), quat=ident)])
     mol = ctx.molecules(types, n_systems=len(frames))
