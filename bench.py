@@ -238,14 +238,6 @@ def run_ours(args):
             out["cpu_baseline"] = cpu_baseline(cfg, specs, pos, quat, stats, args)
     sysb.close()
     ctx.close()
-    if args.mixed:
-        try:
-            mx = run_mixed(args, cfg, specs, pos, quat, f, t, local, rank, world, dist)
-        except Exception as e:   # the headline line stands without the mixed-precision leg
-            mx = {"error": "%s: %s" % (type(e).__name__, e)}
-        if out is not None:
-            out["mixed"] = mx
-            out["gpu_launches"] += mx.get("gpu_launches", 0)
     if args.bd:
         try:
             bd = run_bd(args, local, rank, world, dist)
@@ -258,61 +250,6 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return out
-
-
-# ---------------------------------------------------------------- mixed-precision leg
-def run_mixed(args, cfg, specs, pos, quat, f64, t64, local, rank, world, dist):
-    """The same pose sweep with the IMats stored in FP32 (products accumulated in
-    FP64, everything else FP64): solves/s and the force/torque error against the
-    FP64 path's results of the same call sequence (relative per system, max over
-    systems)."""
-    import torch
-    from pbsam_b200 import replicas, workload
-    ctx, types = workload.open_context(cfg, specs, device=local, cluster_size=args.cluster_size, imat_fp32=1)
-    B = len(pos)
-    sysb = ctx.molecules(types, n_systems=B)
-    stream = torch.cuda.current_stream()
-    sysb.set_stream(stream.cuda_stream)
-    dpos = torch.tensor(pos, dtype=torch.float64, device="cuda")
-    dquat = torch.tensor(quat, dtype=torch.float64, device="cuda")
-    dF = torch.zeros((B, 2, 3), dtype=torch.float64, device="cuda")
-    dT = torch.zeros_like(dF)
-    dS = torch.zeros(B, dtype=torch.int32, device="cuda")
-
-    def step():
-        sysb.set_poses_device(dpos.data_ptr(), dquat.data_ptr())
-        sysb.compute_forces_device(dF.data_ptr(), dT.data_ptr(), dS.data_ptr())
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = replicas.max_over_ranks(e0.elapsed_time(e1), dist if world > 1 else None)
-    # the FP64 results came from 2 * steps + warmup calls at the same poses; repeat that count
-    for _ in range(args.steps):
-        step()
-    torch.cuda.synchronize()
-    fm, tm_ = dF.cpu().numpy(), dT.cpu().numpy()
-    stats = sysb.stats()
-    sysb.close()
-    ctx.close()
-
-    def relerr(a, b):
-        return float(max(np.max(np.abs(a[k] - b[k])) / max(np.max(np.abs(b[k])), 1e-300) for k in range(len(b))))
-
-    units = replicas.sum_over_ranks(B * args.steps, dist if world > 1 else None)
-    return {"metric": "pol. solves/s, pose sweep p=30, IMats in FP32 (FP64 accumulation)",
-            "value": units / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps,
-            "max_rel_force_err_vs_fp64": relerr(fm, f64), "max_rel_torque_err_vs_fp64": relerr(tm_, t64),
-            "inner_iterations_per_step": int(np.sum(stats[:, 1])),
-            "gpu_launches": args.steps * len(set(int(x) for x in stats[:, 5]))}
 
 
 # ---------------------------------------------------------------- Brownian dynamics leg
@@ -603,7 +540,6 @@ def main():
     ap.add_argument("--cpu-limit", type=int, default=60, help="seconds before a sample pose is abandoned")
     ap.add_argument("--cluster-size", type=int, default=-1,
                     help="CTAs per system (0: automatic, -1: adaptive from the previous step's costs)")
-    ap.add_argument("--mixed", type=int, default=1, help="also time the sweep with FP32 IMats")
     ap.add_argument("--bd", type=int, default=1, help="also time the Brownian-dynamics workload")
     ap.add_argument("--bd-traj", type=int, default=1024, help="BD trajectories per GPU")
     ap.add_argument("--bd-steps", type=int, default=20, help="timed BD steps")

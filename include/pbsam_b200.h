@@ -55,11 +55,6 @@ typedef struct pbsam_params {
                              inner-iteration counts, costlier systems getting larger clusters (the
                              rounding of the results may then differ between calls by ~1e-15).
                              No reference counterpart (a B200 launch parameter). */
-  int imat_fp32;          /* 0 = IMats stored and applied in FP64 (the reference's arithmetic);
-                             1 = mixed precision: IMats stored in FP32 (half the bytes of every
-                             matvec), products accumulated in FP64; every other step stays FP64.
-                             No reference counterpart; its error against FP64 is measured by the
-                             tests and the bench. */
 } pbsam_params;
 
 typedef struct pbsam_context pbsam_context;

@@ -195,7 +195,6 @@ extern "C" void pbsam_params_default(pbsam_params *p)
   p->inter_cutoff = 10; p->interact_cutoff = 100; p->intra_cutoff = 30; p->min_sep_numeric = 5;
   p->num_points_x = 10000;
   p->cluster_size = 0;
-  p->imat_fp32 = 0;
 }
 
 static double kappa_of(const pbsam_params &p)
@@ -209,7 +208,6 @@ extern "C" int pbsam_context_create(const pbsam_params *prm, int device, pbsam_c
 {
   if (!prm || !out) return fail(PBSAM_E_BADARG, "null argument");
   if (prm->poles < 1 || prm->poles > 32) return fail(PBSAM_E_BADARG, "poles must be in [1, 32]");
-  if (prm->imat_fp32 != 0 && prm->imat_fp32 != 1) return fail(PBSAM_E_BADARG, "imat_fp32 must be 0 or 1");
   if (prm->cluster_size < -1 || prm->cluster_size > PBSAM_MAX_CREW)
     return fail(PBSAM_E_BADARG, "cluster_size must be -1 (adaptive), 0 (automatic) or 1..16");
   int ndev = 0;
@@ -589,15 +587,7 @@ static int finalize_types(pbsam_context *c)
   TRY(dput(B, &tv.rad, rad)); TRY(dput(B, &tv.spx_off, spx_off)); TRY(dput(B, &tv.spx, spx));
   TRY(dput(B, &tv.nspx, nspx)); TRY(dput(B, &tv.Fself, Fs)); TRY(dput(B, &tv.Hself, Hs));
   TRY(dput(B, &tv.hself_scale, hsc)); TRY(dput(B, &tv.near_off, near_off)); TRY(dput(B, &tv.near, near));
-  if (c->prm.imat_fp32) {
-    std::vector<float> im32(imat.begin(), imat.end());
-    std::vector<double>().swap(imat);
-    TRY(dput(B, &tv.imat32, im32));
-    tv.imat = nullptr;
-  } else {
-    TRY(dput(B, &tv.imat, imat));
-    tv.imat32 = nullptr;
-  }
+  TRY(dput(B, &tv.imat, imat));
   TRY(dput(B, &tv.chg_off, chg_off)); TRY(dput(B, &tv.chg_pos, chg_pos));
   TRY(dput(B, &tv.chg, chg));
   TRY(dput(B, &tv.chg_lab, chg_lab));

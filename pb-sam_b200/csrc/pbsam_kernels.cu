@@ -57,10 +57,9 @@ __host__ __device__ inline long long scr_doubles(int NP, long long S)
   return n;
 }
 
-// IMat rows and matvec operands are stored with a stride rounded up to a multiple
-// of 4 so that every row starts on a 16-byte boundary (double2 loads of FP64 rows,
-// float4 loads of FP32 rows); the pad columns are zero.
-__host__ __device__ inline int imat_ld(int NP2) { return (NP2 + 3) & ~3; }
+// IMat rows and matvec operands are stored with an even stride so that every row
+// starts on a 16-byte boundary (double2 loads); the pad column is zero.
+__host__ __device__ inline int imat_ld(int NP2) { return (NP2 + 1) & ~1; }
 // per-sphere stride of the row-major IMat store
 __host__ __device__ inline size_t imat_stride(int NP2) { return (size_t)NP2 * imat_ld(NP2); }
 
@@ -803,87 +802,11 @@ __device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int
   }
 }
 
-// The same product with the IMat stored in FP32 (mixed-precision mode): 16-byte
-// loads carry four elements instead of two, so the same bytes in flight per lane
-// cover more columns; every element is widened to FP64 and accumulated in FP64
-// against the FP64 operands, with the same fixed-order warp reduction.
-template <int D, int U>
-__device__ __noinline__ void imat_apply32_t(const Team &tm, const float *IMT, int ld, const double *x, int NP2,
-                                            int r_begin, int r_end, double *Y, const double *scale)
+__device__ __forceinline__ void imat_apply(const Team &tm, const double *IMT, int ld, const double *x, int NP2, int D,
+                                           int r_begin, int r_end, double *Y, const double *scale)
 {
-  const int lane = tm.rank & 31, warp = tm.rank >> 5, nw = tm.size >> 5;
-  const int NV = ld >> 2, NX = ld >> 1;
-  const double2 *x2 = (const double2 *)x;
-  for (int r0 = r_begin + warp * 4; r0 < r_end; r0 += nw * 4) {
-    const float4 *rp[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int r = (r0 + j < NP2) ? r0 + j : NP2 - 1;
-      rp[j] = (const float4 *)(IMT + (size_t)r * ld);
-    }
-    double acc[4][D];
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int d = 0; d < D; d++) acc[j][d] = 0.0;
-    for (int k0 = lane; k0 < NV; k0 += 32 * U) {
-      float4 a[U][4];
-#pragma unroll
-      for (int b = 0; b < U; b++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          a[b][j] = (k0 + 32 * b < NV) ? __ldg(rp[j] + k0 + 32 * b) : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-      for (int b = 0; b < U; b++) {
-        if (k0 + 32 * b >= NV) break;
-#pragma unroll
-        for (int d = 0; d < D; d++) {
-          const double2 u0 = x2[d * NX + 2 * (k0 + 32 * b)], u1 = x2[d * NX + 2 * (k0 + 32 * b) + 1];
-#pragma unroll
-          for (int j = 0; j < 4; j++)
-            acc[j][d] += ((double)a[b][j].x * u0.x + (double)a[b][j].y * u0.y) +
-                         ((double)a[b][j].z * u1.x + (double)a[b][j].w * u1.y);
-        }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int d = 0; d < D; d++) {
-        double v = acc[j][d];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        acc[j][d] = v;
-      }
-    if (lane < 4) {
-      const int i = r0 + lane;
-      if (i < r_end) {
-        int n = (int)sqrt((double)i);
-        while (n * n > i) n--;
-        while ((n + 1) * (n + 1) <= i) n++;
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (j == lane)
-#pragma unroll
-            for (int d = 0; d < D; d++) Y[d * NP2 + i] = acc[j][d] * scale[n];
-      }
-    }
-  }
-}
-
-// IMat product of one sphere: FP64 rows (IMT) or, in mixed-precision mode, FP32 rows (IMT32)
-__device__ __forceinline__ void imat_apply(const Team &tm, const double *IMT, const float *IMT32, int ld,
-                                           const double *x, int NP2, int D, int r_begin, int r_end, double *Y,
-                                           const double *scale)
-{
-  if (IMT32) {
-    // the deepest load batches that fit the 128 registers of a 512-thread team
-    if (D == 1) imat_apply32_t<1, 3>(tm, IMT32, ld, x, NP2, r_begin, r_end, Y, scale);
-    else imat_apply32_t<3, 2>(tm, IMT32, ld, x, NP2, r_begin, r_end, Y, scale);
-  } else {
-    if (D == 1) imat_apply_t<1, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
-    else imat_apply_t<3, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
-  }
+  if (D == 1) imat_apply_t<1, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
+  else imat_apply_t<3, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
 }
 
 // ------------------------------------------------------------------ crews (thread-block clusters)
@@ -1036,8 +959,7 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
   const int NP = T.NP, NP2 = NP * NP, len = D * NP2;
   const double *cst = tv.cst + (size_t)ts * CST_N * NP;
   const double *Dfix = tv.Dfix + (size_t)ts * NP2, *Vfix = tv.Vfix + (size_t)ts * NP2;
-  const double *IMT = tv.imat ? tv.imat + (size_t)ts * imat_stride(NP2) : nullptr;
-  const float *IMT32 = tv.imat32 ? tv.imat32 + (size_t)ts * imat_stride(NP2) : nullptr;
+  const double *IMT = tv.imat + (size_t)ts * imat_stride(NP2);
   const int ld = sc.ld;
   double *sF = sc.tile, *sH = sF + len, *sHn = sH + len, *sFb = sHn + len, *sHb = sFb + len;
   short *deg = (short *)(sHb + len);
@@ -1082,11 +1004,11 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
     }
     tm.sync();
     if (crew) {
-      imat_apply(tm, IMT, IMT32, ld, sc.xs, NP2, D, r0, r1, xgF, T.CONST3);
+      imat_apply(tm, IMT, ld, sc.xs, NP2, D, r0, r1, xgF, T.CONST3);
       cl.sync();                // every CTA's rows of the new F are in L2
       for (int k = tm.rank; k < len; k += tm.size) sF[k] = xgF[k];
     } else {
-      imat_apply(tm, IMT, IMT32, ld, sc.xs, NP2, D, 0, NP2, sF, T.CONST3);
+      imat_apply(tm, IMT, ld, sc.xs, NP2, D, 0, NP2, sF, T.CONST3);
     }
     tm.sync();
     for (int k = tm.rank; k < len; k += tm.size) {
@@ -1095,11 +1017,11 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
     }
     tm.sync();
     if (crew) {
-      imat_apply(tm, IMT, IMT32, ld, sc.xs, NP2, D, r0, r1, xgH, cst + CST_INVH * NP);
+      imat_apply(tm, IMT, ld, sc.xs, NP2, D, r0, r1, xgH, cst + CST_INVH * NP);
       cl.sync();
       for (int k = tm.rank; k < len; k += tm.size) sHn[k] = xgH[k];
     } else {
-      imat_apply(tm, IMT, IMT32, ld, sc.xs, NP2, D, 0, NP2, sHn, cst + CST_INVH * NP);
+      imat_apply(tm, IMT, ld, sc.xs, NP2, D, 0, NP2, sHn, cst + CST_INVH * NP);
     }
     tm.sync();
     mv.stop(tm, PH_MATVEC);

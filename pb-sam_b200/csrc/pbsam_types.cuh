@@ -41,8 +41,7 @@ struct TypeView {
   const int *near_off, *near;        // CSR: intra near list (type sphere indices within the type)
   double *Dfix, *Vfix;               // [TS][NP2]
   double *cst;                       // [TS][CST_N][NP]
-  const double *imat;                // [TS][NP2][ld] row-major (see imat_stride); null in FP32 mode
-  const float *imat32;               // [TS][NP2][ld] the same in FP32 (mixed-precision mode), else null
+  const double *imat;                // [TS][NP2][ld] row-major (see imat_stride)
   // charges of each type (for the fixed-charge expansions)
   const int *chg_off;      // [ntypes+1]
   const double *chg_pos;   // [TQ][3] relative to the molecule centre
