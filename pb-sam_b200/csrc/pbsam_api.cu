@@ -722,6 +722,9 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   bv.crew = s->adaptive ? PBSAM_MAX_CREW : s->crew;   // scratch blocks per system: the largest crew it may get
   bv.scr_stride = scr_doubles(NP, S);
   chk(dalloc(Bf, &bv.scr, (size_t)B * bv.crew * bv.scr_stride));
+  bv.wscr_stride = NP <= PBSAM_WARP_MAX_NP ? warp_scr_doubles(NP) : 0;   // no warp transforms above
+  chk(dalloc(Bf, &bv.wscr, (size_t)B * bv.crew * PBSAM_WARPS * bv.wscr_stride));
+  chk(dalloc(Bf, &bv.dorder, (size_t)B * bv.crew * S));
   if (s->adaptive) chk(dalloc(Bf, &s->d_list, B));
   chk(dalloc(Bf, &bv.force, B * n_mol * 3)); chk(dalloc(Bf, &bv.torque, B * n_mol * 3));
   chk(dalloc(Bf, &bv.energy, B)); chk(dalloc(Bf, &bv.status, B)); chk(dalloc(Bf, &bv.stats, B * 8));

@@ -19,6 +19,12 @@ struct Team {
   int rank, size;
   __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
+// one warp working alone on an object (rank = lane, size = 32): the functions
+// templated on the team type run with either
+struct WarpTeam {
+  int rank, size;
+  __device__ __forceinline__ void sync() const { __syncwarp(); }
+};
 
 // Constant tables of one context (built on the host by the same formulas as
 // src/expansion.cpp:39-96, src/rotcoeff.cpp:15-33, 949-983,
@@ -162,7 +168,8 @@ __device__ __forceinline__ void sh_column(const Tab &T, double cost, double sint
 }
 
 // team: full SH expansion of P degrees at (theta, phi) into out[P*P]
-__device__ void sh_full(const Team &tm, const Tab &T, double theta, double phi, int P, double *out)
+template <class TM>
+__device__ void sh_full(const TM &tm, const Tab &T, double theta, double phi, int P, double *out)
 {
   const double cost = cos(theta), sint = sin(theta);
   for (int m = tm.rank; m < P; m += tm.size) {
@@ -203,7 +210,8 @@ struct RotState {
 // entries with n < min(p, nout) in the [n][n+s][m] layout (a prefix of the full
 // layout), which is all the rotation apply reads.  With grad, dR (full layout,
 // n < 2p-1, global) is computed alongside.  shbuf: (2p-1)^2 doubles of scratch.
-__device__ void rot_compute(const Team &tm, const Tab &T, double theta, double phi, double xi, int p, bool grad,
+template <class TM>
+__device__ void rot_compute(const TM &tm, const Tab &T, double theta, double phi, double xi, int p, bool grad,
                             RotState &rs, double2 *R, double2 *dR, double *shbuf, double2 *lvA, double2 *lvB,
                             int nout = 1 << 20)
 {
@@ -298,7 +306,8 @@ __device__ __forceinline__ void quat_angles(const double *q, double &th, double 
 
 // team: rotate Min -> Mout for degrees < p2 (src/rotcoeff.cpp:356-441);
 // Mout is written for degrees < p2 and zeroed up to zero_to degrees.
-__device__ void rot_apply(const Team &tm, const RotState &rs, const double *Min, double *Mout, int p2, bool bFor,
+template <class TM>
+__device__ void rot_apply(const TM &tm, const RotState &rs, const double *Min, double *Mout, int p2, bool bFor,
                           int zero_to)
 {
   for (int i = tm.rank + p2 * p2; i < zero_to * zero_to; i += tm.size) Mout[i] = 0.0;
@@ -386,7 +395,8 @@ __device__ __forceinline__ double2 sing_in0(const double *Mi, int m)
 { return (m == 1) ? make_double2(Mi[0], 0.0) : make_double2(Mi[2 * (m - 1) - 1], Mi[2 * (m - 1)]); }
 
 // team: dR/dtheta (kind 0) or dR/dphi (kind 1) applied to Min (src/rotcoeff.cpp:449-606)
-__device__ void drot_apply(const Team &tm, const Tab &T, const RotState &rs, const double *Min, double *Mout, int p2,
+template <class TM>
+__device__ void drot_apply(const TM &tm, const Tab &T, const RotState &rs, const double *Min, double *Mout, int p2,
                            bool bFor, int kind, int zero_to)
 {
   for (int i = tm.rank + p2 * p2; i < zero_to * zero_to; i += tm.size) Mout[i] = 0.0;
@@ -488,7 +498,8 @@ struct TransState {
 // CTransCoeff::reset + computeCoeff + computeCoeff_ (src/transcoeff.cpp:150-449).
 // kap is this transform's screening (0 for the F re-expansion); the recursion
 // itself always uses the context's kappa, as the reference does.
-__device__ void trans_compute(const Team &tm, const Tab &T, double d, double kap, int p, double scalei, double scaleo,
+template <class TM>
+__device__ void trans_compute(const TM &tm, const Tab &T, double d, double kap, int p, double scalei, double scaleo,
                               bool grad, TransState &ts, double *Tc, double *dTc, double *kbuf)
 {
   ts.p = p; ts.scalei = scalei; ts.scaleo = scaleo; ts.T = Tc; ts.dT = dTc;
@@ -566,7 +577,8 @@ __device__ void trans_compute(const Team &tm, const Tab &T, double d, double kap
 
 // team: forward translate (src/transcoeff.cpp:210-286 and 293-364 with tpose = false);
 // fact[k] = (scaleo/scalei)^k.  Out written for p degrees, zeroed up to zero_to.
-__device__ void trans_apply(const Team &tm, const TransState &ts, const double *fact, const double *Min, double *Mout,
+template <class TM>
+__device__ void trans_apply(const TM &tm, const TransState &ts, const double *fact, const double *Min, double *Mout,
                             bool deriv, int zero_to)
 {
   const int p = ts.p;

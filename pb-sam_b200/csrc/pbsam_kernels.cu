@@ -124,10 +124,63 @@ __device__ Scr make_scr(double *base, int NP, void *smem)
   return s;
 }
 
+// Pairs of truncation order <= PBSAM_WARP_P in the gradient re-expansion lists are
+// transformed by single warps, each with its own scratch block in global memory:
+// spherical harmonics, rotation coefficients (R for n < p, dR for n < 2p-1) and
+// their two recursion levels, translation coefficients and their derivative, the
+// factor table, three work expansions, the transform's output and the warp's sum.
+#define PBSAM_WARP_P 12
+#define PBSAM_WARP_MAX_NP 16      // warp transforms only at pole orders up to this (measured: they pay at
+                                  // p = 10; at p = 30 the wide CTA path stays)
+#define PBSAM_WARPS 16            // warp scratch blocks per CTA (a 512-thread team)
+__host__ __device__ inline long long even_up(long long n) { return (n + 1) & ~1LL; }
+__host__ __device__ inline long long warp_scr_doubles(int NP)
+{
+  const int pw = NP < PBSAM_WARP_P ? NP : PBSAM_WARP_P, NN = 2 * pw - 1;
+  const long long NP2 = (long long)NP * NP;
+  long long n = even_up((long long)NN * NN);
+  n += even_up(2LL * rot_off(pw)) + even_up(2LL * rot_off(NN));
+  n += 2 * even_up(tr_off(NN));
+  n += even_up(2 * NP + 2) + even_up(NP + 8);
+  n += 3 * even_up(3 * NP2);
+  n += 2 * even_up(2LL * NN * NN);
+  return (n + 7) & ~7LL;
+}
+__device__ Scr warp_scr(double *base, int NP)
+{
+  const int pw = NP < PBSAM_WARP_P ? NP : PBSAM_WARP_P, NN = 2 * pw - 1;
+  Scr s;
+  s.NP2 = NP * NP;
+  s.ld = imat_ld(s.NP2);
+  s.tile_pts = 0;
+  double *p = base;
+  auto take = [&](long long n) { double *r = p; p += even_up(n); return r; };
+  s.sh = take((long long)NN * NN);
+  s.R = (double2 *)take(2LL * rot_off(pw));
+  s.dR = (double2 *)take(2LL * rot_off(NN));
+  s.TH = take(tr_off(NN));
+  s.dTH = take(tr_off(NN));
+  s.TF = nullptr;
+  s.kbuf = take(2 * NP + 2);
+  s.fact = take(NP + 8);
+  s.e = take(3LL * s.NP2);        // E(0..2)
+  s.g = take(3LL * s.NP2);        // G(0): the transform's output
+  s.misc = take(3LL * s.NP2);     // the warp's running sum
+  s.lvA = (double2 *)take(2LL * NN * NN);
+  s.lvB = (double2 *)take(2LL * NN * NN);
+  s.sol = nullptr; s.mv = nullptr; s.tile = nullptr; s.xs = nullptr;
+  return s;
+}
+
 // scratch block of CTA `rank` of system b's crew
 __device__ __forceinline__ double *scr_of(const BatchView &bv, int b, int rank)
 {
   return bv.scr + ((size_t)b * bv.crew + rank) * bv.scr_stride;
+}
+// warp scratch block w of CTA `rank` of system b's crew
+__device__ __forceinline__ double *wscr_of(const BatchView &bv, int b, int rank, int w)
+{
+  return bv.wscr + (((size_t)b * bv.crew + rank) * PBSAM_WARPS + w) * bv.wscr_stride;
 }
 
 // ------------------------------------------------------------------ phase timers
@@ -148,11 +201,14 @@ struct PhaseClock {
 
 
 // ------------------------------------------------------------------ team helpers
-__device__ __forceinline__ void tcopy(const Team &tm, double *dst, const double *src, int n)
+template <class TM>
+__device__ __forceinline__ void tcopy(const TM &tm, double *dst, const double *src, int n)
 { for (int i = tm.rank; i < n; i += tm.size) dst[i] = src[i]; }
-__device__ __forceinline__ void tzero(const Team &tm, double *dst, int n)
+template <class TM>
+__device__ __forceinline__ void tzero(const TM &tm, double *dst, int n)
 { for (int i = tm.rank; i < n; i += tm.size) dst[i] = 0.0; }
-__device__ __forceinline__ void tadd(const Team &tm, double *dst, const double *src, int n)
+template <class TM>
+__device__ __forceinline__ void tadd(const TM &tm, double *dst, const double *src, int n)
 { for (int i = tm.rank; i < n; i += tm.size) dst[i] += src[i]; }
 
 // deterministic team sum: xor butterfly within each warp, then the warp sums in order
@@ -193,7 +249,8 @@ struct PairXf {
 
 // Coefficients for re-expanding a source centred at c_src into a target centred
 // at c_tgt, P = c_tgt - c_src.  pF > 0 also prepares the unscreened (F) translation.
-__device__ void prep_pair(const Team &tm, const Tab &T, const Scr &sc, const double *P, int pH, int pF,
+template <class TM>
+__device__ void prep_pair(const TM &tm, const Tab &T, const Scr &sc, const double *P, int pH, int pF,
                           double sS, double sT, bool grad, PairXf &X)
 {
   const Sph S = cart2sph(P[0], P[1], P[2]);
@@ -436,7 +493,8 @@ __device__ __noinline__ void pair_apply_multi(const Team &tm, const Tab &T, cons
 
 // gradient of the re-expansion w.r.t. the target position (src/xforms.cpp:85-115, 164-192);
 // G holds 3 expansions (x, y, z), each zero-padded to NP.
-__device__ void pair_apply_grad(const Team &tm, const Tab &T, const Scr &sc, const PairXf &X, const double *Min,
+template <class TM>
+__device__ void pair_apply_grad(const TM &tm, const Tab &T, const Scr &sc, const PairXf &X, const double *Min,
                                 double *G)
 {
   const int p = X.pH, NP2 = T.NP * T.NP;
@@ -1158,7 +1216,8 @@ struct Sys {
   }
 };
 
-__device__ void add_vec_into(const Team &tm, double *dst, const double *src, int n)
+template <class TM>
+__device__ void add_vec_into(const TM &tm, double *dst, const double *src, int n)
 {
   for (int i = tm.rank; i < n; i += tm.size) dst[i] += src[i];
   tm.sync();
@@ -1315,20 +1374,100 @@ __device__ __noinline__ void grad_xform_from(const Team &tm, const Sys &y, int s
   add_vec_into(tm, acc, G, 3 * y.NP2);
 }
 
+// truncation order of the re-expansion of sphere sm into sphere s (src/molecule.cpp:1516)
+__device__ __forceinline__ int pair_order(const Sys &y, int s, int sm, bool self)
+{
+  double ci[3], cm[3];
+  y.cen_lab(s, ci);
+  y.cen_lab(sm, cm);
+  const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+  const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
+  const double TQ = self ? y.c->tv.tHself[y.ts(sm)] : y.c->bv.tH[y.sc1(sm)];
+  return compute_order(y.NP, rho, TQ, y.rad(sm));
+}
+
+// grad_xform_from run by one warp (tw) with its own scratch ws, added into acc
+__device__ __noinline__ void grad_xform_warp(const WarpTeam &tw, const Sys &y, const Scr &ws, int s, int sm, bool self,
+                                             double *acc)
+{
+  const Tab &T = y.c->T;
+  double ci[3], cm[3];
+  y.cen_lab(s, ci);
+  y.cen_lab(sm, cm);
+  const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+  const int p = pair_order(y, s, sm, self);
+  PairXf X;
+  prep_pair(tw, T, ws, P, p, 0, y.rad(sm), y.rad(s), true, X);
+  double *G = ws.G(0);
+  pair_apply_grad(tw, T, ws, X, self ? y.HselfRot(sm) : y.Hrot(sm), G);
+  add_vec_into(tw, acc, G, 3 * y.NP2);
+}
+
 // This CTA's share of a list of gradient re-expansions into sphere s: the
 // neighbours of s's polarization list (use_ipol) then of its interaction list
 // (use_iact), optionally only those of molecule filter_mol; entries rank,
-// rank + size, ... are summed into part (3 * NP2, zeroed here).
+// rank + size, ... are summed into part (3 * NP2, written here).  The pair orders
+// are computed first, one entry per thread.  When the pole order is at most
+// PBSAM_WARP_MAX_NP and the share holds at least two pairs of order <=
+// PBSAM_WARP_P per warp (most pairs of these lists are far apart
+// and of low order, too narrow to keep a whole CTA busy), those pairs are dealt
+// round-robin to the CTA's warps, each transforming its pairs alone, and the
+// warps' sums are added in warp order; the other pairs are added one by one, each
+// transformed by the whole CTA.
 __device__ void dta_share(const Team &tm, const Sys &y, int s, bool self, int filter_mol, bool use_ipol, bool use_iact,
                           int rank, int size, double *part)
 {
-  tzero(tm, part, 3 * y.NP2);
-  tm.sync();
+  const int NP2 = y.NP2, nw = tm.size >> 5, w = tm.rank >> 5;
+  const int pw = y.NP < PBSAM_WARP_P ? y.NP : PBSAM_WARP_P;
   const int n1 = use_ipol ? y.nipol(s) : 0, n2 = use_iact ? y.niact(s) : 0;
-  for (int e = rank; e < n1 + n2; e += size) {
-    const int sm = e < n1 ? y.ipol(s)[e] : y.iact(s)[e - n1];
-    if (filter_mol >= 0 && y.mol(sm) != filter_mol) continue;
-    grad_xform_from(tm, y, s, sm, self, part);
+  const int cnt = (n1 + n2 > rank) ? (n1 + n2 - rank + size - 1) / size : 0;
+  const BatchView &bv = y.c->bv;
+  int *ord = bv.dorder + ((size_t)y.b * bv.crew + rank) * bv.S;     // order of local entry u, -1 if filtered out
+  int n_low = 0;
+  for (int u0 = 0; u0 < cnt; u0 += tm.size) {
+    const int u = u0 + tm.rank;
+    int low = 0;
+    if (u < cnt) {
+      const int e = rank + u * size;
+      const int sm = e < n1 ? y.ipol(s)[e] : y.iact(s)[e - n1];
+      int o = -1;
+      if (filter_mol < 0 || y.mol(sm) == filter_mol) o = pair_order(y, s, sm, self);
+      ord[u] = o;
+      low = (o >= 0 && o <= pw);
+    }
+    n_low += __syncthreads_count(low);
+  }
+  const bool warps = y.NP <= PBSAM_WARP_MAX_NP && n_low >= 2 * nw;
+  if (warps) {
+    const WarpTeam tw{tm.rank & 31, 32};
+    const Scr ws = warp_scr(wscr_of(bv, y.b, rank, w), y.NP);
+    double *wacc = ws.misc;
+    tzero(tw, wacc, 3 * NP2);
+    tw.sync();
+    int j = 0;
+    for (int u = 0; u < cnt; u++) {
+      const int o = ord[u];
+      if (o < 0 || o > pw) continue;
+      if ((j++ % nw) != w) continue;
+      const int e = rank + u * size;
+      grad_xform_warp(tw, y, ws, s, e < n1 ? y.ipol(s)[e] : y.iact(s)[e - n1], self, wacc);
+    }
+    tm.sync();
+    const size_t moff = (size_t)(warp_scr(wscr_of(bv, y.b, rank, 0), y.NP).misc - wscr_of(bv, y.b, rank, 0));
+    for (int i = tm.rank; i < 3 * NP2; i += tm.size) {
+      double v = 0.0;
+      for (int q = 0; q < nw; q++) v += wscr_of(bv, y.b, rank, q)[moff + i];
+      part[i] = v;
+    }
+  } else {
+    tzero(tm, part, 3 * NP2);
+  }
+  tm.sync();
+  for (int u = 0; u < cnt; u++) {
+    const int o = ord[u];
+    if (o < 0 || (warps && o <= pw)) continue;
+    const int e = rank + u * size;
+    grad_xform_from(tm, y, s, e < n1 ? y.ipol(s)[e] : y.iact(s)[e - n1], self, part);
   }
 }
 
@@ -1342,12 +1481,9 @@ __device__ void crew_dta(const Team &tm, const Sys &y, int s, bool self, int fil
   pc.start(tm);
   const Crew &cw = y.cw;
   if (cw.size == 1) {
-    const int n1 = use_ipol ? y.nipol(s) : 0, n2 = use_iact ? y.niact(s) : 0;
-    for (int e = 0; e < n1 + n2; e++) {
-      const int sm = e < n1 ? y.ipol(s)[e] : y.iact(s)[e - n1];
-      if (filter_mol >= 0 && y.mol(sm) != filter_mol) continue;
-      grad_xform_from(tm, y, s, sm, self, acc);
-    }
+    double *part = y.sc.G(7);
+    dta_share(tm, y, s, self, filter_mol, use_ipol, use_iact, 0, 1, part);
+    add_vec_into(tm, acc, part, 3 * y.NP2);
     pc.stop(tm, PH_DTA);
     return;
   }

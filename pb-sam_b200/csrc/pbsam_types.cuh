@@ -84,6 +84,9 @@ struct BatchView {
   double *sep;               // [B][S][S] sphere-sphere surface gaps
   double *scr;               // [B][crew][scr_stride]: one scratch block per CTA
   long long scr_stride;
+  int *dorder;               // [B][crew][S] pair orders of a CTA's share of a gradient list
+  double *wscr;              // [B][crew][16 warps][wscr_stride]: per-warp scratch of the
+  long long wscr_stride;     // gradient re-expansion lists (pairs of low order)
   int crew;                  // CTAs per system
   double *force, *torque, *energy;  // [B][nmol][3], [B][nmol][3], [B]
   int *status;               // [B]
