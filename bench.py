@@ -256,7 +256,7 @@ def run_ours(args):
 BD_METRIC = "BD steps/s (two-molecule bdnam trajectories, p=10)"
 BD_WORKLOAD = ("bdnam p=10: %d trajectories of 2 molecules x 35 spheres (r 3-6 A, 1200 charges, net +2/-2), start "
                "50 A, escape 150 A, dt 0.02 ps at contact rising to 2 ps at a 30 A gap, Stokes-Einstein D, Philox "
-               "noise; a step = force evaluation (where c2c < 100 A) + Ermak-McCammon move")
+               "noise; a step = force evaluation (where c2c < 100 A) + Ermak-McCammon move, one CUDA graph")
 
 
 def run_bd(args, local, rank, world, dist):
@@ -277,8 +277,7 @@ def run_bd(args, local, rank, world, dist):
     stream = torch.cuda.current_stream()
     sysb.set_stream(stream.cuda_stream)
     sysb.set_poses(pos, quat)
-    sysb.bd_init([0.0, dtr], [drot, drot], mode=0, seed=1234 + rank, persistent=bool(args.bd_persistent),
-                 escape_dist=cfg["escape"],
+    sysb.bd_init([0.0, dtr], [drot, drot], mode=0, seed=1234 + rank, escape_dist=cfg["escape"],
                  dt_min=cfg["dt_min"], dt_max=cfg["dt_max"], dt_ref=0.0,
                  dt_div=cfg["dt_gap"] / (cfg["dt_max"] - cfg["dt_min"]))
     sysb.bd_run(args.warmup)
@@ -317,8 +316,6 @@ def run_bd(args, local, rank, world, dist):
     out = {"metric": BD_METRIC, "value": units_all / (ms_max * 1e-3), "unit": "BD steps/s",
            "ms_per_step": ms_max / args.bd_steps, "steps": args.bd_steps, "warmup": args.warmup, "dtype": "f64",
            "config": {"workload": BD_WORKLOAD % B, "trajectories_per_gpu": B, "team_threads": args.bd_team,
-                      "launch": "persistent: one launch per bd_run, CTAs take whole trajectories" if args.bd_persistent
-                      else "one CUDA graph (3 kernels) per step",
                       "dtr_A2_per_ps": dtr,
                       "drot_rad2_per_ps": drot},
            "force_evaluations_fraction": fe / max(units, 1),
@@ -326,7 +323,7 @@ def run_bd(args, local, rank, world, dist):
                              ((0, "running"), (1, "escaped"), (2, "stuck"), (4, "failed"))},
            "e2e": {"value": e2e_units / (e2e_ms * 1e-3), "unit": "BD steps/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": d2h, "note": "one step per call, state read back to the host each step"},
-           "gpu_launches": 1 if args.bd_persistent else 3 * args.bd_steps, "clocks": clocks, "prep": prep_t}
+           "gpu_launches": 3 * args.bd_steps, "clocks": clocks, "prep": prep_t}
     if rank == 0 and args.cpu_baseline:
         out["cpu_baseline"] = bd_cpu_baseline(cfg, specs, sysb, s1, fe / max(units, 1), args)
     sysb.close()
@@ -547,8 +544,6 @@ def main():
     ap.add_argument("--bd", type=int, default=1, help="also time the Brownian-dynamics workload")
     ap.add_argument("--bd-traj", type=int, default=1024, help="BD trajectories per GPU")
     ap.add_argument("--bd-steps", type=int, default=20, help="timed BD steps")
-    ap.add_argument("--bd-persistent", type=int, default=0,
-                    help="run the BD steps of whole trajectories in one launch (0: one CUDA graph per step)")
     ap.add_argument("--bd-team", type=int, default=512, help="threads per CTA of the BD force kernel (128 or 512)")
     ap.add_argument("--selfpol-rounds-p10", type=int, default=200)
     ap.add_argument("--poses", default="", help="comma-separated subset of the sweep's poses (small cases)")

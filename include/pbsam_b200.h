@@ -184,11 +184,6 @@ typedef struct pbsam_bd_params {
   double coul_k;         /* COUL_K = 2.30708e-18 */
   unsigned long long seed;
   int use_graph;         /* 1: a step is replayed as one CUDA graph */
-  int persistent;        /* 1: pbsam_system_bd_run runs all its steps in one launch in which each
-                            CTA takes whole trajectories from a work queue (one CTA per system,
-                            whatever the context's cluster_size), so no step waits for the slowest
-                            trajectory of the batch; the results equal the stepwise path's with
-                            cluster_size 1 */
 } pbsam_bd_params;
 
 /* Reference values of the chosen driver (src/BDnam.h:10-25, src/BDmulti.cpp:13,

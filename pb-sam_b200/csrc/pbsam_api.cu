@@ -539,7 +539,6 @@ static int set_smem_attrs(int NP)
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   }
   CK(cudaFuncSetAttribute(pbsam_selfpol_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  CK(cudaFuncSetAttribute(pbsam_bd_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   CK(cudaFuncSetAttribute(pbsam_energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   CK(cudaFuncSetAttribute(pbsam_setup1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   CK(cudaFuncSetAttribute(pbsam_setup2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));

@@ -10,13 +10,11 @@
 //         in turn; forces while the minimum separation is below the interaction
 //         cutoff; the time step follows that minimum separation.
 //
-// Stepwise, one step is three launches on the system's stream: pbsam_bd_pre_kernel
+// One step is three launches on the system's stream: pbsam_bd_pre_kernel
 // (time step, whether forces are needed: the mask the force kernel reads),
 // pbsam_forces_kernel (skips masked systems) and pbsam_bd_move_kernel (drift
 // from the forces, Gaussian noise, rejection of moves that make spheres of two
 // molecules overlap, at most max_tries draws per move as the reference's maxc).
-// Persistent, pbsam_bd_persistent_kernel runs many steps of whole trajectories
-// in one launch with the same device functions.
 //
 // Noise: Philox4x64-10 (Salmon et al., "Parallel random numbers: as easy as
 // 1, 2, 3", SC 2011), key (seed, 0), counter (draw, system, 0, 0); one block of
@@ -167,12 +165,12 @@ __device__ void bd_rotate_centres(const Ctx &c, const BDView &v, int b, int i)
     qrot(q, c.tv.cen + 3 * bv.sph_ts[k], v.cen + ((size_t)b * bv.S + k) * 3);
 }
 
-// time step and force mask of system b (all threads of the block; red: a shared
-// buffer of blockDim.x doubles, blockDim.x a power of two)
-__device__ void bd_pre(const Ctx &c, const BDParams &p, const BDView &v, int b, double *red)
+// time step and force mask of every running system
+__global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_kernel(Ctx c, BDParams p, BDView v)
 {
   const BatchView &bv = c.bv;
-  const int nmol = bv.nmol;
+  const int b = blockIdx.x, nmol = bv.nmol;
+  if (b >= bv.B) return;
   if (v.status[b] != BD_RUNNING) {
     if (threadIdx.x == 0) v.need[b] = 0;
     return;
@@ -216,6 +214,7 @@ __device__ void bd_pre(const Ctx &c, const BDParams &p, const BDView &v, int b, 
         mmin = dm;
       }
     }
+  __shared__ double red[PBSAM_BD_THREADS];
   red[threadIdx.x] = smin;
   __syncthreads();
   for (int h = blockDim.x / 2; h > 0; h >>= 1) {
@@ -229,14 +228,6 @@ __device__ void bd_pre(const Ctx &c, const BDParams &p, const BDView &v, int b, 
     v.dt[b] = bd_dt(p, md);
     v.need[b] = md < p.interact_cut;
   }
-}
-
-// time step and force mask of every running system
-__global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_kernel(Ctx c, BDParams p, BDView v)
-{
-  __shared__ double red[PBSAM_BD_THREADS];
-  if (blockIdx.x >= c.bv.B) return;
-  bd_pre(c, p, v, blockIdx.x, red);
 }
 
 // one random vector of standard deviation sd added to base (thread 0 only)
@@ -304,14 +295,14 @@ __device__ int bd_rotate(const Ctx &c, const BDParams &p, const BDView &v, int b
   return tries;
 }
 
-// the move of system b (all threads of the block; bd_rel: shared, 3 doubles per
-// sphere of the largest molecule; sm, s_status: shared scratch)
-__device__ void bd_move(const Ctx &c, const BDParams &p, const BDView &v, int b, double *bd_rel, double *sm,
-                        int &s_status)
+__global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_move_kernel(Ctx c, BDParams p, BDView v)
 {
+  extern __shared__ double bd_rel[];          // [max spheres of a molecule][3]
+  __shared__ double sm[8];
+  __shared__ int s_status;
   const BatchView &bv = c.bv;
-  const int nmol = bv.nmol;
-  if (v.status[b] != BD_RUNNING) return;
+  const int b = blockIdx.x, nmol = bv.nmol;
+  if (b >= bv.B || v.status[b] != BD_RUNNING) return;
   const double dt = v.dt[b];
   const bool need = v.need[b] != 0;
   if (need && bv.status[b] != PBSAM_STATUS_OK) {   // the reference exits here (src/BDnam.cpp:210-212)
@@ -391,50 +382,6 @@ __device__ void bd_move(const Ctx &c, const BDParams &p, const BDView &v, int b,
     v.steps[b]++;
     v.time[b] += dt;
     if (need) v.fevals[b]++;
-  }
-}
-
-__global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_move_kernel(Ctx c, BDParams p, BDView v)
-{
-  extern __shared__ double bd_rel[];          // [max spheres of a molecule][3]
-  __shared__ double sm[8];
-  __shared__ int s_status;
-  if (blockIdx.x >= c.bv.B) return;
-  bd_move(c, p, v, blockIdx.x, bd_rel, sm, s_status);
-}
-
-// Whole trajectories in one launch: every CTA (one 512-thread team, as in the
-// force kernel with one CTA per system) takes the next trajectory from the work
-// counter *next and runs n_steps steps of it (time step and force mask, force
-// evaluation when needed, move) before taking another, so trajectories advance at
-// their own pace and no step waits for the slowest system of the batch.  The
-// arithmetic of a trajectory is the stepwise path's with one CTA per system.
-// *next must be 0 at launch.
-__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_bd_persistent_kernel(Ctx c, BDParams p, BDView v, int n_steps,
-                                                                         int *next)
-{
-  extern __shared__ double2 dsm[];
-  __shared__ double red[PBSAM_TEAM];
-  __shared__ CrewCmd cmd;
-  __shared__ double sm[8];
-  __shared__ int s_status, s_b;
-  const Team tm{(int)threadIdx.x, (int)blockDim.x};
-  const Crew cw{0, 1, &cmd};
-  for (;;) {
-    if (threadIdx.x == 0) s_b = atomicAdd(next, 1);
-    __syncthreads();
-    const int b = s_b;
-    __syncthreads();
-    if (b >= c.bv.B) break;
-    for (int k = 0; k < n_steps; k++) {
-      if (v.status[b] != BD_RUNNING) break;
-      bd_pre(c, p, v, b, red);
-      __syncthreads();
-      if (v.need[b]) forces_body(tm, c, cw, b, dsm, red);
-      __syncthreads();
-      bd_move(c, p, v, b, (double *)dsm, sm, s_status);
-      __syncthreads();
-    }
   }
 }
 

@@ -6,9 +6,7 @@ struct BDHost {
   BDParams p;
   BDView v;
   std::vector<void *> bufs;
-  int use_graph = 0, persistent = 0;
-  int *next = nullptr;                  // work counter of the persistent kernel
-  int persistent_grid = 0;
+  int use_graph = 0;
   size_t move_smem = 0;
   cudaStream_t st = nullptr;            // stream the steps (and the graph) run on
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -46,7 +44,6 @@ extern "C" void pbsam_bd_params_default(int mode, pbsam_bd_params *p)
   p->coul_k = 2.30708e-18;                  // COUL_K, src/BDnam.h:19
   p->seed = 0;
   p->use_graph = 1;
-  p->persistent = 0;
 }
 
 extern "C" int pbsam_system_bd_init(pbsam_system *s, const pbsam_bd_params *prm, const double *dtr, const double *drot)
@@ -74,7 +71,6 @@ extern "C" int pbsam_system_bd_init(pbsam_system *s, const pbsam_bd_params *prm,
   p.interact_cut = s->ctx->prm.interact_cutoff;
   p.seed = prm->seed;
   h->use_graph = prm->use_graph;
-  h->persistent = prm->persistent;
   const size_t B = s->B, nm = s->nmol, S = s->c.bv.S;
   BDView &v = h->v;
   int r = 0;
@@ -82,7 +78,6 @@ extern "C" int pbsam_system_bd_init(pbsam_system *s, const pbsam_bd_params *prm,
   chk(dalloc(h->bufs, &v.status, B)); chk(dalloc(h->bufs, &v.steps, B)); chk(dalloc(h->bufs, &v.fevals, B));
   chk(dalloc(h->bufs, &v.time, B)); chk(dalloc(h->bufs, &v.dt, B)); chk(dalloc(h->bufs, &v.ctr, B));
   chk(dalloc(h->bufs, &v.rot, B * nm * 4)); chk(dalloc(h->bufs, &v.need, B)); chk(dalloc(h->bufs, &v.cen, B * S * 3));
-  chk(dalloc(h->bufs, &h->next, 1));
   std::vector<double> hd(dtr, dtr + nm), hr(drot, drot + nm);
   chk(dput(h->bufs, &v.dtr, hd)); chk(dput(h->bufs, &v.drot, hr));
   if (r) { bd_free(s); return r; }
@@ -98,16 +93,6 @@ extern "C" int pbsam_system_bd_init(pbsam_system *s, const pbsam_bd_params *prm,
   h->move_smem = (size_t)max_ns * 3 * sizeof(double);
   if (h->move_smem > 48 * 1024)
     CK(cudaFuncSetAttribute(pbsam_bd_move_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->move_smem));
-  if (h->persistent) {
-    // one CTA per SM slot the kernel can hold, at most one per trajectory
-    const size_t smem = team_smem_bytes(s->ctx->prm.poles);
-    if (h->move_smem > smem) { bd_free(s); return fail(PBSAM_E_BADARG, "molecule too large for the persistent BD kernel"); }
-    int n_sm = 0, per_sm = 0;
-    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, s->ctx->device));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pbsam_bd_persistent_kernel, PBSAM_TEAM, smem));
-    if (per_sm < 1) { bd_free(s); return fail(PBSAM_E_CUDA, "persistent BD kernel does not fit an SM"); }
-    h->persistent_grid = std::min(s->B, n_sm * per_sm);
-  }
   CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming));
@@ -145,16 +130,6 @@ extern "C" int pbsam_system_bd_run(pbsam_system *s, int n_steps)
   if (n_steps == 0) return PBSAM_OK;
   CK(cudaEventRecord(h->ev_in, s->stream));
   CK(cudaStreamWaitEvent(h->st, h->ev_in, 0));
-  if (h->persistent) {
-    // all n_steps of every trajectory in one launch, trajectories taken from a work counter
-    CK(cudaMemsetAsync(h->next, 0, sizeof(int), h->st));
-    pbsam_bd_persistent_kernel<<<h->persistent_grid, PBSAM_TEAM, team_smem_bytes(s->ctx->prm.poles), h->st>>>(
-        s->c, h->p, h->v, n_steps, h->next);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(h->ev_out, h->st));
-    CK(cudaStreamWaitEvent(s->stream, h->ev_out, 0));
-    return PBSAM_OK;
-  }
   if (h->use_graph && !h->exec) {
     CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = bd_enqueue_step(s, h->st);

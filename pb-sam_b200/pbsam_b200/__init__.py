@@ -49,7 +49,7 @@ class pbsam_bd_params(ctypes.Structure):
                 ("escape_dist", ctypes.c_double), ("dt_min", ctypes.c_double), ("dt_max", ctypes.c_double),
                 ("dt_ref", ctypes.c_double), ("dt_div", ctypes.c_double), ("fact_tr", ctypes.c_double),
                 ("ikbt", ctypes.c_double), ("coul_k", ctypes.c_double), ("seed", ctypes.c_ulonglong),
-                ("use_graph", ctypes.c_int), ("persistent", ctypes.c_int)]
+                ("use_graph", ctypes.c_int)]
 
 
 # every entry point declared in include/pbsam_b200.h, with ctypes signatures
@@ -266,12 +266,12 @@ class Molecules:
         return m.value
 
     # ---- Brownian dynamics (CBDnam::run / CBDmulti::propagate)
-    def bd_init(self, dtr, drot, mode=PBSAM_BD_NAM, seed=0, use_graph=True, persistent=False, **kw):
+    def bd_init(self, dtr, drot, mode=PBSAM_BD_NAM, seed=0, use_graph=True, **kw):
         """Start one trajectory per system from the current poses.  dtr/drot: per-molecule
         translational (A^2/ps) and rotational (rad^2/ps) diffusion coefficients; kw
         overrides fields of pbsam_bd_params (max_tries, force_dist, escape_dist, dt_min,
         dt_max, dt_ref, dt_div, ...)."""
-        p = bd_params(mode, seed=seed, use_graph=int(bool(use_graph)), persistent=int(bool(persistent)), **kw)
+        p = bd_params(mode, seed=seed, use_graph=int(bool(use_graph)), **kw)
         dtr = np.ascontiguousarray(dtr, dtype=np.float64)
         drot = np.ascontiguousarray(drot, dtype=np.float64)
         if dtr.shape != (self.n_mol,) or drot.shape != (self.n_mol,):

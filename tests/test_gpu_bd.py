@@ -47,14 +47,13 @@ def check_step(g, b, o):
     np.testing.assert_allclose(g["quat"][b], o["quat"], rtol=0, atol=1e-9)
 
 
-def run_compare(tmp_path, mol_types, frame, mode, n, seed, dtr, drot, n_sys=2, use_graph=True, persistent=False,
-                **kw):
+def run_compare(tmp_path, mol_types, frame, mode, n, seed, dtr, drot, n_sys=2, use_graph=True, **kw):
     ctx, types, P = tiny_ctx()
     mol = ctx.molecules([types[t] for t in mol_types], n_systems=n_sys)
     pos = np.array([[m[1] for m in frame]] * n_sys)
     quat = np.array([[m[2] for m in frame]] * n_sys)
     mol.set_poses(pos, quat)
-    mol.bd_init(dtr, drot, mode=mode, seed=seed, use_graph=use_graph, persistent=persistent, **kw)
+    mol.bd_init(dtr, drot, mode=mode, seed=seed, use_graph=use_graph, **kw)
     ref = [oracle_traj(str(tmp_path), frame, mode, n, seed, b, dtr, drot, P, **kw) for b in range(n_sys)]
     states = []
     for k in range(n):
@@ -108,37 +107,3 @@ def test_escape_and_stuck_vs_oracle(tmp_path):
     stuck = [fr[0], (fr[1][0], [0.3, 0.0, 0.0], fr[1][2])]
     s2, ref2 = run_compare(tmp_path, [0, 1], stuck, 0, 2, 2, (0.0, 1e-8), DROT, max_tries=1, force_dist=0.0)
     assert ref2[0][0]["status"] == 2 and s2[-1]["status"][0] == 2
-
-
-def test_persistent_vs_oracle(tmp_path):
-    """One launch per call, each CTA running whole trajectories: step by step equal
-    to the oracle, NAM close range and MULTI."""
-    run_compare(tmp_path, [0, 1], gap5_frame(), 0, 6, 11, DTR, DROT, n_sys=3, persistent=True)
-    fr = gap5_frame()
-    third = (0, list(-np.array(fr[1][1])), [0.5, 0.5, -0.5, 0.5])
-    run_compare(tmp_path, [0, 1, 0], fr + [third], 1, 4, 9, (0.03, 0.03, 0.03), (4.5e-5, 4e-5, 4.5e-5),
-                persistent=True)
-
-
-def test_persistent_many_steps_equal_stepwise():
-    """Eight steps of five trajectories in one persistent launch equal eight graph
-    steps with one CTA per system, bit for bit."""
-    out = []
-    for persistent in (False, True):
-        ctx, types, P = tiny_ctx(cluster_size=1)
-        mol = ctx.molecules(types, n_systems=5)
-        fr = gap5_frame()
-        mol.set_poses(np.array([[m[1] for m in fr]] * 5), np.array([[m[2] for m in fr]] * 5))
-        mol.bd_init(DTR, DROT, mode=0, seed=21, persistent=persistent)
-        if persistent:
-            mol.bd_run(8)
-        else:
-            for _ in range(8):
-                mol.bd_run(1)
-        out.append(mol.bd_state())
-        mol.close()
-        ctx.close()
-    a, b = out
-    assert np.array_equal(a["steps"], b["steps"]) and np.array_equal(a["status"], b["status"])
-    assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["quat"], b["quat"])
-    assert np.array_equal(a["fevals"], b["fevals"]) and np.all(a["steps"] == 8)
