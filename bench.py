@@ -267,7 +267,7 @@ def run_bd(args, local, rank, world, dist):
     from pbsam_b200 import replicas, workload
     cfg = dict(workload.BD_P10)
     specs, prep_t, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds_p10)
-    ctx, types = workload.open_context(cfg, specs, device=local, team_threads=args.bd_team)
+    ctx, types = workload.open_context(cfg, specs, device=local)
     mols = workload.molecules(cfg)
     B = args.bd_traj
     pos, quat = workload.bd_start(cfg, mols, B, rank=rank)
@@ -315,8 +315,7 @@ def run_bd(args, local, rank, world, dist):
     d2h = sum(int(v.nbytes) for v in st.values())
     out = {"metric": BD_METRIC, "value": units_all / (ms_max * 1e-3), "unit": "BD steps/s",
            "ms_per_step": ms_max / args.bd_steps, "steps": args.bd_steps, "warmup": args.warmup, "dtype": "f64",
-           "config": {"workload": BD_WORKLOAD % B, "trajectories_per_gpu": B, "team_threads": args.bd_team,
-                      "dtr_A2_per_ps": dtr,
+           "config": {"workload": BD_WORKLOAD % B, "trajectories_per_gpu": B, "dtr_A2_per_ps": dtr,
                       "drot_rad2_per_ps": drot},
            "force_evaluations_fraction": fe / max(units, 1),
            "status_counts": {pb_status: int(np.sum(s1["status"] == k)) for k, pb_status in
@@ -544,7 +543,6 @@ def main():
     ap.add_argument("--bd", type=int, default=1, help="also time the Brownian-dynamics workload")
     ap.add_argument("--bd-traj", type=int, default=1024, help="BD trajectories per GPU")
     ap.add_argument("--bd-steps", type=int, default=20, help="timed BD steps")
-    ap.add_argument("--bd-team", type=int, default=512, help="threads per CTA of the BD force kernel (128 or 512)")
     ap.add_argument("--selfpol-rounds-p10", type=int, default=200)
     ap.add_argument("--poses", default="", help="comma-separated subset of the sweep's poses (small cases)")
     ap.add_argument("--traffic-per-launch", type=float, default=None,

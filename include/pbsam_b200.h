@@ -55,10 +55,6 @@ typedef struct pbsam_params {
                              inner-iteration counts, costlier systems getting larger clusters (the
                              rounding of the results may then differ between calls by ~1e-15).
                              No reference counterpart (a B200 launch parameter). */
-  int team_threads;       /* threads per CTA of the force kernel: 0 or 512 = one CTA per SM;
-                             128 = four CTAs per SM, each working on its own system (for small
-                             pole orders and large batches).  Changes only the rounding.
-                             No reference counterpart (a B200 launch parameter). */
 } pbsam_params;
 
 typedef struct pbsam_context pbsam_context;

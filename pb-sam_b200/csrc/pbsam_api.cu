@@ -154,7 +154,6 @@ struct pbsam_system {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
   int crew = 1;            // CTAs (one cluster) per system in the force kernel
-  int team = PBSAM_TEAM;   // threads per CTA of the force kernel
   // adaptive crews (cluster_size == -1): systems grouped by the cost of their last
   // evaluation, one launch per crew size on side streams
   bool adaptive = false;
@@ -196,7 +195,6 @@ extern "C" void pbsam_params_default(pbsam_params *p)
   p->inter_cutoff = 10; p->interact_cutoff = 100; p->intra_cutoff = 30; p->min_sep_numeric = 5;
   p->num_points_x = 10000;
   p->cluster_size = 0;
-  p->team_threads = 0;
 }
 
 static double kappa_of(const pbsam_params &p)
@@ -210,8 +208,6 @@ extern "C" int pbsam_context_create(const pbsam_params *prm, int device, pbsam_c
 {
   if (!prm || !out) return fail(PBSAM_E_BADARG, "null argument");
   if (prm->poles < 1 || prm->poles > 32) return fail(PBSAM_E_BADARG, "poles must be in [1, 32]");
-  if (prm->team_threads != 0 && prm->team_threads != PBSAM_TEAM && prm->team_threads != PBSAM_TEAM_SMALL)
-    return fail(PBSAM_E_BADARG, "team_threads must be 0 (512), 512 or 128");
   if (prm->cluster_size < -1 || prm->cluster_size > PBSAM_MAX_CREW)
     return fail(PBSAM_E_BADARG, "cluster_size must be -1 (adaptive), 0 (automatic) or 1..16");
   int ndev = 0;
@@ -477,12 +473,11 @@ static int dput(std::vector<void *> &bufs, const T **p, const std::vector<T> &h)
 
 // Launch n_sys crews of C CTAs (a thread-block cluster per system when C > 1).
 template <class... Exp, class... Act>
-static cudaError_t launch_crews(void (*kern)(Exp...), int n_sys, int C, int nt, size_t smem, cudaStream_t st,
-                                Act &&...args)
+static cudaError_t launch_crews(void (*kern)(Exp...), int n_sys, int C, size_t smem, cudaStream_t st, Act &&...args)
 {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(n_sys * C));
-  cfg.blockDim = dim3((unsigned)nt);
+  cfg.blockDim = dim3(PBSAM_TEAM);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
@@ -500,13 +495,13 @@ static cudaError_t launch_crews(void (*kern)(Exp...), int n_sys, int C, int nt, 
 // CTAs per system: the requested size, or the largest of 16, 8, 4, 2 at which all
 // n_sys crews are resident at once (cluster occupancy), else 1.
 template <class K>
-static int pick_crew(K kern, int n_sys, int nt, size_t smem, int requested)
+static int pick_crew(K kern, int n_sys, size_t smem, int requested)
 {
   if (requested > 0) return requested;
   for (int C : {16, 8, 4, 2}) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(n_sys * C));
-    cfg.blockDim = dim3((unsigned)nt);
+    cfg.blockDim = dim3(PBSAM_TEAM);
     cfg.dynamicSmemBytes = smem;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -522,22 +517,13 @@ static int pick_crew(K kern, int n_sys, int nt, size_t smem, int requested)
   return 1;
 }
 
-// the force kernel for a team of nt threads (PBSAM_TEAM or PBSAM_TEAM_SMALL)
-static void (*forces_kernel(int nt))(Ctx, const int *)
-{
-  if (nt == PBSAM_TEAM_SMALL) return pbsam_forces_kernel_t<PBSAM_TEAM_SMALL, 4>;
-  return pbsam_forces_kernel_t<PBSAM_TEAM, 1>;
-}
-
 // opt every team kernel into the dynamic shared memory it needs
 static int set_smem_attrs(int NP)
 {
   const int smem = (int)team_smem_bytes(NP);
-  for (auto k : {forces_kernel(PBSAM_TEAM), forces_kernel(PBSAM_TEAM_SMALL)}) {
-    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    // clusters of up to 16 CTAs (beyond the portable 8)
-    CK(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  }
+  CK(cudaFuncSetAttribute(pbsam_forces_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  // clusters of up to 16 CTAs (beyond the portable 8)
+  CK(cudaFuncSetAttribute(pbsam_forces_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   CK(cudaFuncSetAttribute(pbsam_selfpol_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   CK(cudaFuncSetAttribute(pbsam_energy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   CK(cudaFuncSetAttribute(pbsam_setup1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -716,8 +702,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   chk(dalloc(Bf, &bv.molRS, B * n_mol * 16));
   chk(dalloc(Bf, &bv.sep, B * S * S));
   s->adaptive = c->prm.cluster_size < 0;
-  s->team = c->prm.team_threads == PBSAM_TEAM_SMALL ? PBSAM_TEAM_SMALL : PBSAM_TEAM;
-  s->crew = pick_crew(forces_kernel(s->team), B, s->team, team_smem_bytes(NP), s->adaptive ? 0 : c->prm.cluster_size);
+  s->crew = pick_crew(pbsam_forces_kernel, B, team_smem_bytes(NP), s->adaptive ? 0 : c->prm.cluster_size);
   bv.crew = s->adaptive ? PBSAM_MAX_CREW : s->crew;   // scratch blocks per system: the largest crew it may get
   bv.scr_stride = scr_doubles(NP, S);
   chk(dalloc(Bf, &bv.scr, (size_t)B * bv.crew * bv.scr_stride));
@@ -846,14 +831,14 @@ extern "C" int pbsam_system_compute_forces(pbsam_system *s, double *force, doubl
   }
   CK(cudaEventRecord(s->ev0, s->stream));
   if (!s->adaptive || s->gsize.empty()) {
-    CK(launch_crews(forces_kernel(s->team), s->B, s->crew, s->team, smem, s->stream, s->c, (const int *)nullptr));
+    CK(launch_crews(pbsam_forces_kernel, s->B, s->crew, smem, s->stream, s->c, (const int *)nullptr));
   } else {
     // one launch per crew size on side streams, heaviest first, joined back
     CK(cudaEventRecord(s->ev_fork, s->stream));
     int off = 0;
     for (size_t g = 0; g < s->gsize.size(); g++) {
       CK(cudaStreamWaitEvent(s->gs[g], s->ev_fork, 0));
-      CK(launch_crews(forces_kernel(s->team), s->gcount[g], s->gsize[g], s->team, smem, s->gs[g], s->c,
+      CK(launch_crews(pbsam_forces_kernel, s->gcount[g], s->gsize[g], smem, s->gs[g], s->c,
                       (const int *)(s->d_list + off)));
       CK(cudaEventRecord(s->ev_join[g], s->gs[g]));
       off += s->gcount[g];
@@ -1032,7 +1017,7 @@ extern "C" int pbsam_selfpol(pbsam_context *c, int type_id, int max_rounds, doub
   TRY(pbsam_system_create(c, 1, 1, mt, &s));
   int *drounds = nullptr;
   if (cudaMalloc(&drounds, sizeof(int)) != cudaSuccess) { pbsam_system_destroy(s); return fail(PBSAM_E_NOMEM, "rounds"); }
-  cudaError_t e = launch_crews(pbsam_selfpol_kernel, 1, s->crew, PBSAM_TEAM, team_smem_bytes(c->prm.poles), s->stream, s->c,
+  cudaError_t e = launch_crews(pbsam_selfpol_kernel, 1, s->crew, team_smem_bytes(c->prm.poles), s->stream, s->c,
                                (const double *)c->tv.Eass, max_rounds, drounds);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);

@@ -16,7 +16,6 @@ namespace pbsam {
 namespace cg = cooperative_groups;
 
 #define PBSAM_TEAM 512
-#define PBSAM_TEAM_SMALL 128    // the narrow team variant of the force kernel
 #define PBSAM_MAX_CREW 16       // CTAs (one thread-block cluster) per system at most
 
 // ------------------------------------------------------------------ scratch
@@ -2054,14 +2053,10 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
 
 // Grid: crews of cluster-size CTAs (a plain launch is a crew of one), one per
 // system; crew k works on system list[k] (list == nullptr: system k).
-// NT threads per CTA: 512 (one CTA per SM, the widest team for each system) or
-// 128 (four CTAs per SM with the same 128 registers per thread: four systems
-// share an SM, for small pole orders where a system's work is too narrow for 512)
-template <int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) pbsam_forces_kernel_t(Ctx c, const int *list)
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c, const int *list)
 {
   extern __shared__ double2 dsm[];
-  __shared__ double red[NT];
+  __shared__ double red[PBSAM_TEAM];
   __shared__ CrewCmd cmd;
   const Team tm{(int)threadIdx.x, (int)blockDim.x};
   cg::cluster_group cl = cg::this_cluster();
@@ -2077,8 +2072,6 @@ __global__ void __launch_bounds__(NT, MINB) pbsam_forces_kernel_t(Ctx c, const i
   forces_body(tm, c, cw, b, dsm, red);
   crew_finish(tm, cw);
 }
-template __global__ void pbsam_forces_kernel_t<PBSAM_TEAM, 1>(Ctx, const int *);
-template __global__ void pbsam_forces_kernel_t<PBSAM_TEAM_SMALL, 4>(Ctx, const int *);
 
 // interaction energy on the state left by the last force evaluation.
 // lab == 0: the reference's convention (src/moldynamics.cpp:358-386,

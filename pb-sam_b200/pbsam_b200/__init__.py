@@ -35,8 +35,7 @@ class pbsam_params(ctypes.Structure):
                 ("solve_max_ct", ctypes.c_int), ("max_pol_rounds", ctypes.c_int),
                 ("inter_cutoff", ctypes.c_double), ("interact_cutoff", ctypes.c_double),
                 ("intra_cutoff", ctypes.c_double), ("min_sep_numeric", ctypes.c_double),
-                ("num_points_x", ctypes.c_int), ("cluster_size", ctypes.c_int),
-                ("team_threads", ctypes.c_int)]
+                ("num_points_x", ctypes.c_int), ("cluster_size", ctypes.c_int)]
 
 
 PBSAM_BD_NAM = 0

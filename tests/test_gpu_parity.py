@@ -26,13 +26,12 @@ def poses(case):
     return json.load(open(os.path.join(golden_dir(case), "poses.json")))
 
 
-def make_ctx(case, tight=False, cluster_size=0, team_threads=0):
+def make_ctx(case, tight=False, cluster_size=0):
     import pbsam_b200 as pb
     P = poses(case)
     tol = oracle.TIGHT_TOL if tight else oracle.DEFAULT_TOL
     ctx = pb.CSystem(poles=P["poles"], salt=P["salt"], idiel=P["idiel"], max_polar_dev=tol[0],
-                     solve_tol=tol[1], solve_max_ct=tol[2], max_pol_rounds=tol[3], cluster_size=cluster_size,
-                     team_threads=team_threads)
+                     solve_tol=tol[1], solve_max_ct=tol[2], max_pol_rounds=tol[3], cluster_size=cluster_size)
     d = golden_dir(case)
     ta = ctx.load_moltype(d + "/molA.pqr", d + "/imA", d + "/expA", "molA.0")
     tb = ctx.load_moltype(d + "/molB.pqr", d + "/imB", d + "/expB", "molB.0")
@@ -249,36 +248,3 @@ def test_cluster_sizes_agree():
             f1, t1 = results[1][call]
             for k in range(len(frames)):
                 assert rel(f[k], f1[k]) < 1e-12 and rel(t[k], t1[k]) < 1e-12, (size, call, k)
-
-
-@pytest.mark.parametrize("cluster_size", [1, 4])
-def test_narrow_teams_agree(cluster_size):
-    """128-thread CTAs (four systems per SM) change only the rounding: the first call
-    matches the reference to 1e-8 and three calls in a row agree with 512-thread
-    CTAs to 1e-12."""
-    P = poses("cfg0")
-    frames = [p["frame"] for p in P["poses"]]
-    pos, quat = frame_arrays(frames)
-    refs = [oracle.parse(os.path.join(golden_dir("cfg0"), "ref_default", "pose%d.txt" % k))[0]
-            for k in range(len(frames))]
-    runs = {}
-    for team in (512, 128):
-        ctx, types = make_ctx("cfg0", cluster_size=cluster_size, team_threads=team)
-        mol = ctx.molecules(types, n_systems=len(frames))
-        for call in range(3):
-            mol.set_poses(pos, quat)
-            f, t, st = mol.compute_forces()
-            assert np.all(st == 0)
-            runs.setdefault(team, []).append((f, t))
-        e = mol.compute_energy()
-        runs[team].append((e, e))
-        mol.close()
-        ctx.close()
-    for k in range(len(frames)):
-        f, t = runs[128][0][0][k], runs[128][0][1][k]
-        assert rel(f, refs[k]["force"]) < TOL and rel(t, refs[k]["torque"]) < TOL
-    for call in range(3):
-        for k in range(len(frames)):
-            assert rel(runs[128][call][0][k], runs[512][call][0][k]) < 1e-12
-            assert rel(runs[128][call][1][k], runs[512][call][1][k]) < 1e-12
-    assert np.allclose(runs[128][3][0], runs[512][3][0], rtol=1e-12, atol=0)
