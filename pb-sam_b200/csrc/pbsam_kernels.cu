@@ -1413,7 +1413,7 @@ __device__ __noinline__ void grad_xform_warp(const WarpTeam &tw, const Sys &y, c
 // round-robin to the CTA's warps, each transforming its pairs alone, and the
 // warps' sums are added in warp order; the other pairs are added one by one, each
 // transformed by the whole CTA.
-__device__ void dta_share(const Team &tm, const Sys &y, int s, bool self, int filter_mol, bool use_ipol, bool use_iact,
+__device__ __noinline__ void dta_share(const Team &tm, const Sys &y, int s, bool self, int filter_mol, bool use_ipol, bool use_iact,
                           int rank, int size, double *part)
 {
   const int NP2 = y.NP2, nw = tm.size >> 5, w = tm.rank >> 5;
