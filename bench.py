@@ -11,10 +11,17 @@ prepared on the GPU before timing, like the reference's `pbsam mat` and
 `pbsam spol` (5 self-polarization sweeps).  The IMats (120 x 6.5 MB) exceed L2,
 so no flush is needed.
 
+The same line carries a Brownian-dynamics leg ("bd", --bd 1): 1024 independent
+two-molecule bdnam trajectories at p = 10 (35 + 35 spheres), each step a force
+evaluation where the pair is inside the force distance plus the Ermak-McCammon
+move, one CUDA graph per step of the whole batch; BD steps/s with its own e2e,
+clocks and the reference's computeForces timed on the host cores.
+
 Multi-GPU: one process per GPU (torchrun), each rank solves its own batch of 26
-poses (weak scaling, no data-path collective); rank 0 prints the max-over-ranks
-device time.  --impl reference times the reference's own CPU implementation
-(oracle/_ref, compiled from the reference sources) on the same poses.
+poses and its own 1024 trajectories (weak scaling, no data-path collective); rank 0
+prints the max-over-ranks device time.  --impl reference times the reference's own
+CPU implementation (oracle/_ref, compiled from the reference sources) on the same
+poses.
 """
 import argparse
 import datetime

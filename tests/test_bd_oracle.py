@@ -21,8 +21,6 @@ def test_philox_matches_numpy():
     for ctr, key in (([1, 0, 0, 0], [0, 0]), ([5, 7, 9, 11], [123, 456]), ([2**64 - 1, 3, 0, 1], [2**63, 17])):
         g = np.random.Philox(counter=np.array([(ctr[0] - 1) % 2**64] + ctr[1:], dtype=np.uint64),
                              key=np.array(key, dtype=np.uint64))
-        if ctr[0] == 0:
-            continue
         assert [int(x) for x in g.random_raw(4)] == oracle.philox(ctr, key)
 
 
