@@ -152,6 +152,26 @@ def build_variant(poles, mode, jobs=8):
     subprocess.check_call(cxx + objs + [os.path.join(bindir, "selfp_makemat.o"), "-o",
                                         os.path.join(bindir, "pbsam")])
     subprocess.check_call(cxx + objs + [h, "-o", os.path.join(bindir, "harness")])
+    build_bd_harness(poles, mode)
+
+
+def build_bd_harness(poles, mode):
+    """The reference's own NAM driver (CBDnam, src/BDnam.cpp) with a fixed drand48
+    seed, linked from the staged sources and the objects of build_variant."""
+    src = os.path.join(OUT, "src_p%d_%s" % (poles, mode))
+    bindir = os.path.join(OUT, "p%d_%s" % (poles, mode))
+    if mode == "fast":
+        opt = ["-O3", "-ffast-math", "-funroll-loops", "-m64"]
+    else:
+        opt = ["-O2"]
+    cxx = ["g++", "-std=gnu++11", "-fopenmp", "-fpermissive", "-w",
+           "-D__MKL", "-D__OMP", "-D__ACCURATE__"] + opt + ["-I" + src]
+    objs = [os.path.join(bindir, f.replace(".cpp", ".o")) for f in LIB_SOURCES]
+    bdo = os.path.join(bindir, "BDnam.o")
+    subprocess.check_call(cxx + ["-c", os.path.join(src, "BDnam.cpp"), "-o", bdo])
+    ho = os.path.join(bindir, "ref_bd_harness.o")
+    subprocess.check_call(cxx + ["-c", os.path.join(HERE, "ref_bd_harness.cpp"), "-o", ho])
+    subprocess.check_call(cxx + objs + [bdo, ho, "-o", os.path.join(bindir, "bd_harness")])
     return bindir
 
 

@@ -57,7 +57,7 @@ BD_DEFAULT = dict(max_tries=500, force_dist=100.0, escape_dist=500.0, dt_min=2.0
 
 
 def write_bd_spec(path, moltypes, frame, mode, n_steps, seed, system, dtr, drot, salt=0.05, idiel=4.0, poles=10,
-                  tol=DEFAULT_TOL, **bdp):
+                  tol=DEFAULT_TOL, noise=None, **bdp):
     """Brownian dynamics from one frame's poses (the oracle's BD mode): n_steps steps of
     trajectory `system` (the noise counter's system word) with the given seed."""
     p = dict(BD_DEFAULT)
@@ -71,6 +71,8 @@ def write_bd_spec(path, moltypes, frame, mode, n_steps, seed, system, dtr, drot,
                                                   p["dt_max"], p["dt_ref"], p["dt_div"]))
         for a, b in zip(dtr, drot):
             fh.write("bddiff %r %r\n" % (a, b))
+        if noise is not None:       # (kind, order): kind 1 = the reference's drand48 stream
+            fh.write("bdnoise %d %d\n" % tuple(noise))
 
 
 def run_bd_spec(spec, out):
@@ -94,6 +96,13 @@ def run_bd_spec(spec, out):
         s["pos"] = np.array([s["pos"][i] for i in range(n)])
         s["quat"] = np.array([s["quat"][i] for i in range(n)])
     return steps
+
+
+def ref_bd_harness(poles=6, mode="default"):
+    """The reference's own NAM driver with a fixed drand48 seed (oracle/_ref, built by
+    build_ref.build_bd_harness), or None when it has not been built."""
+    p = os.path.join(HERE, "_ref", "p%d_%s" % (poles, mode), "bd_harness")
+    return p if os.path.exists(p) else None
 
 
 def philox(counter, key):

@@ -1813,7 +1813,39 @@ struct System {
     double time = 0;
     std::vector<double> dtr, drot;
     std::vector<Quat> rot;
+    // noise 0: Philox4x64-10 (the CUDA path's generator); noise 1: the reference's
+    // own stream, drand48 seeded by srand48(seed) with the polar Box-Muller method
+    // of normRand (src/util.h:489-539), the three deviates of a vector drawn in
+    // argument order `order` (0: x first, 1: z first)
+    int noise = 0, order = 0;
+    unsigned long long lcg = 0;
+    bool nr_saved = false;
+    double nr_value = 0.0;
   } bd;
+
+  // drand48 (POSIX): X <- (0x5DEECE66D X + 0xB) mod 2^48, returns X / 2^48
+  double drand()
+  {
+    bd.lcg = (0x5DEECE66DULL * bd.lcg + 0xBULL) & ((1ULL << 48) - 1);
+    return (double)bd.lcg / 281474976710656.0;
+  }
+  double norm_rand()   // normRand, src/util.h:515-539
+  {
+    if (!bd.nr_saved) {
+      double v1, v2, rsq;
+      do {
+        v1 = 2.0 * drand() - 1.0;
+        v2 = 2.0 * drand() - 1.0;
+        rsq = v1 * v1 + v2 * v2;
+      } while (rsq >= 1.0 || rsq == 0.0);
+      const double fac = sqrt(-2.0 * log(rsq) / rsq);
+      bd.nr_value = v1 * fac;
+      bd.nr_saved = true;
+      return fac * v2;
+    }
+    bd.nr_saved = false;
+    return bd.nr_value;
+  }
 
   static void philox(unsigned long long c[4], unsigned long long k0, unsigned long long k1)
   {
@@ -1830,6 +1862,12 @@ struct System {
   }
   P3 rand_vec(double sd)   // CBDnam::getRandVec (src/BDnam.h:44-45)
   {
+    if (bd.noise == 1) {
+      double a, b, c;
+      if (bd.order == 0) { a = norm_rand(); b = norm_rand(); c = norm_rand(); }
+      else { c = norm_rand(); b = norm_rand(); a = norm_rand(); }
+      return sd * P3(a, b, c);
+    }
     unsigned long long c[4] = {bd.ctr++, (unsigned long long)bd.sys, 0ULL, 0ULL};
     philox(c, bd.seed, 0ULL);
     double u[4];
@@ -2020,7 +2058,7 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
   std::vector<std::vector<std::string> > types;
   struct PoseL { int type; double v[7]; };
   std::vector<std::vector<PoseL> > frames;
-  int bdmode = -1, bdsteps = 0, bdsys = 0;
+  int bdmode = -1, bdsteps = 0, bdsys = 0, bdnoise = 0, bdorder = 0;
   unsigned long long bdseed = 0;
   double bdp[7] = {500, 100, 500, 2, 1e300, 5, 15};   // max_tries, force, escape, dt_min, dt_max, dt_ref, dt_div
   std::vector<double> bddtr, bddrot;
@@ -2038,6 +2076,7 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
     else if (tok == "bd") in >> bdmode >> bdsteps >> bdseed >> bdsys;
     else if (tok == "bdp") in >> bdp[0] >> bdp[1] >> bdp[2] >> bdp[3] >> bdp[4] >> bdp[5] >> bdp[6];
     else if (tok == "bddiff") { double a, b; in >> a >> b; bddtr.push_back(a); bddrot.push_back(b); }
+    else if (tok == "bdnoise") in >> bdnoise >> bdorder;
     else return 2;
   }
   System sys;
@@ -2061,6 +2100,8 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
     }
     System::BD &B = sys.bd;
     B.mode = bdmode; B.seed = bdseed; B.sys = bdsys;
+    B.noise = bdnoise; B.order = bdorder;
+    B.lcg = (((unsigned long long)bdseed & 0xFFFFFFFFULL) << 16) | 0x330EULL;   // srand48(seed)
     B.max_tries = (int)bdp[0]; B.force_dist = bdp[1]; B.escape_dist = bdp[2];
     B.dt_min = bdp[3]; B.dt_max = bdp[4]; B.dt_ref = bdp[5]; B.dt_div = bdp[6];
     B.dtr = bddtr; B.drot = bddrot;

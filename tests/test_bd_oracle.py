@@ -6,9 +6,16 @@
   N(0, 2 D dt) per component with the reference's time step 2 + (d - 5)/15 ps,
   and no force evaluation is made (src/BDnam.cpp:196-222, 409-417);
 * escape beyond q_DIST ends the trajectory (src/BDnam.cpp:288);
-* a trajectory whose every move is rejected is STUCK (src/BDnam.cpp:287).
+* a trajectory whose every move is rejected is STUCK (src/BDnam.cpp:287);
+* drawing the reference's own stream (drand48 from srand48(seed), polar
+  Box-Muller, the vector's deviates drawn z first as gcc evaluates
+  CPnt(normRand(), normRand(), normRand())), the oracle's steps equal the
+  reference's own CBDnam::makeMove loop (oracle/ref_bd_harness.cpp, one OpenMP
+  thread: the reference's threaded force path races) bit for bit, at close range
+  and across the force distance with stored rotations.
 """
 import os
+import subprocess
 
 import numpy as np
 import pytest
@@ -82,3 +89,66 @@ def test_same_seed_same_trajectory_other_system_differs(tmp_path, mode):
     assert not np.allclose(a[-1]["pos"], c[-1]["pos"])
     if mode == 0:
         assert np.array_equal(a[-1]["pos"][0], [0, 0, 0])   # NAM: molecule 0 never translates
+
+
+def _ref_steps(path):
+    steps = []
+    for ln in open(path):
+        t = ln.split()
+        if t[0] == "BDSTEP":
+            steps.append(dict(status=int(t[2]), fevals=int(t[3]), time=float(t[4]), pos={}, quat={}))
+        elif t[0] == "POSE":
+            v = [float(x) for x in t[2:]]
+            steps[-1]["pos"][int(t[1])] = v[:3]
+            steps[-1]["quat"][int(t[1])] = v[3:]
+    for st in steps:
+        st["pos"] = np.array([st["pos"][0], st["pos"][1]])
+        st["quat"] = np.array([st["quat"][0], st["quat"][1]])
+    return steps
+
+
+def _vs_reference(tmp_path, frame, n, seed):
+    exe = oracle.ref_bd_harness()
+    if exe is None:
+        pytest.skip("reference BD harness not built (oracle/build_ref.py)")
+    case = golden_dir("tiny")
+    spec = os.path.join(tmp_path, "ref.txt")
+    oracle.write_bd_spec(spec, oracle.golden_moltypes(case), frame, 0, n, seed, 0, (0.0, 0.03), (4.5e-5, 4e-5),
+                         salt=0.1, idiel=4.0, poles=6, noise=(1, 1))
+    out = os.path.join(tmp_path, "ref.out")
+    r = subprocess.run([exe, spec, out], env=dict(os.environ, OMP_NUM_THREADS="1"), capture_output=True)
+    mine = oracle.run_bd_spec(spec, os.path.join(tmp_path, "orc.out"))
+    return r.returncode, (_ref_steps(out) if r.returncode == 0 else []), mine
+
+
+def _gap5_frame():
+    import json
+    P = json.load(open(os.path.join(golden_dir("tiny"), "poses.json")))
+    return [(m["type"], m["pos"], m["quat"]) for m in P["poses"][1]["frame"]]
+
+
+def test_reference_stream_matches_reference_bdnam_close_range(tmp_path):
+    rc, ref, mine = _vs_reference(str(tmp_path), _gap5_frame(), 8, 12345)
+    assert rc == 0 and len(ref) == len(mine) == 8
+    for a, b in zip(mine, ref):
+        assert a["status"] == b["status"] and a["fevals"] == b["fevals"] and a["time"] == b["time"]
+        assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["quat"], b["quat"])
+    assert ref[-1]["fevals"] == 8
+
+
+def test_reference_stream_matches_reference_bdnam_across_force_distance(tmp_path):
+    fr = _gap5_frame()
+    axis = np.array(fr[1][1]) / np.linalg.norm(fr[1][1])
+    frame = [fr[0], (fr[1][0], list(100.4 * axis), fr[1][2])]
+    rc, ref, mine = _vs_reference(str(tmp_path), frame, 30, 777)
+    assert rc == 0 and len(ref) == len(mine) == 30
+    for a, b in zip(mine, ref):
+        assert a["status"] == b["status"] and a["fevals"] == b["fevals"]
+        assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["quat"], b["quat"])
+    assert 0 < ref[-1]["fevals"] < 30          # steps with and without forces, stored rotations applied
+
+
+def test_overlap_ends_the_trajectory_on_both_sides(tmp_path):
+    fr = _gap5_frame()
+    rc, ref, mine = _vs_reference(str(tmp_path), [fr[0], (fr[1][0], [0.3, 0.0, 0.0], fr[1][2])], 3, 5)
+    assert rc == 4 and mine[0]["status"] == 4     # bdnam exits; the oracle reports FAILED
