@@ -180,7 +180,14 @@ typedef struct pbsam_bd_params {
   double coul_k;         /* COUL_K = 2.30708e-18 */
   unsigned long long seed;
   int use_graph;         /* 1: a step is replayed as one CUDA graph */
+  int noise;             /* PBSAM_BD_NOISE_PHILOX (default) or PBSAM_BD_NOISE_DRAND48: the
+                            reference's own stream (drand48 seeded by srand48(seed + system), the
+                            polar Box-Muller of normRand, src/util.h:489-539), drawn sequentially per
+                            system, so that system b repeats the reference's bdnam run seeded with
+                            seed + b (src/BDnam_main.cpp:39-41 seeds from the clock instead) */
 } pbsam_bd_params;
+#define PBSAM_BD_NOISE_PHILOX 0
+#define PBSAM_BD_NOISE_DRAND48 1
 
 /* Reference values of the chosen driver (src/BDnam.h:10-25, src/BDmulti.cpp:13,
  * src/BDnam.cpp:409-417). */

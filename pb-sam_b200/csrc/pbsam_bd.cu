@@ -19,9 +19,10 @@
 // Noise: Philox4x64-10 (Salmon et al., "Parallel random numbers: as easy as
 // 1, 2, 3", SC 2011), key (seed, 0), counter (draw, system, 0, 0); one block of
 // four 64-bit words gives four uniforms in (0,1) and, by the Box-Muller
-// transform, the three normal deviates of one random vector.  The reference
-// draws from drand48 with the polar Box-Muller method (src/util.h:515-539):
-// the same distribution from a different stream.
+// transform, the three normal deviates of one random vector.  Or (noise 1) the
+// reference's own stream: drand48 with the polar Box-Muller method
+// (src/util.h:489-539), sequential per system, with which a trajectory repeats
+// the reference's bdnam run of the same seed.
 #pragma once
 #include "pbsam_types.cuh"
 
@@ -38,6 +39,7 @@ struct BDParams {
   double fact_tr, ikbt, coul_k;       // FACT2, IKbT, COUL_K (src/BDnam.h:10-20)
   double interact_cut;                // MULTI: interaction cutoff (force evaluation)
   unsigned long long seed;
+  int noise;                          // 0: Philox4x64-10; 1: the reference's drand48 stream
 };
 
 struct BDView {
@@ -49,6 +51,9 @@ struct BDView {
   double *cen;                        // [B][S][3] sphere centres rotated by the current orientation
   double *pos, *quat;                 // the system's poses (BatchView::pos/quat), written here
   const double *dtr, *drot;           // [nmol] translational / rotational diffusion coefficients
+  unsigned long long *lcg;            // [B] drand48 state (noise 1)
+  double *nr_val;                     // [B] the second deviate kept by the polar method (noise 1)
+  int *nr_saved;                      // [B]
 };
 
 // ---------------------------------------------------------------- Philox4x64-10
@@ -230,12 +235,51 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_kernel(Ctx c, B
   }
 }
 
-// one random vector of standard deviation sd added to base (thread 0 only)
+// The reference's own stream (noise 1), per system: drand48 (POSIX: X <- (0x5DEECE66D X
+// + 0xB) mod 2^48, value X / 2^48) seeded as srand48(seed + system), and the polar
+// Box-Muller method of normRand (src/util.h:515-539), which keeps its second deviate
+// for the next call.  The rejection loop is capped at 4096 draws (it ends after the
+// first with probability pi/4 each time).
+__device__ __forceinline__ double bd_drand48(unsigned long long &x)
+{
+  x = (0x5DEECE66DULL * x + 0xBULL) & ((1ULL << 48) - 1);
+  return (double)x / 281474976710656.0;
+}
+__device__ double bd_norm_rand(const BDView &v, int b)
+{
+  if (v.nr_saved[b]) {
+    v.nr_saved[b] = 0;
+    return v.nr_val[b];
+  }
+  unsigned long long x = v.lcg[b];
+  double v1 = 0.0, v2 = 0.0, rsq = 0.0;
+  for (int k = 0; k < 4096; k++) {
+    v1 = 2.0 * bd_drand48(x) - 1.0;
+    v2 = 2.0 * bd_drand48(x) - 1.0;
+    rsq = v1 * v1 + v2 * v2;
+    if (!(rsq >= 1.0 || rsq == 0.0)) break;
+  }
+  v.lcg[b] = x;
+  const double fac = sqrt(-2.0 * log(rsq) / rsq);
+  v.nr_val[b] = v1 * fac;
+  v.nr_saved[b] = 1;
+  return fac * v2;
+}
+
+// one random vector of standard deviation sd added to base (thread 0 only); with
+// the reference's stream the deviates are drawn z first, as gcc evaluates the
+// arguments of CPnt(normRand(), normRand(), normRand()) in CBDnam::getRandVec
 __device__ __forceinline__ void bd_kick(const BDParams &p, const BDView &v, int b, const double *base, double sd,
                                         double *o)
 {
   double z[3];
-  bd_normal3(p.seed, v.ctr[b]++, b, z);
+  if (p.noise == 1) {
+    z[2] = bd_norm_rand(v, b);
+    z[1] = bd_norm_rand(v, b);
+    z[0] = bd_norm_rand(v, b);
+  } else {
+    bd_normal3(p.seed, v.ctr[b]++, b, z);
+  }
   for (int a = 0; a < 3; a++) o[a] = base[a] + sd * z[a];
 }
 
@@ -385,7 +429,7 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_move_kernel(Ctx c, 
   }
 }
 
-__global__ void pbsam_bd_init_kernel(Ctx c, BDView v)
+__global__ void pbsam_bd_init_kernel(Ctx c, BDParams p, BDView v)
 {
   const BatchView &bv = c.bv;
   const int b = blockIdx.x;
@@ -393,6 +437,10 @@ __global__ void pbsam_bd_init_kernel(Ctx c, BDView v)
   if (threadIdx.x == 0) {
     v.status[b] = BD_RUNNING; v.steps[b] = 0; v.fevals[b] = 0;
     v.time[b] = 0.0; v.dt[b] = 0.0; v.ctr[b] = 0ULL; v.need[b] = 0;
+    // srand48(seed + b): high 32 bits of the state from the seed, low 16 bits 0x330E
+    v.lcg[b] = (((p.seed + (unsigned long long)b) & 0xFFFFFFFFULL) << 16) | 0x330EULL;
+    v.nr_saved[b] = 0;
+    v.nr_val[b] = 0.0;
   }
   for (int k = threadIdx.x; k < bv.nmol * 4; k += blockDim.x) v.rot[(size_t)b * bv.nmol * 4 + k] = (k % 4 == 0) ? 1.0 : 0.0;
 }

@@ -44,6 +44,7 @@ extern "C" void pbsam_bd_params_default(int mode, pbsam_bd_params *p)
   p->coul_k = 2.30708e-18;                  // COUL_K, src/BDnam.h:19
   p->seed = 0;
   p->use_graph = 1;
+  p->noise = PBSAM_BD_NOISE_PHILOX;
 }
 
 extern "C" int pbsam_system_bd_init(pbsam_system *s, const pbsam_bd_params *prm, const double *dtr, const double *drot)
@@ -70,6 +71,11 @@ extern "C" int pbsam_system_bd_init(pbsam_system *s, const pbsam_bd_params *prm,
   p.fact_tr = prm->fact_tr; p.ikbt = prm->ikbt; p.coul_k = prm->coul_k;
   p.interact_cut = s->ctx->prm.interact_cutoff;
   p.seed = prm->seed;
+  if (prm->noise != PBSAM_BD_NOISE_PHILOX && prm->noise != PBSAM_BD_NOISE_DRAND48) {
+    bd_free(s);
+    return fail(PBSAM_E_BADARG, "bad noise kind");
+  }
+  p.noise = prm->noise;
   h->use_graph = prm->use_graph;
   const size_t B = s->B, nm = s->nmol, S = s->c.bv.S;
   BDView &v = h->v;
@@ -77,6 +83,7 @@ extern "C" int pbsam_system_bd_init(pbsam_system *s, const pbsam_bd_params *prm,
   auto chk = [&](int rr) { if (rr && !r) r = rr; };
   chk(dalloc(h->bufs, &v.status, B)); chk(dalloc(h->bufs, &v.steps, B)); chk(dalloc(h->bufs, &v.fevals, B));
   chk(dalloc(h->bufs, &v.time, B)); chk(dalloc(h->bufs, &v.dt, B)); chk(dalloc(h->bufs, &v.ctr, B));
+  chk(dalloc(h->bufs, &v.lcg, B)); chk(dalloc(h->bufs, &v.nr_val, B)); chk(dalloc(h->bufs, &v.nr_saved, B));
   chk(dalloc(h->bufs, &v.rot, B * nm * 4)); chk(dalloc(h->bufs, &v.need, B)); chk(dalloc(h->bufs, &v.cen, B * S * 3));
   std::vector<double> hd(dtr, dtr + nm), hr(drot, drot + nm);
   chk(dput(h->bufs, &v.dtr, hd)); chk(dput(h->bufs, &v.drot, hr));
@@ -99,7 +106,7 @@ extern "C" int pbsam_system_bd_init(pbsam_system *s, const pbsam_bd_params *prm,
   // start after the work already queued on the system's stream (poses set by the caller)
   CK(cudaEventRecord(h->ev_in, s->stream));
   CK(cudaStreamWaitEvent(h->st, h->ev_in, 0));
-  pbsam_bd_init_kernel<<<s->B, 32, 0, h->st>>>(s->c, v);
+  pbsam_bd_init_kernel<<<s->B, 32, 0, h->st>>>(s->c, p, v);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->st));
   return PBSAM_OK;

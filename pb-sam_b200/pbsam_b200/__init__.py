@@ -40,6 +40,8 @@ class pbsam_params(ctypes.Structure):
 
 PBSAM_BD_NAM = 0
 PBSAM_BD_MULTI = 1
+PBSAM_BD_NOISE_PHILOX = 0
+PBSAM_BD_NOISE_DRAND48 = 1
 BD_STATUS = {0: "RUNNING", 1: "ESCAPED", 2: "STUCK", 3: "DOCKED", 4: "FAILED"}
 
 
@@ -48,7 +50,7 @@ class pbsam_bd_params(ctypes.Structure):
                 ("escape_dist", ctypes.c_double), ("dt_min", ctypes.c_double), ("dt_max", ctypes.c_double),
                 ("dt_ref", ctypes.c_double), ("dt_div", ctypes.c_double), ("fact_tr", ctypes.c_double),
                 ("ikbt", ctypes.c_double), ("coul_k", ctypes.c_double), ("seed", ctypes.c_ulonglong),
-                ("use_graph", ctypes.c_int)]
+                ("use_graph", ctypes.c_int), ("noise", ctypes.c_int)]
 
 
 # every entry point declared in include/pbsam_b200.h, with ctypes signatures

@@ -107,3 +107,53 @@ def test_escape_and_stuck_vs_oracle(tmp_path):
     stuck = [fr[0], (fr[1][0], [0.3, 0.0, 0.0], fr[1][2])]
     s2, ref2 = run_compare(tmp_path, [0, 1], stuck, 0, 2, 2, (0.0, 1e-8), DROT, max_tries=1, force_dist=0.0)
     assert ref2[0][0]["status"] == 2 and s2[-1]["status"][0] == 2
+
+
+def _ref_bd(tmp_path, frame, n, seed, P):
+    """The reference's own CBDnam steps (oracle/ref_bd_harness.cpp) from srand48(seed)."""
+    import subprocess
+    exe = oracle.ref_bd_harness()
+    if exe is None:
+        pytest.skip("reference BD harness not built")
+    spec = os.path.join(tmp_path, "r%d.txt" % seed)
+    oracle.write_bd_spec(spec, oracle.golden_moltypes(golden_dir("tiny")), frame, 0, n, seed, 0, DTR, DROT,
+                         salt=P["salt"], idiel=P["idiel"], poles=P["poles"])
+    out = spec + ".out"
+    subprocess.check_call([exe, spec, out], env=dict(os.environ, OMP_NUM_THREADS="1"),
+                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    steps = []
+    for ln in open(out):
+        t = ln.split()
+        if t[0] == "BDSTEP":
+            steps.append(dict(status=int(t[2]), fevals=int(t[3]), time=float(t[4]), steps=int(t[1]), pos=[], quat=[]))
+        elif t[0] == "POSE":
+            v = [float(x) for x in t[2:]]
+            steps[-1]["pos"].append(v[:3])
+            steps[-1]["quat"].append(v[3:])
+    return steps
+
+
+@pytest.mark.parametrize("far", [False, True])
+def test_reference_stream_vs_reference_bdnam(tmp_path, far):
+    """With the reference's own noise stream (drand48, polar Box-Muller) system b
+    repeats the reference's CBDnam run seeded with seed + b, step by step: at close
+    range with forces every step, and across the force distance with stored
+    rotations (CUDA's log and sqrt differ from the host's in the last bit)."""
+    import pbsam_b200 as pb
+    fr = gap5_frame()
+    if far:
+        axis = np.array(fr[1][1]) / np.linalg.norm(fr[1][1])
+        fr = [fr[0], (fr[1][0], list(100.4 * axis), fr[1][2])]
+    n, seed = (20, 777) if far else (8, 12345)
+    ctx, types, P = tiny_ctx()
+    mol = ctx.molecules(types, n_systems=2)
+    mol.set_poses(np.array([[m[1] for m in fr]] * 2), np.array([[m[2] for m in fr]] * 2))
+    mol.bd_init(DTR, DROT, mode=0, seed=seed, noise=pb.PBSAM_BD_NOISE_DRAND48)
+    refs = [_ref_bd(str(tmp_path), fr, n, seed + b, P) for b in range(2)]
+    for k in range(n):
+        mol.bd_run(1)
+        g = mol.bd_state()
+        for b in range(2):
+            check_step(g, b, dict(refs[b][k], pos=np.array(refs[b][k]["pos"]), quat=np.array(refs[b][k]["quat"])))
+    mol.close()
+    ctx.close()
