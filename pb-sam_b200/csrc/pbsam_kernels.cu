@@ -604,11 +604,22 @@ __device__ __noinline__ void numeric_expand2(const Team &tm, const Tab &T, const
   double *rb = ra + (size_t)TP * P;            // [TP][P]  radial factors, set B
   double *pg = rb + (size_t)TP * P;            // [TP][5]  cos t, sin t, phi, set A valid, set B valid
   double *pw = pg + 5 * TP;                    // [TP][6]  weights A, B
+  // With few harmonics (at least two team-sized copies of them fit the team) the
+  // team splits into G groups, group g adding the tile points g, g + G, ... into its
+  // own partial sums, which are added in group order at the end; otherwise every
+  // thread owns coefficients rank + j * size over all points.
+  const int nsets = useB ? 2 : 1;
+  int G = 1;
+  if (2 * P2 <= tm.size) {
+    G = tm.size / P2;
+    while (G > 1 && (size_t)(G + 1) * 2 * NC * NP2 * sizeof(double) > dyn_region_bytes(NP)) G--;
+  }
+  const int grp = (G > 1) ? tm.rank / P2 : 0;
   double accA[PBSAM_NUM_CPT][NC], accB[PBSAM_NUM_CPT][NC];
   int deg[PBSAM_NUM_CPT];
 #pragma unroll
   for (int j = 0; j < PBSAM_NUM_CPT; j++) {
-    const int c = tm.rank + j * tm.size;
+    const int c = (G > 1) ? ((j == 0 && grp < G) ? tm.rank % P2 : P2) : tm.rank + j * tm.size;
     int n = (int)sqrt((double)c);
     while (n * n > c) n--;
     while ((n + 1) * (n + 1) <= c) n++;
@@ -664,13 +675,13 @@ __device__ __noinline__ void numeric_expand2(const Team &tm, const Tab &T, const
       if (m2 != m1) sh_column(T, ct, st, ph, m2, P, put(m2));
     }
     tm.sync();
-    for (int t = 0; t < nt; t++) {
+    for (int t = grp; t < nt; t += G) {
       const bool okA = pg[5 * t + 3] != 0.0, okB = pg[5 * t + 4] != 0.0;
       if (!okA && !okB) continue;
       const double *yt = Yt + (size_t)t * P2;
 #pragma unroll
       for (int j = 0; j < PBSAM_NUM_CPT; j++) {
-        const int c = tm.rank + j * tm.size;
+        const int c = (G > 1) ? ((j == 0 && grp < G) ? tm.rank % P2 : P2) : tm.rank + j * tm.size;
         if (c < P2) {
           const double yv = yt[c];
           if (okA && c < PA2) {
@@ -693,6 +704,30 @@ __device__ __noinline__ void numeric_expand2(const Team &tm, const Tab &T, const
       }
     }
     tm.sync();
+  }
+  if (G > 1) {
+    // group partial sums staged after the first 2 * NC * NP2 doubles of the tile
+    // region (part may be the tile region itself), then added in group order
+    double *gp = sc.tile + (size_t)2 * NC * NP2;
+    if (grp < G) {
+      const int c = tm.rank % P2;
+#pragma unroll
+      for (int k = 0; k < NC; k++) {
+        gp[((size_t)(grp * 2) * NC + k) * P2 + c] = accA[0][k];
+        gp[((size_t)(grp * 2 + 1) * NC + k) * P2 + c] = accB[0][k];
+      }
+    }
+    tm.sync();
+    for (int u = tm.rank; u < nsets * NC * NP2; u += tm.size) {
+      const int set = u / (NC * NP2), k = (u / NP2) % NC, c = u % NP2;
+      double v = 0.0;
+      if (c < (set ? PB2 : PA2))
+        for (int g = 0; g < G; g++) v += gp[((size_t)(g * 2 + set) * NC + k) * P2 + c];
+      double *o = part ? part + (size_t)(set * NC + k) * NP2 : (set ? B.out : A.out) + (size_t)k * NP2;
+      o[c] = v;
+    }
+    tm.sync();
+    return;
   }
 #pragma unroll
   for (int j = 0; j < PBSAM_NUM_CPT; j++) {
