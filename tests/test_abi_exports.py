@@ -58,3 +58,19 @@ def test_context_without_gpu_fails_cleanly():
         pytest.skip("GPU present")
     with pytest.raises(pb.PbsamError):
         pb.CSystem(poles=6)
+
+
+def test_bd_defaults_match_reference_drivers():
+    """pbsam_bd_params_default gives the constants of the reference's drivers
+    (src/BDnam.h:10-25, src/BDnam.cpp:409-417, src/BDmulti.cpp:13, 451, 511-517);
+    no GPU needed."""
+    if not os.path.exists(pb.LIB_PATH):
+        pytest.skip("CUDA library not built")
+    nam = pb.bd_params(pb.PBSAM_BD_NAM)
+    multi = pb.bd_params(pb.PBSAM_BD_MULTI)
+    assert nam.max_tries == 500 and nam.force_dist == 100.0 and nam.escape_dist == 500.0
+    assert nam.dt_min == 2.0 and nam.dt_ref == 5.0 and nam.dt_div == 15.0 and nam.dt_max >= 1e300
+    assert multi.dt_ref == 10.0 and multi.dt_min == 2.0
+    assert nam.fact_tr == 5.604586e2 and nam.coul_k == 2.30708e-18
+    assert abs(nam.ikbt - 1.0 / (1.3806503e-23 * 298.15)) <= 1e-12 * nam.ikbt
+    assert nam.noise == pb.PBSAM_BD_NOISE_PHILOX and nam.use_graph == 1
