@@ -153,7 +153,9 @@ int pbsam_system_last_kernel_ms(const pbsam_system *sys, double *ms);
  *   PBSAM_BD_MULTI = CBDmulti::propagate / makeMove / compute_dt / computeMinSepDist
  *                    (src/BDmulti.cpp:396-566): every molecule moves in turn;
  *                    forces while the minimum separation is below the context's
- *                    interaction cutoff (no periodic box).
+ *                    interaction cutoff (no periodic box); the minimum separation
+ *                    is the smallest sphere gap over all molecule pairs, at least
+ *                    dt_ref, as the reference's bdm computes it.
  * Time step dt = min(dt_max, dt_min + max(0, d - dt_ref) / dt_div) ps, d the
  * molecule gap (NAM) or the minimum separation (MULTI); drifts D*dt*fact_tr*F and
  * Dr*dt*ikbt*coul_k*torque; noise N(0, 2*D*dt) per component from Philox4x64-10

@@ -172,6 +172,12 @@ def build_bd_harness(poles, mode):
     ho = os.path.join(bindir, "ref_bd_harness.o")
     subprocess.check_call(cxx + ["-c", os.path.join(HERE, "ref_bd_harness.cpp"), "-o", ho])
     subprocess.check_call(cxx + objs + [bdo, ho, "-o", os.path.join(bindir, "bd_harness")])
+    # the multi-molecule driver (CBDmulti, src/BDmulti.cpp)
+    bmo = os.path.join(bindir, "BDmulti.o")
+    subprocess.check_call(cxx + ["-c", os.path.join(src, "BDmulti.cpp"), "-o", bmo])
+    hmo = os.path.join(bindir, "ref_bdm_harness.o")
+    subprocess.check_call(cxx + ["-c", os.path.join(HERE, "ref_bdm_harness.cpp"), "-o", hmo])
+    subprocess.check_call(cxx + objs + [bmo, hmo, "-o", os.path.join(bindir, "bdm_harness")])
     return bindir
 
 

@@ -105,6 +105,12 @@ def ref_bd_harness(poles=6, mode="default"):
     return p if os.path.exists(p) else None
 
 
+def ref_bdm_harness(poles=6, mode="default"):
+    """The reference's own multi-molecule driver (CBDmulti) with a fixed drand48 seed."""
+    p = os.path.join(HERE, "_ref", "p%d_%s" % (poles, mode), "bdm_harness")
+    return p if os.path.exists(p) else None
+
+
 def philox(counter, key):
     """One Philox4x64-10 block of the oracle's noise generator."""
     lib = liboracle()

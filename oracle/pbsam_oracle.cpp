@@ -1964,8 +1964,11 @@ struct System {
       dt = bd_dt(mol_gap(0, 1));
       need = c2c(0, 1) < bd.force_dist;
     } else {
+      // as bdm runs it: CBDmulti::initConstants (src/BDmulti.cpp:26-38) runs before the
+      // molecules set CMolecule::m_interactRcutoff (still DBL_MAX, src/molecule.cpp:26),
+      // so every pair is tracked sphere by sphere, floored at DISTCUTOFF_TIME
       const double ic = prm.interact_cut;
-      const double maxd = bd.dt_ref > ic ? bd.dt_ref : ic, mind = bd.dt_ref > ic ? ic : bd.dt_ref;
+      const double maxd = 1e300, mind = bd.dt_ref;
       double smin = 1e300, mmin = 1e300;
       bool track = false;
       for (int i = 0; i < nmol; i++)

@@ -192,11 +192,13 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_kernel(Ctx c, B
     }
     return;
   }
-  // computeMinSepDist (src/BDmulti.cpp:527-566): sphere gaps of molecule pairs
-  // closer than max(dt_ref, interaction cutoff), floored at min(dt_ref, cutoff);
-  // else the smallest molecule gap (not below 0)
-  const double maxd = p.dt_ref > p.interact_cut ? p.dt_ref : p.interact_cut;
-  const double mind = p.dt_ref > p.interact_cut ? p.interact_cut : p.dt_ref;
+  // computeMinSepDist (src/BDmulti.cpp:527-566) as bdm runs it: CBDmulti::initConstants
+  // (src/BDmulti.cpp:26-38) sets its limits before the molecules exist
+  // (src/BDmulti_main.cpp:67-69), while CMolecule::m_interactRcutoff is still DBL_MAX
+  // (src/molecule.cpp:26), so every molecule pair is tracked sphere by sphere and the
+  // smallest gap is floored at DISTCUTOFF_TIME (dt_ref)
+  const double maxd = 1e300;
+  const double mind = p.dt_ref;
   const double *cen = v.cen + (size_t)b * bv.S * 3;
   double smin = 1e300, mmin = 1e300;
   int track = 0;

@@ -12,7 +12,9 @@
   CPnt(normRand(), normRand(), normRand())), the oracle's steps equal the
   reference's own CBDnam::makeMove loop (oracle/ref_bd_harness.cpp, one OpenMP
   thread: the reference's threaded force path races) bit for bit, at close range
-  and across the force distance with stored rotations.
+  and across the force distance with stored rotations; and the multi-molecule
+  steps equal the reference's own CBDmulti (oracle/ref_bdm_harness.cpp) with three
+  molecules, close together and all farther apart than the interaction cutoff.
 """
 import os
 import subprocess
@@ -91,7 +93,7 @@ def test_same_seed_same_trajectory_other_system_differs(tmp_path, mode):
         assert np.array_equal(a[-1]["pos"][0], [0, 0, 0])   # NAM: molecule 0 never translates
 
 
-def _ref_steps(path):
+def _ref_steps(path, n_mol=2):
     steps = []
     for ln in open(path):
         t = ln.split()
@@ -102,8 +104,8 @@ def _ref_steps(path):
             steps[-1]["pos"][int(t[1])] = v[:3]
             steps[-1]["quat"][int(t[1])] = v[3:]
     for st in steps:
-        st["pos"] = np.array([st["pos"][0], st["pos"][1]])
-        st["quat"] = np.array([st["quat"][0], st["quat"][1]])
+        st["pos"] = np.array([st["pos"][i] for i in range(n_mol)])
+        st["quat"] = np.array([st["quat"][i] for i in range(n_mol)])
     return steps
 
 
@@ -152,3 +154,31 @@ def test_overlap_ends_the_trajectory_on_both_sides(tmp_path):
     fr = _gap5_frame()
     rc, ref, mine = _vs_reference(str(tmp_path), [fr[0], (fr[1][0], [0.3, 0.0, 0.0], fr[1][2])], 3, 5)
     assert rc == 4 and mine[0]["status"] == 4     # bdnam exits; the oracle reports FAILED
+
+
+def _multi_frame(scale):
+    fr = _gap5_frame()
+    posb = np.array(fr[1][1]) * scale
+    return [(0, [0.0, 0.0, 0.0], fr[0][2]), (0, list(-posb), [0.5, 0.5, -0.5, 0.5]), (1, list(posb), fr[1][2])]
+
+
+@pytest.mark.parametrize("scale", [1.0, 9.0])
+def test_reference_stream_matches_reference_bdm(tmp_path, scale):
+    exe = oracle.ref_bdm_harness()
+    if exe is None:
+        pytest.skip("reference BD harness not built (oracle/build_ref.py)")
+    spec = os.path.join(str(tmp_path), "m.txt")
+    # the reference's bdm constants (src/BDmulti.cpp:204-205): D 0.015 for both species,
+    # Dr 4.5e-5 (species 0) and 4e-5 (species 1); species 0 copies first
+    oracle.write_bd_spec(spec, oracle.golden_moltypes(golden_dir("tiny")), _multi_frame(scale), 1, 6, 4242, 0,
+                         (0.015, 0.015, 0.015), (4.5e-5, 4.5e-5, 4e-5), salt=0.1, idiel=4.0, poles=6,
+                         noise=(1, 1))
+    out = os.path.join(str(tmp_path), "m.out")
+    subprocess.check_call([exe, spec, out], env=dict(os.environ, OMP_NUM_THREADS="1"))
+    ref = _ref_steps(out, 3)
+    mine = oracle.run_bd_spec(spec, os.path.join(str(tmp_path), "mo.out"))
+    assert len(ref) == len(mine) == 6
+    for a, b in zip(mine, ref):
+        assert a["fevals"] == b["fevals"] and a["time"] == b["time"]
+        assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["quat"], b["quat"])
+    assert (ref[-1]["fevals"] == 6) if scale == 1.0 else (ref[-1]["fevals"] == 0)

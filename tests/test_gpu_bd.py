@@ -157,3 +157,44 @@ def test_reference_stream_vs_reference_bdnam(tmp_path, far):
             check_step(g, b, dict(refs[b][k], pos=np.array(refs[b][k]["pos"]), quat=np.array(refs[b][k]["quat"])))
     mol.close()
     ctx.close()
+
+
+@pytest.mark.parametrize("scale", [1.0, 9.0])
+def test_reference_stream_vs_reference_bdm(tmp_path, scale):
+    """Multi-molecule steps with the reference's noise stream against the reference's
+    own CBDmulti (three molecules; close together, and all beyond the interaction
+    cutoff, where the time step follows the smallest sphere gap)."""
+    import subprocess
+    import pbsam_b200 as pb
+    exe = oracle.ref_bdm_harness()
+    if exe is None:
+        pytest.skip("reference BD harness not built")
+    fr = gap5_frame()
+    posb = np.array(fr[1][1]) * scale
+    frame = [(0, [0.0, 0.0, 0.0], fr[0][2]), (0, list(-posb), [0.5, 0.5, -0.5, 0.5]), (1, list(posb), fr[1][2])]
+    ctx, types, P = tiny_ctx()
+    dtr, drot = (0.015, 0.015, 0.015), (4.5e-5, 4.5e-5, 4e-5)
+    spec = os.path.join(str(tmp_path), "m.txt")
+    oracle.write_bd_spec(spec, oracle.golden_moltypes(golden_dir("tiny")), frame, 1, 6, 4242, 0, dtr, drot,
+                         salt=P["salt"], idiel=P["idiel"], poles=P["poles"], noise=(1, 1))
+    out = spec + ".out"
+    subprocess.check_call([exe, spec, out], env=dict(os.environ, OMP_NUM_THREADS="1"),
+                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    ref = []
+    for ln in open(out):
+        t = ln.split()
+        if t[0] == "BDSTEP":
+            ref.append(dict(status=0, steps=int(t[1]), fevals=int(t[3]), time=float(t[4]), pos=[], quat=[]))
+        elif t[0] == "POSE":
+            v = [float(x) for x in t[2:]]
+            ref[-1]["pos"].append(v[:3])
+            ref[-1]["quat"].append(v[3:])
+    mol = ctx.molecules([types[m[0]] for m in frame], n_systems=1)
+    mol.set_poses(np.array([[m[1] for m in frame]]), np.array([[m[2] for m in frame]]))
+    mol.bd_init(dtr, drot, mode=pb.PBSAM_BD_MULTI, seed=4242, noise=pb.PBSAM_BD_NOISE_DRAND48)
+    for k in range(6):
+        mol.bd_run(1)
+        g = mol.bd_state()
+        check_step(g, 0, dict(ref[k], pos=np.array(ref[k]["pos"]), quat=np.array(ref[k]["quat"])))
+    mol.close()
+    ctx.close()
