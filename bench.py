@@ -337,6 +337,42 @@ def run_bd(args, local, rank, world, dist):
     return out
 
 
+def reference_bd_step_seconds(cfg, files, pos, quat, limit_s, workdir, steps=3, variant="fast", seed=1):
+    """The reference's own bdnam step (CBDnam: computeForces while the pair is inside
+    f_DIST, then makeMove; oracle/ref_bd_harness.cpp) from each given pose, one
+    single-threaded process per pose, run concurrently; returns the wall seconds per
+    step of the steps after the first (the first builds the solver state that a
+    running trajectory carries), one value per pose that finished."""
+    exe = os.path.join(REPO, "oracle", "_ref", "p%d_%s" % (cfg["poles"], variant), "bd_harness")
+    if not os.path.exists(exe):
+        return None
+    procs = []
+    for j in range(len(pos)):
+        spec = os.path.join(workdir, "bdref%d.txt" % j)
+        _pose_spec(spec, cfg, files, pos[j], quat[j])
+        with open(spec, "a") as fh:
+            fh.write("bd 0 %d %d 0\n" % (steps, seed + j))
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        procs.append((spec, subprocess.Popen([exe, spec, spec + ".out"], env=env, stdout=subprocess.DEVNULL,
+                                             stderr=subprocess.DEVNULL)))
+    t0 = time.time()
+    out = []
+    for spec, p in procs:
+        try:
+            p.wait(timeout=max(1.0, limit_s - (time.time() - t0)))
+        except subprocess.TimeoutExpired:
+            p.kill()
+            p.wait()
+            continue
+        if p.returncode != 0:
+            continue
+        for ln in open(spec + ".out"):
+            t = ln.split()
+            if t and t[0] == "TIME" and int(t[2]) > 0:
+                out.append(float(t[1]) / int(t[2]))
+    return out
+
+
 def bd_cpu_baseline(cfg, specs, sysb, state, force_frac, args):
     """The reference's computeForces (p = 10 build) on consecutive poses of sampled
     trajectories: for each, the harness evaluates the pose before the last step
@@ -351,6 +387,15 @@ def bd_cpu_baseline(cfg, specs, sysb, state, force_frac, args):
     ncores = os.cpu_count() or 1
     run = [b for b in range(len(state["status"])) if state["status"][b] == 0]
     sel = run[:: max(1, len(run) // ncores)][:ncores]
+    with tempfile.TemporaryDirectory() as td:
+        files = workload.write_inputs(cfg, specs, td)
+        per_step = reference_bd_step_seconds(cfg, files, state["pos"][sel], state["quat"][sel], args.cpu_limit, td)
+    if per_step:
+        t = float(np.mean(per_step))
+        return {"value": ncores / t, "unit": "BD steps/s", "cores": ncores, "kind": "reference",
+                "sample": "the reference's own bdnam steps (CBDnam: computeForces + makeMove, `fast` build) from "
+                          "the poses of %d trajectories at the end of the timed run, 1 thread per process, all "
+                          "concurrently; steps 2-3 of each timed (mean %.3f s per step)" % (len(per_step), t)}
     sysb.bd_run(1)
     after = sysb.bd_state()
     times = []

@@ -18,6 +18,7 @@
 //       frame / mol <type> <x> <y> <z> <qw> <qx> <qy> <qz> (two molecules)
 //       bd <mode (0)> <n steps> <seed> <unused>
 // output: BDSTEP <steps> <status> <force evaluations> <time>, then POSE lines,
+// and TIME <wall seconds of the steps after the first> <their count> at the end;
 // statuses numbered 0 running, 1 escaped, 2 stuck, 3 docked; exit status 4 when
 // computeForces reports overlapping spheres (where bdnam exits).
 #include <cmath>
@@ -90,7 +91,10 @@ int main(int argc, char **argv)
   int fevals = 0;
   double time = 0.0;
   const int map_status[4] = {1, 3, 0, 2};       // ESCAPED, DOCKED, RUNNING, STUCK
-  for (int k = 0; k < nsteps && status == CBDnam::RUNNING; k++) {
+  double t_start = 0.0;                         // wall time of the steps after the first
+  int n_done = 0;
+  for (int k = 0; k < nsteps && status == CBDnam::RUNNING; k++, n_done++) {
+    if (k == 1) t_start = read_timer();
     // CBDnam::compute_dt is an inline member of BDnam.cpp, not linkable: its body
     // (src/BDnam.cpp:409-417) on the same members
     const REAL dsep = CMolecule::getSepDist(bd.m_mols[0], bd.m_mols[1]);
@@ -115,6 +119,7 @@ int main(int argc, char **argv)
               q.imag().x(), q.imag().y(), q.imag().z());
     }
   }
+  if (n_done > 1) fprintf(out, "TIME %.6e %d\n", read_timer() - t_start, n_done - 1);
   fclose(out);
   return 0;
 }
