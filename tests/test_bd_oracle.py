@@ -182,3 +182,25 @@ def test_reference_stream_matches_reference_bdm(tmp_path, scale):
         assert a["fevals"] == b["fevals"] and a["time"] == b["time"]
         assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["quat"], b["quat"])
     assert (ref[-1]["fevals"] == 6) if scale == 1.0 else (ref[-1]["fevals"] == 0)
+
+
+def test_reference_stream_matches_reference_bdnam_p10(tmp_path):
+    """The same at pole order 10 on the 8-sphere molecules (reference `default` build
+    at N_POLES 10), 4 A gap, forces every step."""
+    import json
+    exe = oracle.ref_bd_harness(10, "default")
+    if exe is None:
+        pytest.skip("reference BD harness not built (oracle/build_ref.py)")
+    d = golden_dir("cfg0")
+    P = json.load(open(os.path.join(d, "poses.json")))
+    frame = [(m["type"], m["pos"], m["quat"]) for m in P["poses"][2]["frame"]]
+    spec = os.path.join(str(tmp_path), "c.txt")
+    oracle.write_bd_spec(spec, oracle.golden_moltypes(d), frame, 0, 5, 99, 0, (0.0, 0.03), (4.5e-5, 4e-5),
+                         salt=P["salt"], idiel=P["idiel"], poles=P["poles"], noise=(1, 1))
+    out = os.path.join(str(tmp_path), "c.out")
+    subprocess.check_call([exe, spec, out], env=dict(os.environ, OMP_NUM_THREADS="1"), stdout=subprocess.DEVNULL)
+    ref = _ref_steps(out)
+    mine = oracle.run_bd_spec(spec, os.path.join(str(tmp_path), "co.out"))
+    assert len(ref) == len(mine) == 5 and ref[-1]["fevals"] == 5
+    for a, b in zip(mine, ref):
+        assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["quat"], b["quat"])
