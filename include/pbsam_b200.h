@@ -33,6 +33,12 @@ extern "C" {
 #define PBSAM_SYS_OK 0
 #define PBSAM_SYS_OVERLAP 1   /* two spheres of different molecules overlap
                                  (computeForces returns false, src/molecule.cpp:1090-1097) */
+#define PBSAM_SYS_NOT_CONVERGED 2   /* a polarization or gradient sweep loop stopped at
+                                       max_pol_rounds ("Polarization does not converge",
+                                       src/molecule.cpp:1963-1967); forces are returned */
+#define PBSAM_SYS_NAN 3       /* a non-finite pose (coordinate, or a zero quaternion) was
+                                 refused, or the evaluation produced a non-finite force or
+                                 torque (CExpan::isBlownup, src/expansion.h:216-221) */
 
 typedef struct pbsam_params {
   int poles;              /* pole order p (the reference's N_POLES, src/expansion.h:5-9) */
@@ -51,9 +57,11 @@ typedef struct pbsam_params {
   int num_points_x;       /* NUM_POINTS_X cap on surface points, src/molecule.cpp:64 (10000) */
   int cluster_size;       /* CTAs (one thread-block cluster) working on each system: 0 = the largest
                              of 16, 8, 4, 2 that keeps a whole batch resident at once; 1..16 forces it;
-                             -1 = adaptive: after each evaluation the systems are regrouped by its
-                             inner-iteration counts, costlier systems getting larger clusters (the
-                             rounding of the results may then differ between calls by ~1e-15).
+                             -1 = adaptive: before each evaluation the systems are regrouped by the
+                             inner-iteration counts of the previous one, costlier systems getting
+                             larger clusters (the rounding of the results may then differ between
+                             calls by ~1e-15); the call then waits for the previous evaluation's
+                             counters, so consecutive calls of one system do not overlap on the host.
                              No reference counterpart (a B200 launch parameter). */
 } pbsam_params;
 
@@ -120,8 +128,8 @@ int pbsam_system_compute_energy_lab(pbsam_system *sys, double *energy, int on_de
 
 /* Counters of the last force evaluation, 8 ints per system: [0] sweeps,
  * [1] inner F/H iterations, [2] inner solves, [3] gradient solves,
- * [4] 1 if the polarization sweeps hit max_pol_rounds, [5] CTAs that worked on
- * the system. */
+ * [4] bit 0: the polarization sweeps hit max_pol_rounds, bit 1: a gradient phase
+ * hit it, [5] CTAs that worked on the system. */
 int pbsam_system_stats(const pbsam_system *sys, int *stats);
 
 /* CUDA stream the system's work is queued on (cudaStream_t as void*); the

@@ -31,7 +31,10 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = os.environ.get("PBSAM_REFERENCE_SRC", "/root/reference/src")
+# the reference source tree: PBSAM_REFERENCE_SRC, else a checkout named "reference"
+# beside the repository
+REF_SRC = os.environ.get("PBSAM_REFERENCE_SRC",
+                         os.path.normpath(os.path.join(HERE, "..", "..", "reference", "src")))
 OUT = os.path.join(HERE, "_ref")
 
 # reference translation units needed by the pbsam driver and by the force harness

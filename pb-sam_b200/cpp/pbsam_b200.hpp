@@ -163,6 +163,8 @@ class CMolecule {
   }
 
   // CMolecule::computeForces: false when two molecules overlap (src/molecule.cpp:1090-1097)
+  // or the evaluation is not finite; a sweep loop that stopped at its cap returns true
+  // with the forces, as the reference does after printing its warning
   static bool computeForces(std::vector<CMolecule *> &mols, std::vector<CPnt> &force, std::vector<CPnt> &torque)
   {
     pbsam_system *s = system_of(mols);
@@ -173,7 +175,7 @@ class CMolecule {
     if (!CSystem::check(pbsam_system_compute_forces(s, f.data(), t.data(), &status, 0))) return false;
     force.assign(n, CPnt());
     torque.assign(n, CPnt());
-    if (status != PBSAM_SYS_OK) return false;
+    if (status != PBSAM_SYS_OK && status != PBSAM_SYS_NOT_CONVERGED) return false;
     for (size_t i = 0; i < n; i++) {
       force[i] = CPnt(f[3 * i], f[3 * i + 1], f[3 * i + 2]);
       torque[i] = CPnt(t[3 * i], t[3 * i + 1], t[3 * i + 2]);

@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <mutex>
 #include <string>
 #include <algorithm>
 #include <utility>
@@ -381,8 +382,23 @@ static int add_type(pbsam_context *c, HostType &&t0, const std::vector<double> &
   c->types.push_back(std::move(t));
   return (int)c->types.size() - 1;
 }
+static bool all_finite(const std::vector<double> &v)
+{
+  for (double x : v)
+    if (!std::isfinite(x)) return false;
+  return true;
+}
+
 static int add_type_checked(pbsam_context *c, HostType &&t, const std::vector<double> &cen_abs, int *type_id)
 {
+  // a non-finite input would only surface as NaN forces much later
+  if (!all_finite(cen_abs) || !all_finite(t.rad) || !all_finite(t.chg_pos) || !all_finite(t.chg))
+    return fail(PBSAM_E_BADARG, "non-finite sphere centre, radius or charge");
+  for (double r : t.rad)
+    if (!(r > 0.0)) return fail(PBSAM_E_BADARG, "sphere radius must be positive");
+  if (!all_finite(t.imat)) return fail(PBSAM_E_BADARG, "non-finite IMat entry");
+  if (!all_finite(t.fself) || !all_finite(t.hself) || !all_finite(t.hscale))
+    return fail(PBSAM_E_BADARG, "non-finite self-polarized expansion");
   const int r = add_type(c, std::move(t), cen_abs);
   if (r < 0) return r;
   *type_id = r;
@@ -804,8 +820,11 @@ extern "C" int pbsam_system_compute_forces(pbsam_system *s, double *force, doubl
   if (!s) return fail(PBSAM_E_BADARG, "null system");
   CK(cudaSetDevice(s->ctx->device));
   const size_t smem = team_smem_bytes(s->ctx->prm.poles);
-  if (s->adaptive && s->stats_pending && cudaEventQuery(s->ev_stats) == cudaSuccess) {
-    // regroup from the last evaluation's costs
+  if (s->adaptive && s->stats_pending) {
+    // regroup from the last evaluation's costs, every call: wait for the counters of
+    // the previous evaluation, so that the plan depends on the counts alone and not
+    // on how far the GPU has got when the host asks
+    CK(cudaEventSynchronize(s->ev_stats));
     s->stats_pending = false;
     std::vector<int> its(s->B);
     for (int b = 0; b < s->B; b++) its[b] = s->h_stats[8 * b + 1];

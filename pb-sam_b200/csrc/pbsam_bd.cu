@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_move_kernel(Ctx c, 
   if (b >= bv.B || v.status[b] != BD_RUNNING) return;
   const double dt = v.dt[b];
   const bool need = v.need[b] != 0;
-  if (need && bv.status[b] != PBSAM_STATUS_OK) {   // the reference exits here (src/BDnam.cpp:210-212)
+  if (need && bv.status[b] != PBSAM_STATUS_OK && bv.status[b] != PBSAM_STATUS_NOT_CONVERGED) {   // the reference exits here (src/BDnam.cpp:210-212)
     if (threadIdx.x == 0) { v.status[b] = BD_FAILED; v.fevals[b]++; }
     return;
   }

@@ -1819,6 +1819,23 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
     bv.force[(size_t)b * nmol * 3 + t] = 0.0;
     bv.torque[(size_t)b * nmol * 3 + t] = 0.0;
   }
+  // a pose with a non-finite coordinate or a zero quaternion is refused before any
+  // pair test (NaN distances would silently drop every pair)
+  {
+    int bad = 0;
+    for (int t = tm.rank; t < nmol * 7; t += tm.size) {
+      const double v = t < nmol * 3 ? bv.pos[(size_t)b * nmol * 3 + t] : bv.quat[(size_t)b * nmol * 4 + (t - nmol * 3)];
+      if (!isfinite(v)) bad = 1;
+    }
+    for (int i = tm.rank; i < nmol; i += tm.size) {
+      const double *q = bv.quat + 4 * ((size_t)b * nmol + i);
+      if (!(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3] > 0.0)) bad = 1;
+    }
+    if (__syncthreads_or(bad)) {
+      if (tm.rank == 0) bv.status[b] = PBSAM_STATUS_NAN;
+      return;
+    }
+  }
   // sphere centres for this pose (CMolecule::rotate / rotateCenters)
   for (int s = tm.rank; s < S; s += tm.size) {
     const double *q = bv.quat + 4 * ((size_t)b * nmol + y.mol(s));
@@ -1973,7 +1990,7 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
   }
   if (tm.rank == 0) {
     st[0] = ct;
-    if (dev * itot > tol2) st[4] = 1;   // polarization hit the sweep cap
+    if (dev * itot > tol2) st[4] |= 1;   // polarization hit the sweep cap
   }
   // ---- gradient phase (src/molecule.cpp:2081-2228)
   for (int j = 0; j < nmol; j++) {
@@ -2030,6 +2047,7 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
       k++;
       if (k == jsize) { k = 0; gct++; }
     }
+    if (tm.rank == 0 && dv * itj > tol2) st[4] |= 2;   // a gradient phase hit the sweep cap
     for (int h = 0; h < na; h++) {
       const int s = intra[h];
       tcopy(tm, y.gH(s), y.gw(bv.gHw, bv.gkey[y.sc1(s)]), 3 * NP2);
@@ -2082,6 +2100,19 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
     qrot(qn, Tq, bv.torque + ((size_t)b * nmol + i) * 3);
   }
   tm.sync();
+  // per-system outcome: a non-finite force or torque (a blown-up expansion,
+  // CExpan::isBlownup, src/expansion.h:216-221) or a sweep cap that was hit ("Polarization
+  // does not converge", src/molecule.cpp:1963-1967; the forces are still returned)
+  {
+    int bad = 0;
+    for (int t = tm.rank; t < nmol * 3; t += tm.size)
+      if (!isfinite(bv.force[(size_t)b * nmol * 3 + t]) || !isfinite(bv.torque[(size_t)b * nmol * 3 + t])) bad = 1;
+    bad = __syncthreads_or(bad);
+    if (tm.rank == 0) {
+      if (bad) bv.status[b] = PBSAM_STATUS_NAN;
+      else if (st[4]) bv.status[b] = PBSAM_STATUS_NOT_CONVERGED;
+    }
+  }
   fclk.stop(tm, PH_FORCE);
   total.stop(tm, PH_TOTAL);
 }
@@ -2133,7 +2164,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c, int lab
   const Tab &T = c.T;
   const int NP2 = y.NP2;
   double pot = 0.0;
-  if (bv.status[b] == PBSAM_STATUS_OK) {
+  if (bv.status[b] == PBSAM_STATUS_OK || bv.status[b] == PBSAM_STATUS_NOT_CONVERGED) {
     if (lab) {
       // lab-frame centres and H of every sphere
       for (int i = 0; i < bv.nmol; i++) {

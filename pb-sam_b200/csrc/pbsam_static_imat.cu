@@ -35,13 +35,19 @@ namespace pbsam {
 // 3.2 MB per device that loads the library, held until the process exits
 static __device__ __align__(256) double g_static_imat_scratch[PBSAM_STATIC_IMAT_DOUBLES];
 
-// device address of the array, looked up once per device (host code cannot use
-// the symbol's name as a device pointer)
+// device address of the array, looked up on the first call on each device with
+// that device current (host code cannot use the symbol's name as a device pointer)
+// and kept for the life of the process; the lookup is guarded so that host threads
+// making their first calls at once do not race on the cache.  A cudaDeviceReset of a
+// device invalidates the kept address together with every other handle of this
+// library on that device.
 static double *g_static_imat_ptr[64];
+static std::mutex g_static_imat_mu;
 
 static int static_imat_scratch(int device, double **out)
 {
   if (device < 0 || device >= 64) return fail(PBSAM_E_BADARG, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_static_imat_mu);
   if (!g_static_imat_ptr[device]) {
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_static_imat_scratch);

@@ -26,6 +26,8 @@ LIB_PATH = os.path.join(PKG, "lib", "libpbsam_b200.so")
 
 PBSAM_SYS_OK = 0
 PBSAM_SYS_OVERLAP = 1
+PBSAM_SYS_NOT_CONVERGED = 2
+PBSAM_SYS_NAN = 3
 
 
 class pbsam_params(ctypes.Structure):
@@ -104,13 +106,17 @@ def lib():
 
 
 class PbsamError(RuntimeError):
-    pass
+    """A call returned a PBSAM_E_* status; ``code`` holds it."""
+
+    def __init__(self, msg, code=0):
+        super().__init__(msg)
+        self.code = code
 
 
 def _check(rc):
     if rc != 0:
         msg = lib().pbsam_last_error()
-        raise PbsamError("pbsam error %d: %s" % (rc, msg.decode() if msg else ""))
+        raise PbsamError("pbsam error %d: %s" % (rc, msg.decode() if msg else ""), rc)
 
 
 def default_params(**kw):

@@ -60,6 +60,28 @@ def test_static_imat_matches_allocating_builder_twice():
         ctx.close()
 
 
+def test_static_imat_at_its_maximum_order():
+    """p = 16 fills the fixed array's Gram and IMat buffers exactly; two calls in a
+    row still agree with the allocating builder."""
+    import pbsam_b200 as pb
+    from pbsam_b200 import synth
+    cen, rad, _, _ = synth.read_pqr(os.path.join(golden_dir("cfg0"), "molA.pqr"))
+    cen = np.ascontiguousarray(cen[:4], dtype=np.float64)
+    rad = np.ascontiguousarray(rad[:4], dtype=np.float64)
+    ctx = pb.CSystem(poles=16, salt=0.05)
+    try:
+        n_points = 30000
+        ref = ctx.build_imats(cen, rad, n_points=n_points)
+        assert ref.shape == (4, 16 ** 4)
+        for call in range(2):
+            out = np.full(ref.shape, np.nan)
+            assert _call_static(ctx, cen, rad, n_points, out) == 0, pb.lib().pbsam_last_error()
+            assert np.all(np.isfinite(out)), "call %d" % call
+            assert rel(out, ref) < TOL, "call %d: %.3e" % (call, rel(out, ref))
+    finally:
+        ctx.close()
+
+
 def test_static_imat_rejects_orders_beyond_its_buffer():
     import pbsam_b200 as pb
     ctx = pb.CSystem(poles=20, salt=0.05)
