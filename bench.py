@@ -242,7 +242,7 @@ def run_ours(args):
             "prep_s": round(prep_s, 1), "prep": prep_t,
         }
         if args.cpu_baseline:
-            out["cpu_baseline"] = cpu_baseline(cfg, specs, pos, quat, stats, args)
+            out["cpu_baseline"] = cpu_baseline(cfg, specs, pos, quat, args)
     sysb.close()
     ctx.close()
     if args.bd:
@@ -455,126 +455,143 @@ def _pose_spec(path, cfg, files, pos, quat):
                                          " ".join("%.17g" % v for v in quat[m])))
 
 
-def _sample_poses(its, ncores, max_its):
-    """Poses of the bounded CPU sample: up to ncores poses whose inner-iteration
-    count is at most max_its, spread over that range (one process per core)."""
-    order = [int(i) for i in np.argsort(its, kind="stable") if its[i] <= max_its]
-    if len(order) <= ncores:
-        return order
-    pick = np.linspace(0, len(order) - 1, ncores).round().astype(int)
-    return sorted(set(order[k] for k in pick))
-
-
-def run_reference_sample(cfg, files, pos, quat, idx, limit_s, workdir):
-    """Runs the reference harness on poses idx concurrently (one single-threaded
-    process per pose); returns {pose: computeForces seconds (the harness' timer)}."""
+def reference_inputs_cpu(cfg, selfpol_rounds, outdir):
+    """The sweep's inputs made on the host cores, without the CUDA library: IMats
+    (250 000 quadrature points) and self-polarized F/H from the multi-threaded oracle
+    preparation (oracle/pbsam_prep.cpp, pinned to the reference's own `pbsam mat` /
+    `pbsam spol` files), written in the reference's formats.  Returns the file specs
+    and the seconds each part took."""
     import oracle
+    from pbsam_b200 import workload
+    mols = workload.molecules(cfg)
+    specs, tm = [], {}
+    for k, m in enumerate(mols):
+        cen, rad, pos, q = workload._pqr_round(m)
+        t0 = time.time()
+        im = oracle.prep_imats(cfg["poles"], cen, rad)
+        tm["imat_s_%d" % k] = round(time.time() - t0, 1)
+        t0 = time.time()
+        F, H, sc, rounds = oracle.prep_selfpol(cfg["poles"], cen, rad, pos, q, im, salt=cfg["salt"],
+                                               idiel=cfg["idiel"], max_rounds=selfpol_rounds)
+        tm["selfpol_s_%d" % k] = round(time.time() - t0, 1)
+        tm["selfpol_sweeps_%d" % k] = rounds
+        specs.append(dict(centres=cen, radii=rad, chg_pos=pos, chg=q, imats=im, fself=F, hself=H, hself_scale=sc))
+    return workload.write_inputs(cfg, specs, outdir), tm
+
+
+def reference_throughput(cfg, files, pos, quat, steps, warmup, workdir, variant="fast", limit_s=3000, seed=17):
+    """The reference's own computeForces on the sweep's poses, on every host core.
+
+    One single-threaded process of the reference harness (oracle/_ref/p<P>_<variant>,
+    the reference compiled from its sources; its OpenMP path races, so one thread per
+    process) per core.  Each process builds the molecules once and then evaluates its
+    own list of poses in order: `warmup` evaluations of the farthest pose (untimed),
+    then `steps` poses, process c taking pose order[(s * C + c) mod n] at step s, where
+    order is a seeded permutation of the n sweep poses (every pose recurs equally
+    often over the steps).  The harness times each computeForces call; a process's
+    busy time is the sum over its timed poses, and the rate is C * steps / (the
+    largest busy time): the poses solved per second by all cores together, measured
+    without a model."""
+    import oracle
+    exe = os.path.join(REPO, "oracle", "_ref", "p%d_%s" % (cfg["poles"], variant), "harness")
+    if not os.path.exists(exe):
+        return None
+    ncores = os.cpu_count() or 1
+    n = len(pos)
+    order = np.random.default_rng(seed).permutation(n)
+    far = int(np.argmax(np.linalg.norm(pos[:, 1] - pos[:, 0], axis=1)))
     procs = []
-    for j in idx:
-        spec = os.path.join(workdir, "pose%d.txt" % j)
-        _pose_spec(spec, cfg, files, pos[j], quat[j])
+    for c in range(ncores):
+        spec = os.path.join(workdir, "ref_core%d.txt" % c)
+        seq = [far] * warmup + [int(order[(s * ncores + c) % n]) for s in range(steps)]
+        with open(spec, "w") as fh:
+            fh.write("salt %r\nidiel %r\ndump 0\nenergy 0\n" % (cfg["salt"], cfg["idiel"]))
+            for fl in files:
+                fh.write("moltype %s %s %s %s\n" % fl)
+            for j in seq:
+                fh.write("frame\n")
+                for m in range(pos.shape[1]):
+                    fh.write("mol %d %s %s\n" % (m, " ".join("%.17g" % v for v in pos[j, m]),
+                                                 " ".join("%.17g" % v for v in quat[j, m])))
         env = dict(os.environ, OMP_NUM_THREADS="1")
-        procs.append((j, spec, subprocess.Popen([_ref_harness(cfg["poles"]), spec, spec + ".out"], env=env,
-                                                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)))
+        procs.append((c, seq, spec, subprocess.Popen([exe, spec, spec + ".out"], env=env, stdout=subprocess.DEVNULL,
+                                                     stderr=subprocess.DEVNULL)))
     t0 = time.time()
-    out = {}
-    for j, spec, p in procs:
+    busy, solved, failed = [], 0, 0
+    for c, seq, spec, p in procs:
         try:
             p.wait(timeout=max(1.0, limit_s - (time.time() - t0)))
         except subprocess.TimeoutExpired:
             p.kill()
             p.wait()
+        fr = oracle.parse(spec + ".out") if os.path.exists(spec + ".out") else []
+        timed = fr[warmup:]
+        if p.returncode != 0 or len(timed) != steps or not all(f["ok"] for f in timed):
+            failed += 1
             continue
-        if p.returncode == 0:
-            fr = oracle.parse(spec + ".out")
-            if fr and fr[0]["ok"]:
-                out[j] = float(fr[0]["info"][0])
-    return out
+        busy.append(sum(float(f["info"][0]) for f in timed))
+        solved += steps
+    wall = time.time() - t0
+    if failed or not busy:
+        return {"value": None, "failed_processes": failed}
+    T = max(busy)
+    return {"value": ncores * steps / T, "ms_per_step": 1e3 * T / steps, "cores": ncores, "solved": solved,
+            "busy_s_max": round(T, 2), "busy_s_mean": round(float(np.mean(busy)), 2), "wall_s": round(wall, 1),
+            "sample": "%d single-threaded processes of the reference harness (p=%d `%s` build), each evaluating "
+                      "%d poses of the %d-pose sweep (a seeded permutation taken round-robin over the cores: "
+                      "%d solves, every pose about %.1f times) after %d untimed evaluation(s) of the farthest "
+                      "pose; rate = cores x poses per process / the largest summed computeForces time" % (
+                          ncores, cfg["poles"], variant, steps, n, solved, solved / n, warmup)}
 
 
-def reference_rate(times, its, n_cores):
-    """Whole-job rate of the reference on n_cores for all poses, from the sample:
-    per-pose time modelled as a + b * inner iterations (least squares over the
-    sample; the counts are the GPU solve's, which follows the same iteration), the
-    single-threaded solves packed on the cores: T = max(sum t / cores, max t)."""
-    js = sorted(times)
-    x = np.array([its[j] for j in js], dtype=float)
-    y = np.array([times[j] for j in js])
-    if len(js) >= 2 and np.ptp(x) > 0:
-        b, a = np.polyfit(x, y, 1)
-        a = max(a, 0.0)
-    else:
-        a, b = 0.0, float(np.sum(y) / max(np.sum(x), 1.0))
-    t_all = a + b * np.asarray(its, dtype=float)
-    T = max(float(np.sum(t_all)) / n_cores, float(np.max(t_all)))
-    return len(its) / T, dict(a_s=round(float(a), 4), b_ms_per_inner_iteration=round(float(b) * 1e3, 4),
-                              est_total_cpu_s=round(float(np.sum(t_all)), 1), est_makespan_s=round(T, 1))
-
-
-def cpu_baseline(cfg, specs, pos, quat, stats, args):
+def cpu_baseline(cfg, specs, pos, quat, args):
+    """The reference's computeForces on one pose per host core (the bounded sample of
+    the timed region), on the inputs the GPU prepared."""
     from pbsam_b200 import workload
-    if not os.path.exists(_ref_harness(cfg["poles"])):
-        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "reference binary not built"}
-    ncores = os.cpu_count() or 1
-    its = stats[:, 1]
     with tempfile.TemporaryDirectory() as td:
         files = workload.write_inputs(cfg, specs, td)
-        idx = _sample_poses(its, ncores, args.cpu_sample_its)
-        times = run_reference_sample(cfg, files, pos, quat, idx, args.cpu_limit, td)
-    if not times:
-        return {"value": None, "unit": UNIT, "cores": ncores, "kind": "reference", "sample": "no pose finished"}
-    rate, model = reference_rate(times, its, ncores)
-    return {"value": rate, "unit": UNIT, "cores": ncores, "kind": "reference",
-            "sample": "%d poses (inner iterations %s) run concurrently, 1 thread each, computeForces timed by the "
-                      "reference harness (max %.1f s); whole sweep extrapolated per inner iteration" % (
-                          len(times), sorted(int(its[j]) for j in times), max(times.values())),
-            "model": model}
+        r = reference_throughput(cfg, files, pos, quat, 1, 0, td)
+    if r is None:
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "reference binary not built"}
+    if r["value"] is None:
+        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                "sample": "a reference process failed"}
+    return {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "reference", "sample": r["sample"],
+            "busy_s_max": r["busy_s_max"]}
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU implementation of the path, with
+    inputs made on the host cores and no CUDA library loaded."""
     from pbsam_b200 import replicas, workload
     rank, world, local = replicas.rank_env()
     if rank != 0:
         return None
     cfg = dict(workload.SWEEP_P30)
-    if not os.path.exists(_ref_harness(cfg["poles"])):
+    exe = os.path.join(REPO, "oracle", "_ref", "p%d_fast" % cfg["poles"], "harness")
+    if not os.path.exists(exe):
         return {"impl": "reference", "unavailable": "reference binary oracle/_ref/p30_fast/harness not built"}
-    import torch
-    torch.cuda.set_device(local)
-    # inputs and the per-pose iteration counts come from the GPU preparation; the
-    # timed work is the reference's own computeForces on the host cores
-    specs, _, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds)
-    ctx, types = workload.open_context(cfg, specs, device=local)
     mols = workload.molecules(cfg)
     pos, quat, _ = workload.poses(cfg, mols)
-    sysb = ctx.molecules(types, n_systems=len(pos))
-    sysb.set_poses(pos, quat)
-    sysb.compute_forces()
-    stats = sysb.stats()
-    sysb.close()
-    ctx.close()
-    ncores = os.cpu_count() or 1
-    its = stats[:, 1]
-    vals, samples = [], []
     with tempfile.TemporaryDirectory() as td:
-        files = workload.write_inputs(cfg, specs, td)
-        idx = _sample_poses(its, ncores, args.cpu_sample_its)
-        for s in range(args.warmup + args.steps):
-            times = run_reference_sample(cfg, files, pos, quat, idx, args.cpu_limit, td)
-            if s >= args.warmup and times:
-                v, model = reference_rate(times, its, ncores)
-                vals.append(v)
-                samples.append(model)
-    if not vals:
-        return {"impl": "reference", "unavailable": "no reference pose finished within %d s" % args.cpu_limit}
-    v = float(np.mean(vals))
+        t0 = time.time()
+        files, prep = reference_inputs_cpu(cfg, args.selfpol_rounds, td)
+        prep_s = time.time() - t0
+        r = reference_throughput(cfg, files, pos, quat, args.steps, args.warmup, td)
+    if r is None or r["value"] is None:
+        return {"impl": "reference", "unavailable": "a reference process failed or did not finish"}
+    v = r["value"]
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * len(pos) / v, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": WORKLOAD},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores, "kind": "reference",
-                             "sample": "%d poses per step run concurrently, 1 thread each; whole sweep extrapolated "
-                                       "per inner iteration" % len(idx), "model": samples[-1]},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator; IMats and self-polarized "
+                                                       "expansions made on the host cores)",
+            "config": {"workload": WORKLOAD, "poles": cfg["poles"],
+                       "step": "one pose per host core (the sweep's poses round-robin over the cores)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                             "sample": r["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "busy_s_max": r["busy_s_max"], "busy_s_mean": r["busy_s_mean"], "timed_wall_s": r["wall_s"],
+            "prep_s": round(prep_s, 1), "prep": prep}
 
 
 def main():
@@ -587,8 +604,6 @@ def main():
     # the sweeps stop contracting after a few rounds, so the inputs are taken after 5
     ap.add_argument("--selfpol-rounds", type=int, default=5)
     ap.add_argument("--cpu-baseline", type=int, default=1)
-    ap.add_argument("--cpu-sample-its", type=int, default=6000,
-                    help="largest inner-iteration count of a pose in the CPU sample")
     ap.add_argument("--cpu-limit", type=int, default=60, help="seconds before a sample pose is abandoned")
     ap.add_argument("--cluster-size", type=int, default=-1,
                     help="CTAs per system (0: automatic, -1: adaptive from the previous step's costs)")

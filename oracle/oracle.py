@@ -28,6 +28,67 @@ def build(force=False):
     return LIB
 
 
+PREP_LIB = os.path.join(HERE, "libpbsam_prep.so")
+_prep = None
+
+
+def build_prep(force=False):
+    """Compile the multi-threaded preparation library (oracle/pbsam_prep.cpp: the
+    oracle plus OpenMP IMat builder and self-polarization; no GPU needed)."""
+    srcs = [os.path.join(HERE, f) for f in ("pbsam_prep.cpp", "pbsam_oracle.cpp")]
+    if force or not os.path.exists(PREP_LIB) or any(os.path.getmtime(PREP_LIB) < os.path.getmtime(f) for f in srcs):
+        subprocess.check_call(["g++", "-std=c++17", "-O3", "-mavx2", "-mfma", "-fopenmp", "-fPIC", "-shared", "-o", PREP_LIB,
+                               srcs[0]])
+    return PREP_LIB
+
+
+def libprep():
+    global _prep
+    if _prep is None:
+        build_prep()
+        _prep = ctypes.CDLL(PREP_LIB)
+        d = ctypes.POINTER(ctypes.c_double)
+        _prep.pbsam_prep_imat.argtypes = [ctypes.c_int, ctypes.c_int, d, d, ctypes.c_int, d]
+        _prep.pbsam_prep_imat.restype = ctypes.c_int
+        _prep.pbsam_prep_selfpol.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, d, d,
+                                             ctypes.c_int, d, d, d, ctypes.c_int, d, d, d,
+                                             ctypes.POINTER(ctypes.c_int)]
+        _prep.pbsam_prep_selfpol.restype = ctypes.c_int
+    return _prep
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def prep_imats(poles, centres, radii, n_points=250000):
+    """IMats of a molecule's spheres on the host cores ([n_sph, p^4], column-major as
+    imat.sp<k>.out.bin holds them): the reference's `pbsam mat`."""
+    cen = np.ascontiguousarray(centres, dtype=np.float64)
+    rad = np.ascontiguousarray(radii, dtype=np.float64)
+    out = np.zeros((len(rad), poles ** 4))
+    if libprep().pbsam_prep_imat(poles, len(rad), _dp(cen), _dp(rad), n_points, _dp(out)) != 0:
+        raise RuntimeError("pbsam_prep_imat failed")
+    return out
+
+
+def prep_selfpol(poles, centres, radii, chg_pos, chg, imats, salt=0.05, idiel=4.0, max_rounds=1700):
+    """Self-polarized (F, H, H scale, sweeps) on the host cores, rounded as the
+    reference's .exp files: the reference's `pbsam spol`."""
+    cen = np.ascontiguousarray(centres, dtype=np.float64)
+    rad = np.ascontiguousarray(radii, dtype=np.float64)
+    qp = np.ascontiguousarray(chg_pos, dtype=np.float64).reshape(-1, 3)
+    q = np.ascontiguousarray(chg, dtype=np.float64)
+    im = np.ascontiguousarray(imats, dtype=np.float64)
+    n, P2 = len(rad), poles * poles
+    F, H, sc = np.zeros((n, P2)), np.zeros((n, P2)), np.zeros(n)
+    r = ctypes.c_int()
+    if libprep().pbsam_prep_selfpol(poles, salt, idiel, n, _dp(cen), _dp(rad), len(q), _dp(qp), _dp(q), _dp(im),
+                                    max_rounds, _dp(F), _dp(H), _dp(sc), ctypes.byref(r)) != 0:
+        raise RuntimeError("pbsam_prep_selfpol failed")
+    return F, H, sc, r.value
+
+
 def liboracle():
     global _lib
     if _lib is None:

@@ -936,6 +936,10 @@ static bool read_exp(const char *fname, int NP, vec &V, double &scale)
 }
 
 // moltype precompute (src/molecule.cpp:501-696, 756-810, src/expcenter.cpp:469-552, 1042-1060)
+static void init_moltype(const Tables &T, const Params &prm, MolType &mt, const std::vector<P3> &pos,
+                         const std::vector<double> &ch, const std::vector<double> &rad, const std::vector<P3> &cen,
+                         bool self_terms = true);
+
 static bool build_moltype(const Tables &T, const Params &prm, MolType &mt, const char *pqr,
                           const char *imatdir, const char *expdir, const char *expname)
 {
@@ -946,6 +950,31 @@ static bool build_moltype(const Tables &T, const Params &prm, MolType &mt, const
   const int ns = cen.size();
   mt.ns = ns;
   mt.sph.assign(ns, SphType());
+  char fn[1024];
+  for (int k = 0; k < ns; k++) {
+    SphType &S = mt.sph[k];
+    snprintf(fn, sizeof fn, "%s/imat.sp%d.out.bin", imatdir, k);
+    if (!read_imat(fn, NP, S.imat)) return false;
+    double sc;
+    snprintf(fn, sizeof fn, "%s/%s.%d.F.exp", expdir, expname, k);
+    if (!read_exp(fn, NP, S.Fself, sc)) return false;
+    snprintf(fn, sizeof fn, "%s/%s.%d.H.exp", expdir, expname, k);
+    if (!read_exp(fn, NP, S.Hself, S.hself_scale)) return false;
+  }
+  init_moltype(T, prm, mt, pos, ch, rad, cen);
+  return true;
+}
+
+// the rest of the moltype precompute, from absolute charge positions and sphere
+// centres, with each sphere's IMat and self expansions already in mt.sph;
+// self_terms = false skips what depends on the self expansions (surface charges and
+// intra local expansions of the self values), for a type about to be self-polarized
+static void init_moltype(const Tables &T, const Params &prm, MolType &mt, const std::vector<P3> &pos,
+                         const std::vector<double> &ch, const std::vector<double> &rad, const std::vector<P3> &cen,
+                         bool self_terms)
+{
+  const int NP = T.NP;
+  const int ns = cen.size();
   P3 rc;
   for (int i = 0; i < ns; i++) rc = rc + cen[i];
   rc = (1.0 / ns) * rc;
@@ -955,18 +984,7 @@ static bool build_moltype(const Tables &T, const Params &prm, MolType &mt, const
   for (size_t i = 0; i < pos.size(); i++) posr[i] = pos[i] - rc;
   mt.maxR = 0;
   for (int i = 0; i < ns; i++) { double d = cr[i].norm() + rad[i]; if (d > mt.maxR) mt.maxR = d; }
-  char fn[1024];
-  for (int k = 0; k < ns; k++) {
-    SphType &S = mt.sph[k];
-    S.cen = cr[k]; S.rad = rad[k];
-    snprintf(fn, sizeof fn, "%s/imat.sp%d.out.bin", imatdir, k);
-    if (!read_imat(fn, NP, S.imat)) return false;
-    double sc;
-    snprintf(fn, sizeof fn, "%s/%s.%d.F.exp", expdir, expname, k);
-    if (!read_exp(fn, NP, S.Fself, sc)) return false;
-    snprintf(fn, sizeof fn, "%s/%s.%d.H.exp", expdir, expname, k);
-    if (!read_exp(fn, NP, S.Hself, S.hself_scale)) return false;
-  }
+  for (int k = 0; k < ns; k++) { mt.sph[k].cen = cr[k]; mt.sph[k].rad = rad[k]; }
   // exposed surface points (generateMolSPX / getXFormSpherePoints)
   for (int k = 0; k < ns; k++) {
     SphType &S = mt.sph[k];
@@ -1023,7 +1041,7 @@ static bool build_moltype(const Tables &T, const Params &prm, MolType &mt, const
     }
   }
   // self surface charges (generateMolExposedChargesFH)
-  for (int k = 0; k < ns; k++) {
+  for (int k = 0; k < ns && self_terms; k++) {
     SphType &S = mt.sph[k];
     const double dA = 4.0 * M_PI / double(S.nspx);
     std::vector<double> bI(NP + 1, 1.0);
@@ -1053,7 +1071,7 @@ static bool build_moltype(const Tables &T, const Params &prm, MolType &mt, const
       else { far[ki].push_back(kj); far[kj].push_back(ki); }
     }
   // moltype self local expansions (computeMolTypeValues)
-  for (int ki = 0; ki < ns; ki++) {
+  for (int ki = 0; ki < ns && self_terms; ki++) {
     SphType &Si = mt.sph[ki];
     Si.LFfar.assign(NP * NP, 0); Si.LHfar.assign(NP * NP, 0);
     for (size_t t = 0; t < far[ki].size(); t++) {
@@ -1112,7 +1130,6 @@ static bool build_moltype(const Tables &T, const Params &prm, MolType &mt, const
       }
     }
   }
-  return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -1216,12 +1233,30 @@ struct System {
         }
     oldH = H; outerOldH = H;
     auto matmul = [&](const vec &X, vec &Y) {      // applyMMat: Y = IMat * X (column-major)
+#ifdef PBSAM_PREP
+      // the same sums, row blocks across threads, columns streamed in order
+      for (int d = 0; d < D; d++) {
+#pragma omp parallel for schedule(static)
+        for (int i0 = 0; i0 < p2; i0 += 64) {
+          const int i1 = i0 + 64 < p2 ? i0 + 64 : p2;
+          double acc[64];
+          for (int i = i0; i < i1; i++) acc[i - i0] = 0.0;
+          for (int kk = 0; kk < p2; kk++) {
+            const double x = X[d * p2 + kk];
+            const double *a = S.imat.data() + (size_t)kk * p2;
+            for (int i = i0; i < i1; i++) acc[i - i0] += a[i] * x;
+          }
+          for (int i = i0; i < i1; i++) Y[d * p2 + i] = acc[i - i0];
+        }
+      }
+#else
       for (int d = 0; d < D; d++)
         for (int i = 0; i < p2; i++) {
           double s = 0.0;
           for (int kk = 0; kk < p2; kk++) s += S.imat[(size_t)kk * p2 + i] * X[d * p2 + kk];
           Y[d * p2 + i] = s;
         }
+#endif
     };
     auto iterate = [&]() {
       for (int d = 0, k = 0; d < D; d++)
@@ -1410,26 +1445,41 @@ struct System {
     const SphType &Si = st(i, ki);
     Z.LFS.assign(NP * NP, 0.0);
     Z.LHS = Z.LS;
-    for (int kj : Si.near) {
-      const SphType &Sj = st(i, kj);
-      const SphState &Zj = mols[i].s[kj];
-      P3 P = Si.cen - Sj.cen;
-      double rho = P.norm(), sep = rho - Si.rad - Sj.rad;
+    const int nn = Si.near.size();
+#ifdef PBSAM_PREP
+    // neighbours' terms computed across threads, added in list order
+    std::vector<vec> ta(nn), tb(nn);
+#pragma omp parallel for schedule(dynamic)
+    for (int t = 0; t < nn; t++) intra_near_term(i, ki, Si.near[t], ta[t], tb[t]);
+    for (int t = 0; t < nn; t++) { add_into(Z.LFS, ta[t]); add_into(Z.LHS, tb[t]); }
+#else
+    for (int t = 0; t < nn; t++) {
       vec a, b;
-      if (sep > 0 && !(sep < 5)) {
-        int pF = compute_order(NP, rho, Zj.tF, Sj.rad), pH = compute_order(NP, rho, Zj.tH, Sj.rad);
-        XForm X; X.reset_intra(T, P, pH, pF, Sj.rad, Si.rad);
-        X.xformF(Zj.F, a); X.xformH(Zj.H, b);
-      } else {
-        int pF = compute_order(NP, rho, Zj.tF, Sj.rad), pH = compute_order(NP, rho, Zj.tH, Sj.rad);
-        a.assign(pF * pF, 0.0); b.assign(pH * pH, 0.0);
-        for (size_t h = 0; h < Sj.spx.size(); h++) {
-          P3 d = Sj.spx[h] - P;
-          if (Zj.qF[h] != 0.0) add_local_charge(T, a, Zj.qF[h], d, false, pF, Si.rad);
-          if (Zj.qH[h] != 0.0) add_local_charge(T, b, Zj.qH[h], d, true, pH, Si.rad);
-        }
-      }
+      intra_near_term(i, ki, Si.near[t], a, b);
       add_into(Z.LFS, a); add_into(Z.LHS, b);
+    }
+#endif
+  }
+  // one near neighbour kj's F (a) and H (b) re-expanded into sphere ki
+  void intra_near_term(int i, int ki, int kj, vec &a, vec &b) const
+  {
+    const SphType &Si = st(i, ki);
+    const SphType &Sj = st(i, kj);
+    const SphState &Zj = mols[i].s[kj];
+    P3 P = Si.cen - Sj.cen;
+    double rho = P.norm(), sep = rho - Si.rad - Sj.rad;
+    if (sep > 0 && !(sep < 5)) {
+      int pF = compute_order(NP, rho, Zj.tF, Sj.rad), pH = compute_order(NP, rho, Zj.tH, Sj.rad);
+      XForm X; X.reset_intra(T, P, pH, pF, Sj.rad, Si.rad);
+      X.xformF(Zj.F, a); X.xformH(Zj.H, b);
+    } else {
+      int pF = compute_order(NP, rho, Zj.tF, Sj.rad), pH = compute_order(NP, rho, Zj.tH, Sj.rad);
+      a.assign(pF * pF, 0.0); b.assign(pH * pH, 0.0);
+      for (size_t h = 0; h < Sj.spx.size(); h++) {
+        P3 d = Sj.spx[h] - P;
+        if (Zj.qF[h] != 0.0) add_local_charge(T, a, Zj.qF[h], d, false, pF, Si.rad);
+        if (Zj.qH[h] != 0.0) add_local_charge(T, b, Zj.qH[h], d, true, pH, Si.rad);
+      }
     }
   }
   double solve_surface(int i, int ki, const vec &Finit, const vec &Hinit, bool rotH)   // src/expcenter.cpp:608-629
