@@ -1277,12 +1277,64 @@ struct System {
       oldH = H;
       return dv;
     };
+    if (exact_inner) {
+      // the fixed point of the iteration solved directly (Gaussian elimination with
+      // partial pivoting): F = C3 M (fb + cH1 H + cF1 F), H = CI M (hb + cH2 H + cF2 F)
+      const int n2 = 2 * p2;
+      std::vector<int> deg(p2);
+      for (int n = 0; n < p; n++) for (int k = n * n; k < (n + 1) * (n + 1); k++) deg[k] = n;
+      std::vector<double> A((size_t)n2 * n2, 0.0);
+      for (int i = 0; i < p2; i++) {
+        const double c3 = T.CONST3[deg[i]], ci = S.cInvH[deg[i]];
+        for (int kk = 0; kk < p2; kk++) {
+          const double m = S.imat[(size_t)kk * p2 + i];
+          A[(size_t)i * n2 + kk] -= c3 * m * S.cF1[deg[kk]];
+          A[(size_t)i * n2 + p2 + kk] -= c3 * m * S.cH1[deg[kk]];
+          A[(size_t)(p2 + i) * n2 + kk] -= ci * m * S.cF2[deg[kk]];
+          A[(size_t)(p2 + i) * n2 + p2 + kk] -= ci * m * S.cH2[deg[kk]];
+        }
+        A[(size_t)i * n2 + i] += 1.0;
+        A[(size_t)(p2 + i) * n2 + p2 + i] += 1.0;
+      }
+      for (int d = 0; d < D; d++) {
+        std::vector<double> B = A, y(n2, 0.0);
+        for (int i = 0; i < p2; i++) {
+          double sf = 0.0, sh = 0.0;
+          for (int kk = 0; kk < p2; kk++) {
+            sf += S.imat[(size_t)kk * p2 + i] * fbase[d * p2 + kk];
+            sh += S.imat[(size_t)kk * p2 + i] * hbase[d * p2 + kk];
+          }
+          y[i] = T.CONST3[deg[i]] * sf;
+          y[p2 + i] = S.cInvH[deg[i]] * sh;
+        }
+        for (int c = 0; c < n2; c++) {
+          int piv = c;
+          for (int r = c + 1; r < n2; r++) if (fabs(B[(size_t)r * n2 + c]) > fabs(B[(size_t)piv * n2 + c])) piv = r;
+          if (piv != c) { for (int k = 0; k < n2; k++) std::swap(B[(size_t)c * n2 + k], B[(size_t)piv * n2 + k]); std::swap(y[c], y[piv]); }
+          for (int r = c + 1; r < n2; r++) {
+            const double f = B[(size_t)r * n2 + c] / B[(size_t)c * n2 + c];
+            if (f == 0.0) continue;
+            for (int k = c; k < n2; k++) B[(size_t)r * n2 + k] -= f * B[(size_t)c * n2 + k];
+            y[r] -= f * y[c];
+          }
+        }
+        for (int c = n2 - 1; c >= 0; c--) {
+          double sum = y[c];
+          for (int k = c + 1; k < n2; k++) sum -= B[(size_t)c * n2 + k] * y[k];
+          y[c] = sum / B[(size_t)c * n2 + c];
+        }
+        for (int i = 0; i < p2; i++) { F[d * p2 + i] = y[i]; H[d * p2 + i] = y[p2 + i]; }
+      }
+      n_inner += 1; n_solves++;
+      return compute_dev2(outerOldH.data(), H.data(), p, D);
+    }
     double dev = iterate();
     int ct = 1;
     while (dev > prm.solve_tol && ct < prm.solve_max_ct) { dev = iterate(); ct++; }
     n_inner += ct; n_solves++;
     return compute_dev2(outerOldH.data(), H.data(), p, D);
   }
+  bool exact_inner = false;   // solve each sphere's F/H fixed point directly
   mutable long n_inner = 0, n_solves = 0;
 
   // exposed surface charges (src/expcenter.cpp:1419-1440)
@@ -1686,7 +1738,9 @@ struct System {
           for (size_t ki = 0; ki < mols[i].s.size(); ki++) {
             if (mols[i].s[ki].interPol.empty()) continue;
             double d = mols[i].s[ki].dev;
-            if (d > 0.1 * MAXDEV) d = recompute(i, ki);
+            // the exact form sweeps every sphere until the fixed point: the selective
+            // update can leave a sphere whose last change was small out of date
+            if (exact_inner || d > 0.1 * MAXDEV) d = recompute(i, ki);
             if (maxdevs[i] < d) maxdevs[i] = d;
             dmol += d;
           }
@@ -1697,6 +1751,7 @@ struct System {
       ct++;
     }
     n_sweeps = ct;
+    if (skip_grad) return;
     // gradient phase
     for (int j = 0; j < nmol; j++) {
       Molecule &Mj = mols[j];
@@ -1738,6 +1793,7 @@ struct System {
     }
   }
   int n_sweeps = 0;
+  bool skip_grad = false;   // energies only: leave out the per-molecule gradient solves
 
   // forces (src/moldynamics.cpp:524-587, src/expcenter.cpp:123-149)
   bool compute_forces(std::vector<P3> &force, std::vector<P3> &torque)
@@ -1845,6 +1901,360 @@ struct System {
         pot += e;
       }
     return pot;
+  }
+
+  // ---------------------------------------------------------------- adjoint (pinning form)
+  // Gradient of the lab-frame interaction energy (total_energy_lab) with respect to
+  // every molecule's position and orientation, through the converged polarization
+  // of the reference's procedure (polarize_mutual, src/molecule.cpp:1988-2263): the
+  // first round from self values (recomputeFromSelfVal), its rotated H frozen for the
+  // later rounds (solveSurfaceCharges() does not rotate, src/expcenter.cpp:594-598),
+  // then the intra-molecular fixed point.  Every linear operator is made an explicit
+  // matrix here and transposed exactly; truncation orders and surface point sets are
+  // held at their converged values.  It is the checker of the CUDA backward pass,
+  // itself checked against central differences of total_energy_lab.
+  struct LinMat {
+    int nin = 0, nout = 0;
+    std::vector<double> a;   // row-major nout x nin
+    vec apply(const vec &x) const
+    {
+      vec y(nout, 0.0);
+      for (int r = 0; r < nout; r++) {
+        double s = 0.0;
+        for (int c = 0; c < nin && c < (int)x.size(); c++) s += a[(size_t)r * nin + c] * x[c];
+        y[r] = s;
+      }
+      return y;
+    }
+    vec applyT(const vec &w) const
+    {
+      vec y(nin, 0.0);
+      for (int r = 0; r < nout && r < (int)w.size(); r++)
+        for (int c = 0; c < nin; c++) y[c] += a[(size_t)r * nin + c] * w[r];
+      return y;
+    }
+  };
+  template <class Fn>
+  static LinMat lin_of(int nin, int nout, Fn f)
+  {
+    LinMat M;
+    M.nin = nin; M.nout = nout;
+    M.a.assign((size_t)nin * nout, 0.0);
+    vec e(nin, 0.0), o;
+    for (int c = 0; c < nin; c++) {
+      e[c] = 1.0;
+      o.clear();
+      f(e, o);
+      for (int r = 0; r < nout && r < (int)o.size(); r++) M.a[(size_t)r * nin + c] = o[r];
+      e[c] = 0.0;
+    }
+    return M;
+  }
+  static double vdot(const vec &a, const vec &b)
+  {
+    double s = 0.0;
+    for (size_t k = 0; k < a.size() && k < b.size(); k++) s += a[k] * b[k];
+    return s;
+  }
+  static void vacc(vec &a, const vec &b, double w = 1.0)
+  {
+    if (a.size() < b.size()) a.resize(b.size(), 0.0);
+    for (size_t k = 0; k < b.size(); k++) a[k] += w * b[k];
+  }
+  // molecule rotation matrices: forward (molecule -> lab) or back, and their
+  // derivatives for a lab-frame rotation of the molecule about axis c
+  LinMat rot_mat(const Quat &q, bool fwd) const
+  {
+    Rot R;
+    R.reset_quat(T, q, NP);
+    const int p2 = NP * NP;
+    return lin_of(p2, p2, [&](const vec &x, vec &y) { R.rotate_xi(x, y, NP, fwd); });
+  }
+  LinMat drot_mat(const Quat &q, int c, bool fwd, double eps = 1e-5) const
+  {
+    P3 ax(c == 0, c == 1, c == 2);
+    LinMat Mp = rot_mat(qmul(axis_angle(ax, eps), q), fwd), Mm = rot_mat(qmul(axis_angle(ax, -eps), q), fwd);
+    for (size_t k = 0; k < Mp.a.size(); k++) Mp.a[k] = (Mp.a[k] - Mm.a[k]) / (2 * eps);
+    return Mp;
+  }
+  // inner solve transposed (src/expcenter.cpp:1079-1135 at its fixed point): given
+  // dU/dF, dU/dH of the solved sphere, returns dU/dLF, dU/dLH (each NP^2)
+  void solve_T(const SphType &S, const vec &gF, const vec &gH, vec &gLF, vec &gLH) const
+  {
+    const int p = NP, p2 = p * p, n2 = 2 * p2;
+    std::vector<double> A((size_t)n2 * n2, 0.0);   // A x = rhs, x = (F, H)
+    std::vector<int> deg(p2);
+    for (int n = 0; n < p; n++) for (int k = n * n; k < (n + 1) * (n + 1); k++) deg[k] = n;
+    auto M = [&](int i, int kk) { return S.imat[(size_t)kk * p2 + i]; };
+    for (int i = 0; i < p2; i++) {
+      const double c3 = T.CONST3[deg[i]], ci = S.cInvH[deg[i]];
+      for (int kk = 0; kk < p2; kk++) {
+        const double m = M(i, kk);
+        A[(size_t)i * n2 + kk] -= c3 * m * S.cF1[deg[kk]];
+        A[(size_t)i * n2 + p2 + kk] -= c3 * m * S.cH1[deg[kk]];
+        A[(size_t)(p2 + i) * n2 + kk] -= ci * m * S.cF2[deg[kk]];
+        A[(size_t)(p2 + i) * n2 + p2 + kk] -= ci * m * S.cH2[deg[kk]];
+      }
+      A[(size_t)i * n2 + i] += 1.0;
+      A[(size_t)(p2 + i) * n2 + p2 + i] += 1.0;
+    }
+    // solve A^T y = g by Gaussian elimination with partial pivoting
+    std::vector<double> B((size_t)n2 * n2), y(n2);
+    for (int r = 0; r < n2; r++) for (int c = 0; c < n2; c++) B[(size_t)r * n2 + c] = A[(size_t)c * n2 + r];
+    for (int k = 0; k < p2; k++) { y[k] = k < (int)gF.size() ? gF[k] : 0.0; y[p2 + k] = k < (int)gH.size() ? gH[k] : 0.0; }
+    for (int c = 0; c < n2; c++) {
+      int piv = c;
+      for (int r = c + 1; r < n2; r++) if (fabs(B[(size_t)r * n2 + c]) > fabs(B[(size_t)piv * n2 + c])) piv = r;
+      if (piv != c) { for (int k = 0; k < n2; k++) std::swap(B[(size_t)c * n2 + k], B[(size_t)piv * n2 + k]); std::swap(y[c], y[piv]); }
+      for (int r = c + 1; r < n2; r++) {
+        const double f = B[(size_t)r * n2 + c] / B[(size_t)c * n2 + c];
+        if (f == 0.0) continue;
+        for (int k = c; k < n2; k++) B[(size_t)r * n2 + k] -= f * B[(size_t)c * n2 + k];
+        y[r] -= f * y[c];
+      }
+    }
+    for (int c = n2 - 1; c >= 0; c--) {
+      double s = y[c];
+      for (int k = c + 1; k < n2; k++) s -= B[(size_t)c * n2 + k] * y[k];
+      y[c] = s / B[(size_t)c * n2 + c];
+    }
+    // y = dU/d(C3 M fb) and dU/d(CI M hb): back through M and the diagonal scalings
+    vec gfb(p2, 0.0), ghb(p2, 0.0);
+    for (int i = 0; i < p2; i++) {
+      const double yf = y[i] * T.CONST3[deg[i]], yh = y[p2 + i] * S.cInvH[deg[i]];
+      for (int kk = 0; kk < p2; kk++) { gfb[kk] += M(i, kk) * yf; ghb[kk] += M(i, kk) * yh; }
+    }
+    gLF.assign(p2, 0.0); gLH.assign(p2, 0.0);
+    for (int k = 0; k < p2; k++) {
+      const int n = deg[k];
+      gLH[k] = S.cLH1[n] * gfb[k] + S.cLH2[n] * ghb[k];
+      gLF[k] = S.cLF1[n] * gfb[k] + S.cLF2[n] * ghb[k];
+    }
+  }
+  // intra near coupling of sphere kj (F, H) into sphere ki (LF, LH) with frozen
+  // orders: analytic (sep >= 5) or numeric through the surface charges (sep < 5)
+  void intra_maps(int i, int ki, int kj, LinMat &AF, LinMat &AH) const
+  {
+    const SphType &Si = st(i, ki), &Sj = st(i, kj);
+    const SphState &Zj = mols[i].s[kj];
+    const int p2 = NP * NP;
+    P3 P = Si.cen - Sj.cen;
+    const double rho = P.norm(), sep = rho - Si.rad - Sj.rad;
+    const int pF = compute_order(NP, rho, Zj.tF, Sj.rad), pH = compute_order(NP, rho, Zj.tH, Sj.rad);
+    if (sep > 0 && !(sep < 5)) {
+      XForm X; X.reset_intra(T, P, pH, pF, Sj.rad, Si.rad);
+      AF = lin_of(p2, p2, [&](const vec &x, vec &y) { X.xformF(x, y); });
+      AH = lin_of(p2, p2, [&](const vec &x, vec &y) { X.xformH(x, y); });
+      return;
+    }
+    const double dA = 4 * M_PI / double(Sj.nspx);
+    auto numeric = [&](const vec &v, vec &L, bool kap) {
+      L.assign(p2, 0.0);
+      for (size_t h = 0; h < Sj.spx.size(); h++) {
+        Sph q = cart2sph(Sj.spx[h]);
+        vec Y; sph_harm(T, q.theta, q.phi, NP, Y);
+        for (int n = 0; n < NP; n++)
+          for (int m = 0; m < 2 * n + 1; m++) Y[IDX(n) + m] *= kap ? Sj.cChgH[n] : T.CONST2[n];
+        const double qh = inprod_unit(v, Y) * dA;
+        if (qh == 0.0) continue;
+        vec Lh;
+        add_local_charge(T, Lh, qh, Sj.spx[h] - P, kap, kap ? pH : pF, Si.rad);
+        vacc(L, Lh);
+      }
+    };
+    AF = lin_of(p2, p2, [&](const vec &x, vec &y) { numeric(x, y, false); });
+    AH = lin_of(p2, p2, [&](const vec &x, vec &y) { numeric(x, y, true); });
+  }
+  // geometric part of one inter-molecular pair transform: L_tgt += T(P) v with
+  // P = c_tgt - c_src, weighted by g = dU/dL_tgt; adds dU/dv into gv and the pose terms
+  void pair_adjoint(int it, int kt, int is, int ks, int p, const vec &v, const vec &g, vec &gv,
+                    std::vector<P3> &dpos, std::vector<P3> &drot) const
+  {
+    const int p2 = NP * NP;
+    P3 P = cen_lab(it, kt) - cen_lab(is, ks);
+    XForm X; X.reset(T, P, p, st(is, ks).rad, st(it, kt).rad, true);
+    LinMat Tm = lin_of(p2, p2, [&](const vec &x, vec &y) { X.xformH(x, y); });
+    vacc(gv, Tm.applyT(g));
+    vec G[3];
+    X.xformH_grad(v, G);
+    const P3 gP(vdot(g, G[0]), vdot(g, G[1]), vdot(g, G[2]));
+    dpos[it] = dpos[it] + gP; dpos[is] = dpos[is] - gP;
+    drot[it] = drot[it] + cross(mols[it].s[kt].cenRot, gP);
+    drot[is] = drot[is] - cross(mols[is].s[ks].cenRot, gP);
+  }
+  // dU/dpos and dU/domega (lab frame) of total_energy_lab after compute_forces
+  void backward(std::vector<P3> &dpos, std::vector<P3> &drot, int max_its = 2000) const
+  {
+    const int nmol = mols.size(), p2 = NP * NP;
+    dpos.assign(nmol, P3()); drot.assign(nmol, P3());
+    std::vector<LinMat> RF(nmol), RB(nmol), dRF(3 * nmol), dRB(3 * nmol);
+    for (int i = 0; i < nmol; i++) {
+      RF[i] = rot_mat(mols[i].orient, true); RB[i] = rot_mat(mols[i].orient, false);
+      for (int c = 0; c < 3; c++) { dRF[3 * i + c] = drot_mat(mols[i].orient, c, true); dRB[3 * i + c] = drot_mat(mols[i].orient, c, false); }
+    }
+    std::vector<std::vector<vec> > Hl(nmol), gHl(nmol), gH(nmol);
+    for (int i = 0; i < nmol; i++) {
+      Hl[i].resize(mols[i].s.size()); gHl[i].assign(mols[i].s.size(), vec(p2, 0.0)); gH[i] = gHl[i];
+      for (size_t k = 0; k < mols[i].s.size(); k++) Hl[i][k] = RF[i].apply(trunc_or_pad(mols[i].s[k].H, NP));
+    }
+    // energy
+    for (int i = 0; i < nmol; i++)
+      for (int j = i + 1; j < nmol; j++)
+        for (size_t ki = 0; ki < mols[i].s.size(); ki++) {
+          const SphType &Si = st(i, ki);
+          const SphState &Zi = mols[i].s[ki];
+          vec a(p2);
+          const double fact = 1 / (Zi.hscale * Si.rad);
+          double sc = 1.0;
+          for (int n = 0; n < NP; n++, sc *= fact)
+            for (int m = 0; m < 2 * n + 1; m++) a[IDX(n) + m] = (m == 0 ? 1.0 : 2.0) * sc;
+          vec wi(p2);
+          for (int k = 0; k < p2; k++) wi[k] = a[k] * Hl[i][ki][k];
+          for (size_t kj = 0; kj < mols[j].s.size(); kj++) {
+            const SphType &Sj = st(j, kj);
+            const SphState &Zj = mols[j].s[kj];
+            P3 P = cen_lab(i, ki) - cen_lab(j, kj);
+            const double rho = P.norm();
+            int pi2j = compute_order(NP, rho, Zi.tH, Si.rad), pj2i = compute_order(NP, rho, Zj.tH, Sj.rad);
+            const int minp = pi2j < pj2i ? pi2j : pj2i;
+            XForm X; X.reset(T, P, minp, Sj.rad, Si.rad, false);
+            vec L; X.xformH(Hl[j][kj], L);
+            for (int k = 0; k < (int)L.size(); k++) gHl[i][ki][k] += a[k] * L[k];
+            pair_adjoint(i, ki, j, kj, minp, Hl[j][kj], wi, gHl[j][kj], dpos, drot);
+          }
+        }
+    // Hlab = RF H
+    for (int i = 0; i < nmol; i++)
+      for (size_t k = 0; k < mols[i].s.size(); k++) {
+        const vec H = trunc_or_pad(mols[i].s[k].H, NP);
+        for (int c = 0; c < 3; c++) {
+          const double d = vdot(gHl[i][k], dRF[3 * i + c].apply(H));
+          if (c == 0) drot[i].x += d; else if (c == 1) drot[i].y += d; else drot[i].z += d;
+        }
+        gH[i][k] = RF[i].applyT(gHl[i][k]);
+      }
+    // the intra-molecular fixed point over the polarized spheres (stage 2)
+    std::vector<std::pair<int, int> > P;
+    std::map<std::pair<int, int>, int> idx;
+    for (int i = 0; i < nmol; i++)
+      if (mols[i].interXForm)
+        for (size_t k = 0; k < mols[i].s.size(); k++)
+          if (!mols[i].s[k].interPol.empty()) { idx[{i, (int)k}] = P.size(); P.push_back({i, (int)k}); }
+    const int nP = P.size();
+    std::vector<std::vector<std::pair<int, std::pair<LinMat, LinMat> > > > Ain(nP);   // s <- (s2, AF, AH)
+    for (int u = 0; u < nP; u++) {
+      const int i = P[u].first, ki = P[u].second;
+      for (int kj : st(i, ki).near) {
+        auto it = idx.find({i, kj});
+        if (it == idx.end()) continue;
+        LinMat AF, AH;
+        intra_maps(i, ki, kj, AF, AH);
+        Ain[u].push_back({it->second, {AF, AH}});
+      }
+    }
+    // transposed fixed point lambda_v = g_v + sum_u A_uv^T S_u^T lambda_u, swept in the
+    // reverse of the forward sphere order with the latest values (Gauss-Seidel on the
+    // transposed system; the forward's splitting converges, Jacobi need not)
+    std::vector<std::vector<std::pair<int, int> > > Aout(nP);   // v -> (u, index in Ain[u])
+    for (int u = 0; u < nP; u++)
+      for (size_t e = 0; e < Ain[u].size(); e++) Aout[Ain[u][e].first].push_back({u, (int)e});
+    std::vector<vec> lF(nP, vec(p2, 0.0)), lH(nP), mF(nP), mH(nP);
+    for (int u = 0; u < nP; u++) {
+      lH[u] = gH[P[u].first][P[u].second];
+      solve_T(st(P[u].first, P[u].second), lF[u], lH[u], mF[u], mH[u]);
+    }
+    for (int it = 0; it < max_its; it++) {
+      double dn = 0.0, nn = 0.0;
+      for (int v = nP - 1; v >= 0; v--) {
+        vec nF(p2, 0.0), nH = gH[P[v].first][P[v].second];
+        for (auto &ue : Aout[v]) {
+          const auto &A = Ain[ue.first][ue.second].second;
+          vacc(nF, A.first.applyT(mF[ue.first]));
+          vacc(nH, A.second.applyT(mH[ue.first]));
+        }
+        for (int k = 0; k < p2; k++) {
+          dn += (nF[k] - lF[v][k]) * (nF[k] - lF[v][k]) + (nH[k] - lH[v][k]) * (nH[k] - lH[v][k]);
+          nn += nF[k] * nF[k] + nH[k] * nH[k];
+        }
+        lF[v] = nF; lH[v] = nH;
+        solve_T(st(P[v].first, P[v].second), lF[v], lH[v], mF[v], mH[v]);
+      }
+      if (dn <= 1e-30 * nn) break;
+    }
+    // stage-2 LS: LS = RB(sum T(Hrot)); its dU/dLS is the LH part of mu
+    std::vector<std::vector<vec> > gHrot(nmol);
+    for (int i = 0; i < nmol; i++) gHrot[i].assign(mols[i].s.size(), vec(p2, 0.0));
+    for (int u = 0; u < nP; u++) {
+      const int i = P[u].first, ki = P[u].second;
+      const SphState &Z = mols[i].s[ki];
+      vec LSrot(p2, 0.0);
+      for (auto &e : Z.interPol) {
+        const SphState &Zm = mols[e.first].s[e.second];
+        P3 Pv = cen_lab(i, ki) - cen_lab(e.first, e.second);
+        const int p = compute_order(NP, Pv.norm(), Zm.tH, st(e.first, e.second).rad);
+        XForm X; X.reset(T, Pv, p, st(e.first, e.second).rad, st(i, ki).rad, false);
+        vec t; X.xformH(trunc_or_pad(Zm.Hrot, NP), t); vacc(LSrot, t);
+      }
+      const vec gLSrot = RB[i].applyT(mH[u]);
+      for (int c = 0; c < 3; c++) {
+        const double d = vdot(mH[u], dRB[3 * i + c].apply(LSrot));
+        if (c == 0) drot[i].x += d; else if (c == 1) drot[i].y += d; else drot[i].z += d;
+      }
+      for (auto &e : Z.interPol) {
+        const SphState &Zm = mols[e.first].s[e.second];
+        P3 Pv = cen_lab(i, ki) - cen_lab(e.first, e.second);
+        const int p = compute_order(NP, Pv.norm(), Zm.tH, st(e.first, e.second).rad);
+        pair_adjoint(i, ki, e.first, e.second, p, trunc_or_pad(Zm.Hrot, NP), gLSrot, gHrot[e.first][e.second], dpos, drot);
+      }
+    }
+    // Hrot = RF H1 (stage 1), H1 = RB Hrot
+    std::vector<std::vector<vec> > gHsr(nmol);
+    for (int i = 0; i < nmol; i++) gHsr[i].assign(mols[i].s.size(), vec(p2, 0.0));
+    for (int u = 0; u < nP; u++) {
+      const int i = P[u].first, ki = P[u].second;
+      const SphState &Z = mols[i].s[ki];
+      const vec H1 = RB[i].apply(trunc_or_pad(Z.Hrot, NP));
+      for (int c = 0; c < 3; c++) {
+        const double d = vdot(gHrot[i][ki], dRF[3 * i + c].apply(H1));
+        if (c == 0) drot[i].x += d; else if (c == 1) drot[i].y += d; else drot[i].z += d;
+      }
+      const vec gH1 = RF[i].applyT(gHrot[i][ki]);
+      vec g1F, g1H;
+      solve_T(st(i, ki), vec(p2, 0.0), gH1, g1F, g1H);
+      // stage-1 LS from the neighbours' rotated self H
+      vec LSrot(p2, 0.0);
+      for (auto &e : Z.interPol) {
+        const SphType &Sm = st(e.first, e.second);
+        P3 Pv = cen_lab(i, ki) - cen_lab(e.first, e.second);
+        const int p = compute_order(NP, Pv.norm(), Sm.tHself, Sm.rad);
+        XForm X; X.reset(T, Pv, p, Sm.rad, st(i, ki).rad, false);
+        vec t; X.xformH(trunc_or_pad(mols[e.first].s[e.second].HselfRot, NP), t); vacc(LSrot, t);
+      }
+      const vec gLSrot = RB[i].applyT(g1H);
+      for (int c = 0; c < 3; c++) {
+        const double d = vdot(g1H, dRB[3 * i + c].apply(LSrot));
+        if (c == 0) drot[i].x += d; else if (c == 1) drot[i].y += d; else drot[i].z += d;
+      }
+      for (auto &e : Z.interPol) {
+        const SphType &Sm = st(e.first, e.second);
+        P3 Pv = cen_lab(i, ki) - cen_lab(e.first, e.second);
+        const int p = compute_order(NP, Pv.norm(), Sm.tHself, Sm.rad);
+        pair_adjoint(i, ki, e.first, e.second, p, trunc_or_pad(mols[e.first].s[e.second].HselfRot, NP), gLSrot,
+                     gHsr[e.first][e.second], dpos, drot);
+      }
+    }
+    // HselfRot = RF Hself
+    for (int i = 0; i < nmol; i++)
+      for (size_t k = 0; k < mols[i].s.size(); k++) {
+        bool any = false;
+        for (double x : gHsr[i][k]) if (x != 0.0) { any = true; break; }
+        if (!any) continue;
+        const vec Hs = trunc_or_pad(st(i, k).Hself, NP);
+        for (int c = 0; c < 3; c++) {
+          const double d = vdot(gHsr[i][k], dRF[3 * i + c].apply(Hs));
+          if (c == 0) drot[i].x += d; else if (c == 1) drot[i].y += d; else drot[i].z += d;
+        }
+      }
   }
 
   // ---------------------------------------------------------------- Brownian dynamics
@@ -2107,7 +2517,7 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
   std::ifstream in(spec_path);
   if (!in) return 2;
   Params prm;
-  int NP = 10, dump = 0, energy = 1;
+  int NP = 10, dump = 0, energy = 1, backward = 0, nograd = 0, exact = 0;
   std::vector<std::vector<std::string> > types;
   struct PoseL { int type; double v[7]; };
   std::vector<std::vector<PoseL> > frames;
@@ -2121,6 +2531,9 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
     else if (tok == "idiel") in >> prm.idiel;
     else if (tok == "dump") in >> dump;
     else if (tok == "energy") in >> energy;
+    else if (tok == "backward") in >> backward;
+    else if (tok == "nograd") in >> nograd;
+    else if (tok == "exact") in >> exact;
     else if (tok == "poles") in >> NP;
     else if (tok == "tol") in >> prm.max_polar_dev >> prm.solve_tol >> prm.solve_max_ct >> prm.max_pol_rounds;
     else if (tok == "moltype") { std::vector<std::string> t(4); in >> t[0] >> t[1] >> t[2] >> t[3]; types.push_back(t); }
@@ -2135,6 +2548,8 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
   System sys;
   sys.prm = prm;
   sys.NP = NP;
+  sys.skip_grad = nograd != 0;
+  sys.exact_inner = exact != 0;
   const double kappa = kappa_of_salt(prm.salt, prm.sdiel, prm.temperature);
   sys.T.init(NP, kappa);
   sys.types.resize(types.size());
@@ -2187,6 +2602,14 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
     }
     if (energy) fprintf(out, "ENERGY %.17e\n", sys.total_energy());
     if (energy > 1) fprintf(out, "ENERGYLAB %.17e\n", sys.total_energy_lab());
+    if (backward) {
+      std::vector<P3> dpos, drot;
+      sys.backward(dpos, drot);
+      for (size_t i = 0; i < dpos.size(); i++) {
+        fprintf(out, "DPOS %d %.17e %.17e %.17e\n", (int)i, dpos[i].x, dpos[i].y, dpos[i].z);
+        fprintf(out, "DROT %d %.17e %.17e %.17e\n", (int)i, drot[i].x, drot[i].y, drot[i].z);
+      }
+    }
     if (dump)
       for (size_t i = 0; i < sys.mols.size(); i++)
         for (size_t ki = 0; ki < sys.mols[i].s.size(); ki++) {
