@@ -1961,8 +1961,7 @@ struct System {
     if (a.size() < b.size()) a.resize(b.size(), 0.0);
     for (size_t k = 0; k < b.size(); k++) a[k] += w * b[k];
   }
-  // molecule rotation matrices: forward (molecule -> lab) or back, and their
-  // derivatives for a lab-frame rotation of the molecule about axis c
+  // molecule rotation matrix: forward (molecule -> lab) or back
   LinMat rot_mat(const Quat &q, bool fwd) const
   {
     Rot R;
@@ -1970,12 +1969,43 @@ struct System {
     const int p2 = NP * NP;
     return lin_of(p2, p2, [&](const vec &x, vec &y) { R.rotate_xi(x, y, NP, fwd); });
   }
-  LinMat drot_mat(const Quat &q, int c, bool fwd, double eps = 1e-5) const
+  // generator of a lab-frame rotation about axis c acting on a packed expansion:
+  // d/de [rotation by e about c] v at e = 0.  Within degree n it couples order m
+  // to m +- 1 with half ladder coefficients c_m = sqrt((n - m)(n + m + 1)) / 2 (the
+  // m = 0 entry, weighted 1 against 2 for the others, takes 2 c_0); about z it turns
+  // (Re, Im) of order m by m.  Checked against differenced rotation coefficients.
+  static void rot_generator(int c, const vec &v, vec &o, int P)
   {
-    P3 ax(c == 0, c == 1, c == 2);
-    LinMat Mp = rot_mat(qmul(axis_angle(ax, eps), q), fwd), Mm = rot_mat(qmul(axis_angle(ax, -eps), q), fwd);
-    for (size_t k = 0; k < Mp.a.size(); k++) Mp.a[k] = (Mp.a[k] - Mm.a[k]) / (2 * eps);
-    return Mp;
+    o.assign(P * P, 0.0);
+    for (int n = 1; n < P; n++) {
+      const int b = n * n;
+      auto cm = [&](int m) { return 0.5 * sqrt((double)(n - m) * (n + m + 1)); };
+      auto re = [&](int m) { return m == 0 ? b : b + 2 * m - 1; };
+      auto im = [&](int m) { return b + 2 * m; };
+      for (int m = 0; m <= n; m++) {
+        if (c == 2) {
+          if (m > 0) { o[re(m)] = -m * v[im(m)]; o[im(m)] = m * v[re(m)]; }
+          continue;
+        }
+        if (m == 0) {
+          if (n >= 1) o[b] = (c == 0 ? 2 * cm(0) * v[im(1)] : -2 * cm(0) * v[re(1)]);
+          continue;
+        }
+        double r = 0.0, i = 0.0;
+        if (c == 0) {
+          if (m >= 2) r += cm(m - 1) * v[im(m - 1)];
+          if (m < n) r += cm(m) * v[im(m + 1)];
+          i -= cm(m - 1) * v[re(m - 1)];
+          if (m < n) i -= cm(m) * v[re(m + 1)];
+        } else {
+          r += cm(m - 1) * v[re(m - 1)];
+          if (m < n) r -= cm(m) * v[re(m + 1)];
+          if (m >= 2) i += cm(m - 1) * v[im(m - 1)];
+          if (m < n) i -= cm(m) * v[im(m + 1)];
+        }
+        o[re(m)] = r; o[im(m)] = i;
+      }
+    }
   }
   // inner solve transposed (src/expcenter.cpp:1079-1135 at its fixed point): given
   // dU/dF, dU/dH of the solved sphere, returns dU/dLF, dU/dLH (each NP^2)
@@ -2087,11 +2117,17 @@ struct System {
   {
     const int nmol = mols.size(), p2 = NP * NP;
     dpos.assign(nmol, P3()); drot.assign(nmol, P3());
-    std::vector<LinMat> RF(nmol), RB(nmol), dRF(3 * nmol), dRB(3 * nmol);
-    for (int i = 0; i < nmol; i++) {
-      RF[i] = rot_mat(mols[i].orient, true); RB[i] = rot_mat(mols[i].orient, false);
-      for (int c = 0; c < 3; c++) { dRF[3 * i + c] = drot_mat(mols[i].orient, c, true); dRB[3 * i + c] = drot_mat(mols[i].orient, c, false); }
-    }
+    std::vector<LinMat> RF(nmol), RB(nmol);
+    for (int i = 0; i < nmol; i++) { RF[i] = rot_mat(mols[i].orient, true); RB[i] = rot_mat(mols[i].orient, false); }
+    // derivatives of the molecule rotations for a lab-frame turn about axis c:
+    // d(RF v) = J_c RF v, d(RB v) = -RB J_c v
+    auto dRFv = [&](int i, int c, const vec &v) { vec o; rot_generator(c, RF[i].apply(v), o, NP); return o; };
+    auto dRBv = [&](int i, int c, const vec &v) {
+      vec o; rot_generator(c, v, o, NP);
+      vec r = RB[i].apply(o);
+      for (double &x : r) x = -x;
+      return r;
+    };
     std::vector<std::vector<vec> > Hl(nmol), gHl(nmol), gH(nmol);
     for (int i = 0; i < nmol; i++) {
       Hl[i].resize(mols[i].s.size()); gHl[i].assign(mols[i].s.size(), vec(p2, 0.0)); gH[i] = gHl[i];
@@ -2128,7 +2164,7 @@ struct System {
       for (size_t k = 0; k < mols[i].s.size(); k++) {
         const vec H = trunc_or_pad(mols[i].s[k].H, NP);
         for (int c = 0; c < 3; c++) {
-          const double d = vdot(gHl[i][k], dRF[3 * i + c].apply(H));
+          const double d = vdot(gHl[i][k], dRFv(i, c, H));
           if (c == 0) drot[i].x += d; else if (c == 1) drot[i].y += d; else drot[i].z += d;
         }
         gH[i][k] = RF[i].applyT(gHl[i][k]);
@@ -2197,7 +2233,7 @@ struct System {
       }
       const vec gLSrot = RB[i].applyT(mH[u]);
       for (int c = 0; c < 3; c++) {
-        const double d = vdot(mH[u], dRB[3 * i + c].apply(LSrot));
+        const double d = vdot(mH[u], dRBv(i, c, LSrot));
         if (c == 0) drot[i].x += d; else if (c == 1) drot[i].y += d; else drot[i].z += d;
       }
       for (auto &e : Z.interPol) {
@@ -2215,7 +2251,7 @@ struct System {
       const SphState &Z = mols[i].s[ki];
       const vec H1 = RB[i].apply(trunc_or_pad(Z.Hrot, NP));
       for (int c = 0; c < 3; c++) {
-        const double d = vdot(gHrot[i][ki], dRF[3 * i + c].apply(H1));
+        const double d = vdot(gHrot[i][ki], dRFv(i, c, H1));
         if (c == 0) drot[i].x += d; else if (c == 1) drot[i].y += d; else drot[i].z += d;
       }
       const vec gH1 = RF[i].applyT(gHrot[i][ki]);
@@ -2232,7 +2268,7 @@ struct System {
       }
       const vec gLSrot = RB[i].applyT(g1H);
       for (int c = 0; c < 3; c++) {
-        const double d = vdot(g1H, dRB[3 * i + c].apply(LSrot));
+        const double d = vdot(g1H, dRBv(i, c, LSrot));
         if (c == 0) drot[i].x += d; else if (c == 1) drot[i].y += d; else drot[i].z += d;
       }
       for (auto &e : Z.interPol) {
@@ -2251,7 +2287,7 @@ struct System {
         if (!any) continue;
         const vec Hs = trunc_or_pad(st(i, k).Hself, NP);
         for (int c = 0; c < 3; c++) {
-          const double d = vdot(gHsr[i][k], dRF[3 * i + c].apply(Hs));
+          const double d = vdot(gHsr[i][k], dRFv(i, c, Hs));
           if (c == 0) drot[i].x += d; else if (c == 1) drot[i].y += d; else drot[i].z += d;
         }
       }
