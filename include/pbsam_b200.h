@@ -63,6 +63,18 @@ typedef struct pbsam_params {
                              calls by ~1e-15); the call then waits for the previous evaluation's
                              counters, so consecutive calls of one system do not overlap on the host.
                              No reference counterpart (a B200 launch parameter). */
+  int exact;              /* 0 (default): the reference's iteration, reproduced step by step
+                             (src/molecule.cpp:1988-2263, src/expcenter.cpp:1079-1135).
+                             1: the exact form of the same equations: every sphere's inner F/H
+                             fixed point solved directly through an operator prepared once per
+                             sphere type at the first system (the reference's iteration of it
+                             does not converge on every sphere: its spectral radius can exceed
+                             one, and its result then moves with solve_max_ct), every polarized
+                             sphere swept until its change is below 1e-14 relative, and forces
+                             and torques taken as the exact negative gradient of the lab-frame
+                             energy (pbsam_system_compute_energy_lab) by the adjoint of that state,
+                             in the lab frame (pbsam_system_backward).  One CTA per system; pole
+                             order <= 32.  No reference counterpart. */
 } pbsam_params;
 
 typedef struct pbsam_context pbsam_context;
@@ -126,10 +138,25 @@ int pbsam_system_compute_energy(pbsam_system *sys, double *energy, int on_device
  * H, in the corrected form; the reference has no such call. */
 int pbsam_system_compute_energy_lab(pbsam_system *sys, double *energy, int on_device);
 
+/* Backward pass (exact form only: contexts made with exact = 1).  After
+ * pbsam_system_compute_forces, the gradient of each system's lab-frame interaction
+ * energy U with respect to every molecule's position and orientation, each scaled by
+ * seed[b] = dL/dU of system b (NULL: 1): dpos[n_systems*n_mol*3] = dL/dpos,
+ * dquat[n_systems*n_mol*4] = dL/dquat (the derivative along q' = (1, w/2) q,
+ * tangent to the unit sphere, w the lab-frame rotation vector), drot[n_systems*n_mol*3]
+ * = dL/dw (minus the torque).  Any output may be NULL.  Replaces the reference's
+ * per-molecule gradient solves (CMolecule::polarize_mutual phase D,
+ * src/molecule.cpp:2081-2228, with prepareDTA / recomputeGrad, src/molecule.cpp:1483-1843)
+ * by one transposed solve of the converged state; the reference's own forces are not
+ * the gradient of its energy (its energy, src/molecule.cpp:1850-1890, ignores the
+ * orientation and its gradient solves differentiate a state its sweeps do not reach). */
+int pbsam_system_backward(pbsam_system *sys, const double *seed, double *dpos, double *dquat, double *drot,
+                          int on_device);
+
 /* Counters of the last force evaluation, 8 ints per system: [0] sweeps,
  * [1] inner F/H iterations, [2] inner solves, [3] gradient solves,
  * [4] bit 0: the polarization sweeps hit max_pol_rounds, bit 1: a gradient phase
- * hit it, [5] CTAs that worked on the system. */
+ * (or the exact form's transposed sweeps) hit it, [5] CTAs that worked on the system. */
 int pbsam_system_stats(const pbsam_system *sys, int *stats);
 
 /* CUDA stream the system's work is queued on (cudaStream_t as void*); the

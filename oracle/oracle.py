@@ -105,8 +105,11 @@ def write_spec(path, moltypes, frames, salt=0.05, idiel=4.0, poles=10, tol=DEFAU
     of (type, pos[3], quat[4]).  energy 2 adds the lab-frame energy; backward 1 its
     gradient (DPOS / DROT); nograd 1 leaves out the reference's gradient solves."""
     with open(path, "w") as fh:
-        fh.write("salt %r\nidiel %r\npoles %d\ndump %d\nenergy %d\nbackward %d\nnograd %d\nexact %d\n" % (
-            salt, idiel, poles, dump, energy, backward, nograd, exact))
+        fh.write("salt %r\nidiel %r\npoles %d\ndump %d\nenergy %d\n" % (salt, idiel, poles, dump, energy))
+        # options of the oracle alone (the reference harnesses do not read them)
+        for key, val in (("backward", backward), ("nograd", nograd), ("exact", exact)):
+            if val:
+                fh.write("%s %d\n" % (key, val))
         fh.write("tol %r %r %d %d\n" % tuple(tol))
         for mt in moltypes:
             fh.write("moltype %s %s %s %s\n" % tuple(mt))

@@ -17,6 +17,7 @@
 #include "pbsam_kernels.cu"
 #include "pbsam_setup.cu"
 #include "pbsam_bd.cu"
+#include "pbsam_adjoint.cu"
 
 using namespace pbsam;
 
@@ -196,6 +197,7 @@ extern "C" void pbsam_params_default(pbsam_params *p)
   p->inter_cutoff = 10; p->interact_cutoff = 100; p->intra_cutoff = 30; p->min_sep_numeric = 5;
   p->num_points_x = 10000;
   p->cluster_size = 0;
+  p->exact = 0;
 }
 
 static double kappa_of(const pbsam_params &p)
@@ -211,6 +213,8 @@ extern "C" int pbsam_context_create(const pbsam_params *prm, int device, pbsam_c
   if (prm->poles < 1 || prm->poles > 32) return fail(PBSAM_E_BADARG, "poles must be in [1, 32]");
   if (prm->cluster_size < -1 || prm->cluster_size > PBSAM_MAX_CREW)
     return fail(PBSAM_E_BADARG, "cluster_size must be -1 (adaptive), 0 (automatic) or 1..16");
+  if (prm->exact != 0 && prm->exact != 1) return fail(PBSAM_E_BADARG, "exact must be 0 or 1");
+  if (prm->exact && prm->poles > 32) return fail(PBSAM_E_BADARG, "the exact form supports pole orders up to 32");
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
   if (device < 0 || device >= ndev) return fail(PBSAM_E_BADARG, "no such CUDA device");
@@ -654,6 +658,35 @@ static int finalize_types(pbsam_context *c)
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   cudaFree(scr);
   if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("setup kernels: ") + cudaGetErrorString(e));
+  if (c->prm.exact) {
+    // exact form: the inner fixed point of every type sphere solved once for all
+    // right-hand sides (pbsam_direct_kernel), in chunks whose elimination blocks
+    // take at most about 2 GB
+    const long long n = 2 * NP2;
+    double *G = nullptr;
+    TRY(dalloc(B, &G, (size_t)TS * n * n));
+    tv.Gdir = G;
+    const size_t blk = (size_t)n * 2 * n * sizeof(double);
+    int chunk = (int)std::max<size_t>(1, (size_t)(2ULL << 30) / blk);
+    if (chunk > TS) chunk = TS;
+    double *work = nullptr;
+    int *derr = nullptr;
+    if (cudaMalloc(&work, blk * chunk) != cudaSuccess) return fail(PBSAM_E_NOMEM, "exact-form elimination blocks");
+    if (cudaMalloc(&derr, sizeof(int)) != cudaSuccess) { cudaFree(work); return fail(PBSAM_E_NOMEM, "flag"); }
+    cudaMemset(derr, 0, sizeof(int));
+    for (int t0 = 0; e == cudaSuccess && t0 < TS; t0 += chunk) {
+      const int nb = TS - t0 < chunk ? TS - t0 : chunk;
+      pbsam_direct_kernel<<<nb, PBSAM_TEAM>>>(c->T, tv, t0, work, derr);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    }
+    int herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(work);
+    cudaFree(derr);
+    if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("exact-form operators: ") + cudaGetErrorString(e));
+    if (herr) return fail(PBSAM_E_BADARG, "a sphere's inner fixed point is singular; the exact form cannot be used");
+  }
   c->finalized = true;
   return PBSAM_OK;
 }
@@ -717,8 +750,9 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   chk(dalloc(Bf, &bv.molR, (size_t)B * n_mol * rot_off(2 * NP - 1)));
   chk(dalloc(Bf, &bv.molRS, B * n_mol * 16));
   chk(dalloc(Bf, &bv.sep, B * S * S));
-  s->adaptive = c->prm.cluster_size < 0;
-  s->crew = pick_crew(pbsam_forces_kernel, B, team_smem_bytes(NP), s->adaptive ? 0 : c->prm.cluster_size);
+  // the exact form runs one CTA per system (its backward pass is not shared by a crew)
+  s->adaptive = c->prm.cluster_size < 0 && !c->prm.exact;
+  s->crew = c->prm.exact ? 1 : pick_crew(pbsam_forces_kernel, B, team_smem_bytes(NP), s->adaptive ? 0 : c->prm.cluster_size);
   bv.crew = s->adaptive ? PBSAM_MAX_CREW : s->crew;   // scratch blocks per system: the largest crew it may get
   bv.scr_stride = scr_doubles(NP, S);
   chk(dalloc(Bf, &bv.scr, (size_t)B * bv.crew * bv.scr_stride));
@@ -727,6 +761,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   chk(dalloc(Bf, &bv.dorder, (size_t)B * bv.crew * S));
   if (s->adaptive) chk(dalloc(Bf, &s->d_list, B));
   chk(dalloc(Bf, &bv.force, B * n_mol * 3)); chk(dalloc(Bf, &bv.torque, B * n_mol * 3));
+  chk(dalloc(Bf, &bv.dpos, B * n_mol * 3)); chk(dalloc(Bf, &bv.drot, B * n_mol * 3));
   chk(dalloc(Bf, &bv.energy, B)); chk(dalloc(Bf, &bv.status, B)); chk(dalloc(Bf, &bv.stats, B * 8));
   chk(dalloc(Bf, &bv.tphase, B * PH_N));
   if (r) {
@@ -740,6 +775,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   p.max_polar_dev = c->prm.max_polar_dev; p.solve_tol = c->prm.solve_tol; p.solve_max_ct = c->prm.solve_max_ct;
   p.max_pol_rounds = c->prm.max_pol_rounds; p.inter_cut = c->prm.inter_cutoff; p.interact_cut = c->prm.interact_cutoff;
   p.min_sep_numeric = c->prm.min_sep_numeric; p.idiel = c->prm.idiel; p.sdiel = c->prm.sdiel;
+  p.exact = c->prm.exact;
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);
   if (s->adaptive) {
@@ -902,6 +938,52 @@ extern "C" int pbsam_system_compute_energy(pbsam_system *s, double *energy, int 
 extern "C" int pbsam_system_compute_energy_lab(pbsam_system *s, double *energy, int on_device)
 {
   return energy_launch(s, energy, on_device, 1);
+}
+
+extern "C" int pbsam_system_backward(pbsam_system *s, const double *seed, double *dpos, double *dquat, double *drot,
+                                     int on_device)
+{
+  if (!s) return fail(PBSAM_E_BADARG, "null system");
+  if (!s->ctx->prm.exact) return fail(PBSAM_E_STATE, "the backward pass needs a context made with exact = 1");
+  CK(cudaSetDevice(s->ctx->device));
+  const size_t n = (size_t)s->B * s->nmol;
+  std::vector<void *> tmp;
+  auto cleanup = [&]() { for (void *p : tmp) cudaFree(p); };
+  double *dseed = nullptr, *dp = nullptr, *dq = nullptr, *dr = nullptr;
+  if (seed) {
+    if (on_device) dseed = (double *)seed;
+    else {
+      if (cudaMalloc(&dseed, s->B * sizeof(double)) != cudaSuccess) return fail(PBSAM_E_NOMEM, "seed");
+      tmp.push_back(dseed);
+      if (cudaMemcpyAsync(dseed, seed, s->B * sizeof(double), cudaMemcpyHostToDevice, s->stream) != cudaSuccess) {
+        cleanup();
+        return fail(PBSAM_E_CUDA, "seed copy");
+      }
+    }
+  }
+  auto out = [&](double *user, size_t len, double **dev) -> int {
+    if (!user) { *dev = nullptr; return PBSAM_OK; }
+    if (on_device) { *dev = user; return PBSAM_OK; }
+    if (cudaMalloc(dev, len * sizeof(double)) != cudaSuccess) return fail(PBSAM_E_NOMEM, "backward output");
+    tmp.push_back(*dev);
+    return PBSAM_OK;
+  };
+  int r = out(dpos, 3 * n, &dp);
+  if (!r) r = out(dquat, 4 * n, &dq);
+  if (!r) r = out(drot, 3 * n, &dr);
+  if (r) { cudaStreamSynchronize(s->stream); cleanup(); return r; }
+  pbsam_backward_out_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s->stream>>>(s->c.bv, dseed, dp, dq, dr);
+  cudaError_t e = cudaGetLastError();
+  if (!on_device) {
+    if (e == cudaSuccess && dpos) e = cudaMemcpyAsync(dpos, dp, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && dquat) e = cudaMemcpyAsync(dquat, dq, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && drot) e = cudaMemcpyAsync(drot, dr, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+  }
+  cudaError_t e2 = cudaStreamSynchronize(s->stream);
+  if (e == cudaSuccess) e = e2;
+  cleanup();
+  if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("backward: ") + cudaGetErrorString(e));
+  return PBSAM_OK;
 }
 
 extern "C" int pbsam_system_stats(const pbsam_system *s, int *stats)

@@ -1289,6 +1289,57 @@ __device__ void reexpand_LS(const Team &tm, const Sys &y, int s, bool fromSelf)
   pc.stop(tm, PH_LS);
 }
 
+// The inner F/H fixed point of one sphere solved directly (the exact form): with
+// fb = Vfix + cLH1 LH + cLF1 LF and hb = Dfix + cLH2 LH + cLF2 LF, (F, H) = G (fb, hb),
+// G (2 NP2 x 2 NP2, row-major, one warp per row) the solution operator of the fixed
+// point of CSolExpCenter::solveFH (src/expcenter.cpp:1079-1135) prepared per sphere
+// type by pbsam_direct_kernel.  Returns computeDev2 (src/expcenter.cpp:1336-1370) of H.
+__device__ __noinline__ double solve_direct(const Team &tm, const Tab &T, const TypeView &tv, const Scr &sc, int ts,
+                                            double *F, double *H, const double *LF, const double *LH, double *red,
+                                            int *stats)
+{
+  const int NP = T.NP, NP2 = NP * NP, n2 = 2 * NP2;
+  const double *cst = tv.cst + (size_t)ts * CST_N * NP;
+  const double *Dfix = tv.Dfix + (size_t)ts * NP2, *Vfix = tv.Vfix + (size_t)ts * NP2;
+  const double *G = tv.Gdir + (size_t)ts * n2 * n2;
+  double *x = sc.xs, *Hold = sc.sol;
+  for (int k = tm.rank; k < NP2; k += tm.size) {
+    int n = (int)sqrt((double)k);
+    while (n * n > k) n--;
+    while ((n + 1) * (n + 1) <= k) n++;
+    x[k] = Vfix[k] + cst[CST_LH1 * NP + n] * LH[k] + cst[CST_LF1 * NP + n] * LF[k];
+    x[NP2 + k] = Dfix[k] + cst[CST_LH2 * NP + n] * LH[k] + cst[CST_LF2 * NP + n] * LF[k];
+    Hold[k] = H[k];
+  }
+  tm.sync();
+  const int lane = tm.rank & 31, w = tm.rank >> 5, nw = tm.size >> 5;
+  for (int r = w; r < n2; r += nw) {
+    const double *g = G + (size_t)r * n2;
+    double acc = 0.0;
+    for (int j = lane; j < n2; j += 32) acc += g[j] * x[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+      if (r < NP2) F[r] = acc;
+      else H[r - NP2] = acc;
+    }
+  }
+  tm.sync();
+  double pd = 0.0, ps = 0.0;
+  for (int u = tm.rank; u < NP2; u += tm.size) {
+    int n = (int)sqrt((double)u);
+    while (n * n > u) n--;
+    while ((n + 1) * (n + 1) <= u) n++;
+    const double a = Hold[u], b = H[u], df = a - b;
+    const double wt = (u == n * n) ? 1.0 : 2.0;
+    pd += wt * (df * df);
+    ps += wt * (a * a + b * b);
+  }
+  const double td = team_sum(tm, pd, red), tsm = team_sum(tm, ps, red);
+  if (tm.rank == 0 && stats) { stats[1] += 1; stats[2] += 1; }
+  return tsm > 0.0 ? td / (4 * tsm) : 0.0;
+}
+
 // F/H solve + surface charges of one sphere (src/expcenter.cpp:594-629)
 __device__ double solve_surface(const Team &tm, const Sys &y, int s, bool rotH)
 {
@@ -1296,7 +1347,10 @@ __device__ double solve_surface(const Team &tm, const Sys &y, int s, bool rotH)
   const int ts = y.ts(s);
   PhaseClock pc{y.tph, 0};
   pc.start(tm);
-  double dv = solve_fh(tm, y.cw, y.tph, T, y.c->tv, y.c->prm, y.sc, ts, 1, y.F(s), y.H(s), y.LFS(s), y.LHS(s), y.red, y.stats());
+  double dv = y.c->prm.exact
+                  ? solve_direct(tm, T, y.c->tv, y.sc, ts, y.F(s), y.H(s), y.LFS(s), y.LHS(s), y.red, y.stats())
+                  : solve_fh(tm, y.cw, y.tph, T, y.c->tv, y.c->prm, y.sc, ts, 1, y.F(s), y.H(s), y.LFS(s), y.LHS(s),
+                             y.red, y.stats());
   pc.stop(tm, PH_SOLVE);
   pc.start(tm);
   if (rotH) {
@@ -1793,6 +1847,8 @@ __device__ Sys helper_sys(const Ctx &c, const Crew &cw, int b, void *dsm, double
   return y;
 }
 
+__device__ __noinline__ bool backward_body(const Team &tm, const Sys &y);   // pbsam_adjoint.cu
+
 // One system (the crew leader's part): CMolecule::computeForces.
 __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b, void *dsm, double *red)
 {
@@ -1967,7 +2023,9 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
   }
   int ct = 1;
   const double itot = (mtotal > 0 ? 1.0 / mtotal : 0);
-  const double tol2 = c.prm.max_polar_dev * c.prm.max_polar_dev;
+  // the exact form sweeps to the fixed point whatever max_polar_dev says
+  const double tol2 = c.prm.exact ? fmin(c.prm.max_polar_dev * c.prm.max_polar_dev, 1e-28)
+                                  : c.prm.max_polar_dev * c.prm.max_polar_dev;
   while (dev * itot > tol2 && ct < c.prm.max_pol_rounds) {
     dev = 0.0;
     double maxdevs[32];
@@ -1978,7 +2036,9 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
         for (int s = bv.mol_off[i]; s < bv.mol_off[i + 1]; s++) {
           if (y.nipol(s) == 0) continue;
           double d = bv.dev[y.sc1(s)];
-          if (d > 0.1 * MAXDEV) d = recompute(tm, y, s);
+          // the exact form recomputes every sphere (the selective update can leave a
+          // sphere whose last change was small out of date)
+          if (c.prm.exact || d > 0.1 * MAXDEV) d = recompute(tm, y, s);
           if (maxdevs[i] < d) maxdevs[i] = d;
           dmol += d;
         }
@@ -1991,6 +2051,30 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
   if (tm.rank == 0) {
     st[0] = ct;
     if (dev * itot > tol2) st[4] |= 1;   // polarization hit the sweep cap
+  }
+  if (c.prm.exact) {
+    // forces and torques: the adjoint of the converged state (lab frame)
+    tm.sync();
+    PhaseClock bk{y.tph, 0};
+    bk.start(tm);
+    const bool ok = backward_body(tm, y);
+    bk.stop(tm, PH_GRX);
+    for (int t = tm.rank; t < nmol * 3; t += tm.size) {
+      bv.force[(size_t)b * nmol * 3 + t] = -bv.dpos[(size_t)b * nmol * 3 + t];
+      bv.torque[(size_t)b * nmol * 3 + t] = -bv.drot[(size_t)b * nmol * 3 + t];
+    }
+    int bad = 0;
+    for (int t = tm.rank; t < nmol * 3; t += tm.size)
+      if (!isfinite(bv.force[(size_t)b * nmol * 3 + t]) || !isfinite(bv.torque[(size_t)b * nmol * 3 + t])) bad = 1;
+    bad = __syncthreads_or(bad);
+    if (tm.rank == 0) {
+      if (!ok) st[4] |= 2;
+      if (bad) bv.status[b] = PBSAM_STATUS_NAN;
+      else if (st[4]) bv.status[b] = PBSAM_STATUS_NOT_CONVERGED;
+    }
+    tm.sync();
+    total.stop(tm, PH_TOTAL);
+    return;
   }
   // ---- gradient phase (src/molecule.cpp:2081-2228)
   for (int j = 0; j < nmol; j++) {

@@ -18,6 +18,7 @@ struct SolveParams {
   double interact_cut;     // inter-molecular interaction cutoff
   double min_sep_numeric;  // intra pairs closer than this re-expand numerically
   double idiel, sdiel;
+  int exact;               // 1: exact form (direct inner solves, full sweeps, adjoint forces)
 };
 
 // Per-sphere constant block layout inside TypeView::cst (NP doubles each).
@@ -54,6 +55,8 @@ struct TypeView {
   double2 *pR;             // [TE][rot_off(NP)]
   double *pTH, *pTF;       // [TE][tr_off(NP)] screened / unscreened translation
   double *pS;              // [TE][16] rotation scalars
+  const double *Gdir;      // [TS][2NP2][2NP2] row-major or null: the inner fixed point solved for
+                           // (fb, hb) -> (F, H) (exact form, pbsam_direct_kernel)
 };
 
 // Batch of B independent systems with the same list of molecules.
@@ -89,6 +92,7 @@ struct BatchView {
   long long wscr_stride;     // gradient re-expansion lists (pairs of low order)
   int crew;                  // CTAs per system
   double *force, *torque, *energy;  // [B][nmol][3], [B][nmol][3], [B]
+  double *dpos, *drot;       // [B][nmol][3]: dU/dpos, dU/domega (lab frame) of the last backward pass
   int *status;               // [B]
   const int *fmask;          // [B] or null: systems with fmask[b] == 0 are skipped by the
                              // force kernel (Brownian dynamics steps without forces)

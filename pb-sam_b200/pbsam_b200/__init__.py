@@ -37,7 +37,7 @@ class pbsam_params(ctypes.Structure):
                 ("solve_max_ct", ctypes.c_int), ("max_pol_rounds", ctypes.c_int),
                 ("inter_cutoff", ctypes.c_double), ("interact_cutoff", ctypes.c_double),
                 ("intra_cutoff", ctypes.c_double), ("min_sep_numeric", ctypes.c_double),
-                ("num_points_x", ctypes.c_int), ("cluster_size", ctypes.c_int)]
+                ("num_points_x", ctypes.c_int), ("cluster_size", ctypes.c_int), ("exact", ctypes.c_int)]
 
 
 PBSAM_BD_NAM = 0
@@ -75,6 +75,7 @@ SIGNATURES = {
     "pbsam_system_compute_energy": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "pbsam_system_compute_energy_lab": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "pbsam_system_stats": (ctypes.c_int, [_P, _IP]),
+    "pbsam_system_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int]),
     "pbsam_system_set_stream": (ctypes.c_int, [_P, _P]),
     "pbsam_system_last_kernel_ms": (ctypes.c_int, [_P, _DP]),
     "pbsam_system_phase_ms": (ctypes.c_int, [_P, _DP]),
@@ -249,6 +250,19 @@ class Molecules:
         f = lib().pbsam_system_compute_energy_lab if lab else lib().pbsam_system_compute_energy
         _check(f(self.handle, e.ctypes.data, 0))
         return e
+
+    def backward(self, seed=None):
+        """Gradient of the lab-frame energy of the last (exact-form) evaluation, times a
+        per-system seed dL/dU: (dpos[n_sys, n_mol, 3], dquat[n_sys, n_mol, 4],
+        drot[n_sys, n_mol, 3]), drot the derivative for a lab-frame rotation of each
+        molecule (minus its torque)."""
+        dp = np.zeros((self.n_systems, self.n_mol, 3))
+        dq = np.zeros((self.n_systems, self.n_mol, 4))
+        dr = np.zeros((self.n_systems, self.n_mol, 3))
+        sd = None if seed is None else np.ascontiguousarray(seed, dtype=np.float64).reshape(self.n_systems)
+        _check(lib().pbsam_system_backward(self.handle, None if sd is None else sd.ctypes.data, dp.ctypes.data,
+                                           dq.ctypes.data, dr.ctypes.data, 0))
+        return dp, dq, dr
 
     def stats(self):
         s = np.zeros((self.n_systems, 8), dtype=np.int32)
