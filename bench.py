@@ -246,13 +246,24 @@ def run_ours(args):
     sysb.close()
     ctx.close()
     if args.bd:
+        specs_bd = None
         try:
-            bd = run_bd(args, local, rank, world, dist)
+            bd, specs_bd = run_bd(args, local, rank, world, dist)
         except Exception as e:   # the headline line stands without the BD leg
             bd = {"error": "%s: %s" % (type(e).__name__, e), "gpu_launches": 0}
         if out is not None:
             out["bd"] = bd
             out["gpu_launches"] += bd["gpu_launches"]
+        if args.bd_exact:
+            try:
+                bdx, _ = run_bd(args, local, rank, world, dist, exact=True, specs=specs_bd)
+                if "value" in bd and "value" in bdx:
+                    bdx["vs_plain_bd"] = bdx["value"] / bd["value"]
+            except Exception as e:
+                bdx = {"error": "%s: %s" % (type(e).__name__, e), "gpu_launches": 0}
+            if out is not None:
+                out["bd_exact"] = bdx
+                out["gpu_launches"] += bdx["gpu_launches"]
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -266,21 +277,62 @@ BD_WORKLOAD = ("bdnam p=10: %d trajectories of 2 molecules x 35 spheres (r 3-6 A
                "noise; a step = force evaluation (where c2c < 100 A) + Ermak-McCammon move, one CUDA graph")
 
 
-def run_bd(args, local, rank, world, dist):
+def fd_force_check(ctx, types, pos, quat, h=1e-3, hr=1e-4):
+    """Relative error of the exact form's adjoint forces and torques against central
+    differences of its lab-frame energy (h A, hr rad), one pose, every perturbed pose a
+    system of one batch."""
+    n = pos.shape[0]
+
+    def qmul(a, b):
+        w1, v1, w2, v2 = a[0], a[1:], b[0], b[1:]
+        return np.concatenate([[w1 * w2 - v1 @ v2], w1 * v2 + w2 * v1 + np.cross(v1, v2)])
+    P, Q = [pos], [quat]
+    for i in range(n):
+        for c in range(3):
+            for sg in (1, -1):
+                p = pos.copy()
+                p[i, c] += sg * h
+                P.append(p)
+                Q.append(quat)
+            for sg in (1, -1):
+                ax = np.zeros(3)
+                ax[c] = np.sin(sg * hr / 2)
+                q = quat.copy()
+                q[i] = qmul(np.concatenate([[np.cos(sg * hr / 2)], ax]), quat[i])
+                P.append(pos)
+                Q.append(q)
+    m = ctx.molecules(types, n_systems=len(P))
+    m.set_poses(np.array(P), np.array(Q))
+    f, t, st = m.compute_forces()
+    E = m.compute_energy(lab=True)[1:].reshape(n, 3, 4)
+    m.close()
+    fdf = -(E[:, :, 0] - E[:, :, 1]) / (2 * h)
+    fdt = -(E[:, :, 2] - E[:, :, 3]) / (2 * hr)
+    ef = float(np.max(np.abs(f[0] - fdf)) / max(np.max(np.abs(fdf)), 1e-300))
+    et = float(np.max(np.abs(t[0] - fdt)) / max(np.max(np.abs(fdt)), 1e-300))
+    return {"force_rel_err": ef, "torque_rel_err": et, "h_A": h, "h_rad": hr, "status": int(st[0])}
+
+
+def run_bd(args, local, rank, world, dist, exact=False, specs=None):
     """BD steps per second of a batch of independent two-molecule trajectories:
     every step (a CUDA graph: time step and force mask, force kernel, move kernel)
-    of every trajectory counts as one unit."""
+    of every trajectory counts as one unit.  exact: the exact form (direct inner
+    solves, sweeps to the fixed point, forces by the adjoint of the lab-frame energy)."""
     import torch
     from pbsam_b200 import replicas, workload
     cfg = dict(workload.BD_P10)
-    specs, prep_t, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds_p10)
-    ctx, types = workload.open_context(cfg, specs, device=local)
+    prep_t = {}
+    if specs is None:
+        specs, prep_t, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds_p10)
+    t_ctx = time.time()
+    ctx, types = workload.open_context(cfg, specs, device=local, **({"exact": 1} if exact else {}))
     mols = workload.molecules(cfg)
     B = args.bd_traj
     pos, quat = workload.bd_start(cfg, mols, B, rank=rank)
     ext = max(m.extent() for m in mols)
     dtr, drot = workload.stokes_einstein(ext, cfg["viscosity"], cfg["temperature"])
     sysb = ctx.molecules(types, n_systems=B)
+    prep_t["context_s"] = round(time.time() - t_ctx, 2)
     stream = torch.cuda.current_stream()
     sysb.set_stream(stream.cuda_stream)
     sysb.set_poses(pos, quat)
@@ -330,11 +382,24 @@ def run_bd(args, local, rank, world, dist):
            "e2e": {"value": e2e_units / (e2e_ms * 1e-3), "unit": "BD steps/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": d2h, "note": "one step per call, state read back to the host each step"},
            "gpu_launches": 3 * args.bd_steps, "clocks": clocks, "prep": prep_t}
-    if rank == 0 and args.cpu_baseline:
+    ph = sysb.phase_ms()
+    names = ["solve", "surface", "numeric", "intra", "LS", "DTA", "grad_or_backward", "total"]
+    out["mean_phase_ms"] = {k: round(float(v), 2) for k, v in zip(names, ph[:, :8].mean(axis=0))}
+    st_last = sysb.stats()
+    out["mean_sweeps"] = float(st_last[:, 0].mean())
+    out["mean_inner_solves"] = float(st_last[:, 2].mean())
+    if exact:
+        out["metric"] = BD_METRIC + ", exact form with adjoint forces"
+        out["config"]["form"] = ("exact: direct inner solves, sweeps to the fixed point, forces and torques the "
+                                 "negative gradient of the lab-frame energy by the adjoint (lab frame)")
+        run = [b for b in range(B) if s1["status"][b] == 0]
+        if rank == 0 and run:
+            out["accuracy"] = fd_force_check(ctx, types, s1["pos"][run[0]], s1["quat"][run[0]])
+    if rank == 0 and args.cpu_baseline and not exact:
         out["cpu_baseline"] = bd_cpu_baseline(cfg, specs, sysb, s1, fe / max(units, 1), args)
     sysb.close()
     ctx.close()
-    return out
+    return out, specs
 
 
 def reference_bd_step_seconds(cfg, files, pos, quat, limit_s, workdir, steps=3, variant="fast", seed=1):
@@ -609,6 +674,8 @@ def main():
                     help="CTAs per system (0: automatic, -1: adaptive from the previous step's costs)")
     ap.add_argument("--bd", type=int, default=1, help="also time the Brownian-dynamics workload")
     ap.add_argument("--bd-traj", type=int, default=1024, help="BD trajectories per GPU")
+    ap.add_argument("--bd-exact", type=int, default=1,
+                    help="also time the BD workload in the exact form with adjoint forces")
     ap.add_argument("--bd-steps", type=int, default=20, help="timed BD steps")
     ap.add_argument("--selfpol-rounds-p10", type=int, default=200)
     ap.add_argument("--poses", default="", help="comma-separated subset of the sweep's poses (small cases)")

@@ -165,13 +165,16 @@ def test_exact_eight_molecules_central_differences():
     rng = np.random.default_rng(4242)
     mols = [synth.make_molecule(40, 3.0, 6.0, 1200, 0.6, float(rng.integers(-3, 4)), seed=5000 + k) for k in range(8)]
     prep = pb.CSystem(poles=10, salt=0.05)
-    specs = []
-    for m in mols:
+    raw, tids, specs = [], [], []
+    for m in mols:     # every type first: types are frozen once a system exists
         cen, rad, qp, q = workload._pqr_round(m)
         im = prep.build_imats(cen, rad, n_points=40000)
-        t = prep.create_moltype(cen, rad, qp, q, im, np.zeros((len(rad), 100)), np.zeros((len(rad), 100)), 1.0 / rad)
+        raw.append((cen, rad, qp, q, im))
+        tids.append(prep.create_moltype(cen, rad, qp, q, im, np.zeros((len(rad), 100)), np.zeros((len(rad), 100)),
+                                        1.0 / rad))
+    for t, r in zip(tids, raw):
         F, H, sc, _ = prep.self_polarize(t, max_rounds=6)
-        specs.append((cen, rad, qp, q, im, F, H, sc))
+        specs.append(r + (F, H, sc))
     prep.close()
     ctx = pb.CSystem(poles=10, salt=0.05, exact=1, max_pol_rounds=400)
     try:
