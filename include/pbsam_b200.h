@@ -153,6 +153,15 @@ int pbsam_system_compute_energy_lab(pbsam_system *sys, double *energy, int on_de
 int pbsam_system_backward(pbsam_system *sys, const double *seed, double *dpos, double *dquat, double *drot,
                           int on_device);
 
+/* Electrostatic potential at points from the state of the last force evaluation:
+ * replaces CMolecule::computePotInSpace (src/moldynamics.cpp:470-506) for molecules that
+ * are not aggregated (as in the BD drivers).  points[n_points*3] shared by every system,
+ * or [n_systems*n_points*3] with per_system != 0; pot[n_systems*n_points].  lab = 0 uses
+ * the reference's convention (unrotated sphere centres and molecule-frame H, as its
+ * energy), lab = 1 the rotated centres and lab-frame H. */
+int pbsam_system_potential(pbsam_system *sys, int n_points, const double *points, int per_system, int lab,
+                           double *pot, int on_device);
+
 /* Counters of the last force evaluation, 8 ints per system: [0] sweeps,
  * [1] inner F/H iterations, [2] inner solves, [3] gradient solves,
  * [4] bit 0: the polarization sweeps hit max_pol_rounds, bit 1: a gradient phase

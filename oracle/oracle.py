@@ -100,16 +100,18 @@ def liboracle():
 
 
 def write_spec(path, moltypes, frames, salt=0.05, idiel=4.0, poles=10, tol=DEFAULT_TOL, dump=0, energy=1,
-               backward=0, nograd=0, exact=0):
+               backward=0, nograd=0, exact=0, potpoints=(), potlab=0):
     """moltypes: list of (pqr, imatdir, expdir, expname); frames: list of lists
     of (type, pos[3], quat[4]).  energy 2 adds the lab-frame energy; backward 1 its
     gradient (DPOS / DROT); nograd 1 leaves out the reference's gradient solves."""
     with open(path, "w") as fh:
         fh.write("salt %r\nidiel %r\npoles %d\ndump %d\nenergy %d\n" % (salt, idiel, poles, dump, energy))
         # options of the oracle alone (the reference harnesses do not read them)
-        for key, val in (("backward", backward), ("nograd", nograd), ("exact", exact)):
+        for key, val in (("backward", backward), ("nograd", nograd), ("exact", exact), ("potlab", potlab)):
             if val:
                 fh.write("%s %d\n" % (key, val))
+        for pt in potpoints:   # potential at points (both the oracle and the reference harness)
+            fh.write("potpoint %.17g %.17g %.17g\n" % tuple(pt))
         fh.write("tol %r %r %d %d\n" % tuple(tol))
         for mt in moltypes:
             fh.write("moltype %s %s %s %s\n" % tuple(mt))
@@ -214,6 +216,8 @@ def parse(path):
                 cur["energy"] = float(t[1])
             elif t[0] == "ENERGYLAB":
                 cur["energy_lab"] = float(t[1])
+            elif t[0] == "POT":
+                cur.setdefault("pot", {})[int(t[1])] = float(t[2])
             elif t[0] in ("DPOS", "DROT"):
                 cur.setdefault(t[0].lower(), {})[int(t[1])] = [float(x) for x in t[2:5]]
             elif t[0] == "KAPPA":
@@ -224,6 +228,8 @@ def parse(path):
         n = len(fr["force"])
         fr["force"] = np.array([fr["force"][i] for i in range(n)]).reshape(-1, 3)
         fr["torque"] = np.array([fr["torque"][i] for i in range(n)]).reshape(-1, 3)
+        if "pot" in fr:
+            fr["pot"] = np.array([fr["pot"][i] for i in range(len(fr["pot"]))])
         for key in ("dpos", "drot"):
             if key in fr:
                 fr[key] = np.array([fr[key][i] for i in range(len(fr[key]))]).reshape(-1, 3)

@@ -1903,6 +1903,32 @@ struct System {
     return pot;
   }
 
+  // electrostatic potential at a point from every sphere's H (CMolecule::computePotInSpace,
+  // src/moldynamics.cpp:470-506, molecules not aggregated): the reference's convention uses
+  // the unrotated sphere centres and molecule-frame H; lab = true the rotated centres and
+  // lab-frame H
+  double potential(const P3 &P, bool lab) const
+  {
+    double pot = 0.0;
+    for (size_t i = 0; i < mols.size(); i++) {
+      Rot R;
+      if (lab) R.reset_quat(T, mols[i].orient, NP);
+      for (size_t k = 0; k < mols[i].s.size(); k++) {
+        const SphType &S = st(i, k);
+        const SphState &Z = mols[i].s[k];
+        const P3 c = lab ? mols[i].s[k].cenRot : S.cen;
+        const P3 d = P - mols[i].rcen - c;
+        const int p = compute_order(NP, d.norm(), Z.tH, S.rad);
+        vec L;
+        add_local_charge(T, L, 1.0, d, true, p, S.rad);
+        vec H = Z.H;
+        if (lab) R.rotate_xi(Z.H, H, NP, true);
+        pot += inprod_ml(H, Z.hscale, L, S.rad);
+      }
+    }
+    return pot;
+  }
+
   // ---------------------------------------------------------------- adjoint (pinning form)
   // Gradient of the lab-frame interaction energy (total_energy_lab) with respect to
   // every molecule's position and orientation, through the converged polarization
@@ -2553,7 +2579,8 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
   std::ifstream in(spec_path);
   if (!in) return 2;
   Params prm;
-  int NP = 10, dump = 0, energy = 1, backward = 0, nograd = 0, exact = 0;
+  int NP = 10, dump = 0, energy = 1, backward = 0, nograd = 0, exact = 0, potlab = 0;
+  std::vector<P3> potpts;
   std::vector<std::vector<std::string> > types;
   struct PoseL { int type; double v[7]; };
   std::vector<std::vector<PoseL> > frames;
@@ -2570,6 +2597,8 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
     else if (tok == "backward") in >> backward;
     else if (tok == "nograd") in >> nograd;
     else if (tok == "exact") in >> exact;
+    else if (tok == "potpoint") { double x, y, z; in >> x >> y >> z; potpts.push_back(P3(x, y, z)); }
+    else if (tok == "potlab") in >> potlab;
     else if (tok == "poles") in >> NP;
     else if (tok == "tol") in >> prm.max_polar_dev >> prm.solve_tol >> prm.solve_max_ct >> prm.max_pol_rounds;
     else if (tok == "moltype") { std::vector<std::string> t(4); in >> t[0] >> t[1] >> t[2] >> t[3]; types.push_back(t); }
@@ -2638,6 +2667,8 @@ extern "C" int pbsam_oracle_run(const char *spec_path, const char *out_path)
     }
     if (energy) fprintf(out, "ENERGY %.17e\n", sys.total_energy());
     if (energy > 1) fprintf(out, "ENERGYLAB %.17e\n", sys.total_energy_lab());
+    for (size_t k = 0; k < potpts.size(); k++)
+      fprintf(out, "POT %d %.17e\n", (int)k, sys.potential(potpts[k], potlab != 0));
     if (backward) {
       std::vector<P3> dpos, drot;
       sys.backward(dpos, drot);

@@ -17,6 +17,9 @@
 //   moltype <pqr> <imat dir> <exp dir> <exp name>      (repeat per type)
 //   frame                                               (starts a frame)
 //   mol <type> <x> <y> <z> <qw> <qx> <qy> <qz>          (one per molecule)
+//   potpoint <x> <y> <z>                                (optional, repeat: after each
+//                                                       frame, CMolecule::computePotInSpace
+//                                                       at the point, src/moldynamics.cpp:470-506)
 // The molecule list (types and count) must be the same in every frame.
 #include <cstdio>
 #include <cstdlib>
@@ -83,6 +86,7 @@ int main(int argc, char **argv)
   int dump = 0, energy = 1;
   std::vector<std::vector<std::string> > types;
   std::vector<std::vector<Pose> > frames;
+  std::vector<CPnt> potpts;
   std::string tok;
   while (in >> tok) {
     if (tok == "salt") in >> salt;
@@ -97,6 +101,9 @@ int main(int argc, char **argv)
     else if (tok == "mol") {
       Pose p; in >> p.type >> p.x >> p.y >> p.z >> p.qw >> p.qx >> p.qy >> p.qz;
       frames.back().push_back(p);
+    } else if (tok == "potpoint") {
+      double x, y, z; in >> x >> y >> z;
+      potpts.push_back(CPnt(x, y, z));
     } else { fprintf(stderr, "bad token %s\n", tok.c_str()); return 2; }
   }
   // constants as in the reference BD driver (src/BDnam_main.cpp:49-58)
@@ -144,6 +151,8 @@ int main(int argc, char **argv)
       double e = CMolecule::computeTotalIntEnergy(mols);
       fprintf(out, "ENERGY %.17e\n", e);
     }
+    for (size_t k = 0; k < potpts.size(); k++)
+      fprintf(out, "POT %d %.17e\n", (int)k, CMolecule::computePotInSpace(mols, potpts[k]));
     if (dump) {
       for (size_t i = 0; i < mols.size(); i++)
         for (int ki = 0; ki < mols[i]->getNKS(); ki++) {

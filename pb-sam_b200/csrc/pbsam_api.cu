@@ -986,6 +986,40 @@ extern "C" int pbsam_system_backward(pbsam_system *s, const double *seed, double
   return PBSAM_OK;
 }
 
+extern "C" int pbsam_system_potential(pbsam_system *s, int n_points, const double *points, int per_system, int lab,
+                                      double *pot, int on_device)
+{
+  if (!s || n_points <= 0 || !points || !pot) return fail(PBSAM_E_BADARG, "bad argument");
+  CK(cudaSetDevice(s->ctx->device));
+  const size_t np = (size_t)n_points * (per_system ? s->B : 1), no = (size_t)n_points * s->B;
+  const double *dpts = points;
+  double *dpot = pot, *tp = nullptr, *to = nullptr;
+  if (!on_device) {
+    if (cudaMalloc(&tp, np * 3 * sizeof(double)) != cudaSuccess) return fail(PBSAM_E_NOMEM, "points");
+    if (cudaMalloc(&to, no * sizeof(double)) != cudaSuccess) { cudaFree(tp); return fail(PBSAM_E_NOMEM, "potential"); }
+    dpts = tp;
+    dpot = to;
+  }
+  cudaError_t e = cudaSuccess;
+  if (!on_device) e = cudaMemcpyAsync(tp, points, np * 3 * sizeof(double), cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess && lab) {
+    pbsam_hlab_kernel<<<s->B, PBSAM_TEAM, team_smem_bytes(s->ctx->prm.poles), s->stream>>>(s->c);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    pbsam_potential_kernel<<<(unsigned)((no + 127) / 128), 128, 0, s->stream>>>(s->c, n_points, dpts, per_system ? 1 : 0,
+                                                                                 lab ? 1 : 0, dpot);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && !on_device) e = cudaMemcpyAsync(pot, to, no * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+  const cudaError_t e2 = cudaStreamSynchronize(s->stream);
+  if (e == cudaSuccess) e = e2;
+  if (tp) cudaFree(tp);
+  if (to) cudaFree(to);
+  if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("potential: ") + cudaGetErrorString(e));
+  return PBSAM_OK;
+}
+
 extern "C" int pbsam_system_stats(const pbsam_system *s, int *stats)
 {
   if (!s || !stats) return fail(PBSAM_E_BADARG, "null argument");

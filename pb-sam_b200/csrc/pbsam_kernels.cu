@@ -2302,6 +2302,82 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c, int lab
   if (tm.rank == 0) bv.energy[b] = pot;
 }
 
+// lab-frame sphere centres and H of every sphere of every system (one team per
+// system), for the lab-frame potential
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_hlab_kernel(Ctx c)
+{
+  extern __shared__ double2 dsm[];
+  const Team tm{(int)threadIdx.x, (int)blockDim.x};
+  const BatchView &bv = c.bv;
+  const int b = blockIdx.x;
+  if (b >= bv.B) return;
+  const int NP = c.T.NP, NP2 = NP * NP;
+  const Scr sc = make_scr(scr_of(bv, b, 0), NP, dsm);
+  for (int i = 0; i < bv.nmol; i++) {
+    const double *q = bv.quat + 4 * ((size_t)b * bv.nmol + i);
+    double qn[4];
+    const double in = 1.0 / sqrt((q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) + q[0] * q[0]);
+    qn[0] = q[0] * in; qn[1] = q[1] * in; qn[2] = q[2] * in; qn[3] = q[3] * in;
+    for (int s = bv.mol_off[i] + tm.rank; s < bv.mol_off[i + 1]; s += tm.size)
+      qrot(qn, c.tv.cen + 3 * bv.sph_ts[s], bv.cenRot + 3 * ((size_t)b * bv.S + s));
+    double th, ph, xi;
+    quat_angles(qn, th, ph, xi);
+    RotState rs;
+    double2 *Rm = bv.molR + ((size_t)b * bv.nmol + i) * rot_off(2 * NP - 1);
+    rot_compute(tm, c.T, th, ph, xi, NP, false, rs, Rm, nullptr, sc.sh, sc.lvA, sc.lvB);
+    tm.sync();
+    for (int s = bv.mol_off[i]; s < bv.mol_off[i + 1]; s++) {
+      rot_apply_xi(tm, rs, bv.H + ((size_t)b * bv.S + s) * NP2, bv.Hlab + ((size_t)b * bv.S + s) * NP2, NP, true, NP);
+      tm.sync();
+    }
+  }
+}
+
+// Electrostatic potential at points from every sphere's H (CMolecule::computePotInSpace,
+// src/moldynamics.cpp:470-506, for molecules that are not aggregated, as in the BD
+// drivers): at each sphere the local expansion of a unit charge at the point
+// (CLExpan, screened, truncated at computeOrder of the sphere's total charge) against
+// H.  One thread per (system, point).  lab = 0: the reference's convention, the
+// unrotated sphere centres and molecule-frame H (as its energy); lab = 1: the rotated
+// centres and lab-frame H of pbsam_hlab_kernel.  pts: [npts][3], or per system
+// [B][npts][3] when per_system; pot: [B][npts].
+__global__ void pbsam_potential_kernel(Ctx c, int npts, const double *pts, int per_system, int lab, double *pot)
+{
+  const BatchView &bv = c.bv;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)bv.B * npts) return;
+  const int b = (int)(t / npts), k = (int)(t % npts);
+  const double *P = pts + 3 * ((per_system ? (size_t)b * npts : 0) + k);
+  const Tab &T = c.T;
+  const int NP = T.NP, NP2 = NP * NP;
+  double rad[64];
+  double acc = 0.0;
+  for (int i = 0; i < bv.nmol; i++) {
+    const double *pi = bv.pos + 3 * ((size_t)b * bv.nmol + i);
+    for (int s = bv.mol_off[i]; s < bv.mol_off[i + 1]; s++) {
+      const int ts = bv.sph_ts[s];
+      const double *cs = lab ? bv.cenRot + 3 * ((size_t)b * bv.S + s) : c.tv.cen + 3 * ts;
+      const Sph sp = cart2sph(P[0] - pi[0] - cs[0], P[1] - pi[1] - cs[1], P[2] - pi[2] - cs[2]);
+      const double r = c.tv.rad[ts];
+      const int p = compute_order(NP, sp.rho, bv.tH[(size_t)b * bv.S + s], r);
+      radial_factors(T, sp.rho, 1.0, true, true, p, r, rad);
+      const double *H = (lab ? bv.Hlab : bv.H) + ((size_t)b * bv.S + s) * NP2;
+      const double fact = 1.0 / (bv.hscale[(size_t)b * bv.S + s] * r);
+      double scale = 1.0;
+      double fn[64];
+      for (int n = 0; n < p; n++) { fn[n] = scale * rad[n]; scale *= fact; }
+      double st, ct;
+      sincos(sp.theta, &st, &ct);
+      for (int m = 0; m < p; m++)
+        sh_column(T, ct, st, sp.phi, m, p, [&](int n, double re, double im) {
+          if (m == 0) acc += fn[n] * H[IDX(n)] * re;
+          else acc += 2.0 * fn[n] * (H[IDX(n) + 2 * m - 1] * re + H[IDX(n) + 2 * m] * im);
+        });
+    }
+  }
+  pot[t] = acc;
+}
+
 // state of every system reset to the self-polarized values (CSolExpCenter BD constructor,
 // src/expcenter.cpp:398-425, and initGradient, src/expcenter.cpp:559-569)
 __global__ void pbsam_init_kernel(Ctx c)

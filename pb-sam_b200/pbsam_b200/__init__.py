@@ -76,6 +76,7 @@ SIGNATURES = {
     "pbsam_system_compute_energy_lab": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "pbsam_system_stats": (ctypes.c_int, [_P, _IP]),
     "pbsam_system_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int]),
+    "pbsam_system_potential": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int]),
     "pbsam_system_set_stream": (ctypes.c_int, [_P, _P]),
     "pbsam_system_last_kernel_ms": (ctypes.c_int, [_P, _DP]),
     "pbsam_system_phase_ms": (ctypes.c_int, [_P, _DP]),
@@ -263,6 +264,17 @@ class Molecules:
         _check(lib().pbsam_system_backward(self.handle, None if sd is None else sd.ctypes.data, dp.ctypes.data,
                                            dq.ctypes.data, dr.ctypes.data, 0))
         return dp, dq, dr
+
+    def potential(self, points, lab=False):
+        """Potential at points ([n, 3] shared, or [n_systems, n, 3]) from the state of the
+        last force evaluation (CMolecule::computePotInSpace): [n_systems, n]."""
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        per = pts.ndim == 3
+        n = pts.shape[-2]
+        out = np.zeros((self.n_systems, n))
+        _check(lib().pbsam_system_potential(self.handle, n, pts.ctypes.data, int(per), int(bool(lab)),
+                                            out.ctypes.data, 0))
+        return out
 
     def stats(self):
         s = np.zeros((self.n_systems, 8), dtype=np.int32)
