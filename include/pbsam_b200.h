@@ -75,6 +75,14 @@ typedef struct pbsam_params {
                              energy (pbsam_system_compute_energy_lab) by the adjoint of that state,
                              in the lab frame (pbsam_system_backward).  One CTA per system; pole
                              order <= 32.  No reference counterpart. */
+  double box_length;      /* 0 (default): no periodic box.  > 0: a cubic periodic box of this
+                             edge in A, as CSystem::initConstants(kappa, sdiel, T, true, L)
+                             (src/system.h:18-20) sets it for bdm: every displacement between
+                             molecules (pair lists, re-expansions, energy, potential, minimum
+                             separations, overlap tests) is taken to its minimum image
+                             (CSystem::pbcPos, src/system.cpp:46-55), and BD moves wrap
+                             positions into the box (CMolecule::translate,
+                             src/molecule.h:327). */
 } pbsam_params;
 
 typedef struct pbsam_context pbsam_context;
@@ -278,6 +286,12 @@ int pbsam_imat_build_static(pbsam_context *ctx, int n_sph, const double *centres
  * receives the number of sweeps. */
 int pbsam_selfpol(pbsam_context *ctx, int type_id, int max_rounds, double *fself, double *hself,
                   double *hself_scale, int *rounds);
+
+/* No counterpart in the reference.  The FP64 FMA rate (TFLOP/s) and the L2 read
+ * bandwidth (GB/s) of a device, timed in place over every SM (best of three launches):
+ * the denominators of the force kernel's roofline, whose IMat rows stay in L2 and whose
+ * arithmetic is FP64. */
+int pbsam_device_peaks(int device, double *fp64_tflops, double *l2_gbs);
 
 /* Text of the last error on the calling thread. */
 const char *pbsam_last_error(void);

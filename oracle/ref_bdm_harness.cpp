@@ -1,7 +1,7 @@
 // Brownian-dynamics harness around the reference's own CBDmulti (test oracle only).
 //
-// Builds the reference's multi-molecule driver as bdm does (CSystem::initConstants
-// without the periodic box, CBDmulti::initConstants(2) before the molecules exist,
+// Builds the reference's multi-molecule driver as bdm does (CSystem::initConstants,
+// with the periodic box when the spec has `box <L>`, CBDmulti::initConstants(2) before the molecules exist,
 // the CBDmulti constructor with np1 copies of species 0 and np2 of species 1,
 // src/BDmulti_main.cpp:28-90, src/BDmulti.cpp:26-207), seeds drand48 with a given
 // seed, places the molecules at the spec's poses (species 0 copies first), and runs
@@ -39,6 +39,7 @@ int main(int argc, char **argv)
   std::ifstream in(argv[1]);
   if (!in) return 2;
   double salt = 0.05, idiel = 4.0;
+  double box = 0.0;
   std::vector<std::vector<std::string> > types;
   std::vector<int> ptype;
   std::vector<std::vector<double> > poses;
@@ -55,6 +56,7 @@ int main(int argc, char **argv)
       ptype.push_back(ty); poses.push_back(v);
     }
     else if (tok == "bd") in >> mode >> nsteps >> seed >> unused;
+    else if (tok == "box") in >> box;
     else if (tok == "poles" || tok == "dump" || tok == "energy") { std::string x; in >> x; }
     else if (tok == "tol") { std::string a, b, c, d; in >> a >> b >> c >> d; }
     else if (tok == "bdp" || tok == "bddiff" || tok == "bdnoise") { std::string rest; std::getline(in, rest); }
@@ -69,7 +71,9 @@ int main(int argc, char **argv)
   const double sdiel = 78.0, temperature = 298.15;
   const double kappa = ANGSTROM * sqrt((2 * salt * AVOGADRO_NUM / LITRE * ELECT_CHG * ELECT_CHG) /
                                        (sdiel * PERMITTIVITY_VAC * KB * temperature));
-  CSystem::initConstants(kappa, sdiel, temperature);
+  // a cubic periodic box when the spec gives one (bdm: src/BDmulti_main.cpp:67)
+  if (box > 0) CSystem::initConstants(kappa, sdiel, temperature, true, box);
+  else CSystem::initConstants(kappa, sdiel, temperature);
   CBDmulti::initConstants(2);
   std::vector<char *> f1, f2;
   for (int k = 0; k < 4; k++) {

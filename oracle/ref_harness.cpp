@@ -17,6 +17,8 @@
 //   moltype <pqr> <imat dir> <exp dir> <exp name>      (repeat per type)
 //   frame                                               (starts a frame)
 //   mol <type> <x> <y> <z> <qw> <qx> <qy> <qz>          (one per molecule)
+//   box <L>                                             (optional: a cubic periodic box,
+//                                                       CSystem::initConstants(..., true, L))
 //   potpoint <x> <y> <z>                                (optional, repeat: after each
 //                                                       frame, CMolecule::computePotInSpace
 //                                                       at the point, src/moldynamics.cpp:470-506)
@@ -82,7 +84,7 @@ int main(int argc, char **argv)
   if (argc < 3) { fprintf(stderr, "usage: harness <spec> <out>\n"); return 2; }
   std::ifstream in(argv[1]);
   if (!in) { fprintf(stderr, "cannot open spec\n"); return 2; }
-  double salt = 0.05, idiel = 4.0;
+  double salt = 0.05, idiel = 4.0, box = 0.0;
   int dump = 0, energy = 1;
   std::vector<std::vector<std::string> > types;
   std::vector<std::vector<Pose> > frames;
@@ -101,6 +103,8 @@ int main(int argc, char **argv)
     else if (tok == "mol") {
       Pose p; in >> p.type >> p.x >> p.y >> p.z >> p.qw >> p.qx >> p.qy >> p.qz;
       frames.back().push_back(p);
+    } else if (tok == "box") {
+      in >> box;
     } else if (tok == "potpoint") {
       double x, y, z; in >> x >> y >> z;
       potpts.push_back(CPnt(x, y, z));
@@ -112,7 +116,8 @@ int main(int argc, char **argv)
   const double KBOLTZ = 1.3806503e-23, ANG = 1e-10, LIT = 1e-3;
   const double kappa = ANG * sqrt((2 * salt * AVO / LIT * ECHG * ECHG) /
                                   (sdiel * EPS0 * KBOLTZ * temperature));
-  CSystem::initConstants(kappa, sdiel, temperature);
+  if (box > 0) CSystem::initConstants(kappa, sdiel, temperature, true, box);   // periodic box (bdm)
+  else CSystem::initConstants(kappa, sdiel, temperature);
 
   std::vector<MolTypeData> mt(types.size());
   for (size_t t = 0; t < types.size(); t++)

@@ -291,7 +291,8 @@ __device__ void pair_adjoint(const Team &tm, const Sys &y, int kt, int ks, int p
   double ct[3], cs[3];
   y.cen_lab(kt, ct);
   y.cen_lab(ks, cs);
-  const double P[3] = {ct[0] - cs[0], ct[1] - cs[1], ct[2] - cs[2]};
+  double P[3] = {ct[0] - cs[0], ct[1] - cs[1], ct[2] - cs[2]};
+  min_image(y.c->prm.box, P);
   const double Pm[3] = {-P[0], -P[1], -P[2]};
   PairXf X;
   prep_pair(tm, T, sc, P, p, 0, y.rad(ks), y.rad(kt), true, X);
@@ -392,8 +393,9 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
           double ci[3], cj[3];
           y.cen_lab(si, ci);
           y.cen_lab(sj, cj);
-          const double rho = sqrt((ci[0] - cj[0]) * (ci[0] - cj[0]) + (ci[1] - cj[1]) * (ci[1] - cj[1]) +
-                                  (ci[2] - cj[2]) * (ci[2] - cj[2]));
+          double dd[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+          min_image(c.prm.box, dd);
+          const double rho = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
           const int pi2j = compute_order(NP, rho, bv.tH[y.sc1(si)], y.rad(si));
           const int pj2i = compute_order(NP, rho, bv.tH[y.sc1(sj)], y.rad(sj));
           const int minp = pi2j < pj2i ? pi2j : pj2i;
@@ -509,8 +511,9 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
       double cu[3], c2[3];
       y.cen_lab(u, cu);
       y.cen_lab(s2, c2);
-      const double rho = sqrt((cu[0] - c2[0]) * (cu[0] - c2[0]) + (cu[1] - c2[1]) * (cu[1] - c2[1]) +
-                              (cu[2] - c2[2]) * (cu[2] - c2[2]));
+      double dd[3] = {cu[0] - c2[0], cu[1] - c2[1], cu[2] - c2[2]};
+      min_image(c.prm.box, dd);
+      const double rho = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
       const int p = compute_order(NP, rho, bv.tH[y.sc1(s2)], y.rad(s2));
       pair_adjoint(tm, y, u, s2, p, y.Hrot(s2), gLSrot, gHrot(s2));
     }
@@ -536,7 +539,8 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
       double cu[3], c2[3];
       y.cen_lab(u, cu);
       y.cen_lab(s2, c2);
-      const double P[3] = {cu[0] - c2[0], cu[1] - c2[1], cu[2] - c2[2]};
+      double P[3] = {cu[0] - c2[0], cu[1] - c2[1], cu[2] - c2[2]};
+      min_image(c.prm.box, P);
       const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
       const int p = compute_order(NP, rho, c.tv.tHself[y.ts(s2)], y.rad(s2));
       PairXf X;
@@ -552,8 +556,9 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
       double cu[3], c2[3];
       y.cen_lab(u, cu);
       y.cen_lab(s2, c2);
-      const double rho = sqrt((cu[0] - c2[0]) * (cu[0] - c2[0]) + (cu[1] - c2[1]) * (cu[1] - c2[1]) +
-                              (cu[2] - c2[2]) * (cu[2] - c2[2]));
+      double dd[3] = {cu[0] - c2[0], cu[1] - c2[1], cu[2] - c2[2]};
+      min_image(c.prm.box, dd);
+      const double rho = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
       const int p = compute_order(NP, rho, c.tv.tHself[y.ts(s2)], y.rad(s2));
       pair_adjoint(tm, y, u, s2, p, y.HselfRot(s2), gLSrot1, gHsr(s2));
     }

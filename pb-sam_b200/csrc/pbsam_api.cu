@@ -198,6 +198,7 @@ extern "C" void pbsam_params_default(pbsam_params *p)
   p->num_points_x = 10000;
   p->cluster_size = 0;
   p->exact = 0;
+  p->box_length = 0.0;
 }
 
 static double kappa_of(const pbsam_params &p)
@@ -214,6 +215,8 @@ extern "C" int pbsam_context_create(const pbsam_params *prm, int device, pbsam_c
   if (prm->cluster_size < -1 || prm->cluster_size > PBSAM_MAX_CREW)
     return fail(PBSAM_E_BADARG, "cluster_size must be -1 (adaptive), 0 (automatic) or 1..16");
   if (prm->exact != 0 && prm->exact != 1) return fail(PBSAM_E_BADARG, "exact must be 0 or 1");
+  if (!(prm->box_length >= 0.0) || !std::isfinite(prm->box_length))
+    return fail(PBSAM_E_BADARG, "box_length must be 0 (no periodic box) or a positive edge");
   if (prm->exact && prm->poles > 32) return fail(PBSAM_E_BADARG, "the exact form supports pole orders up to 32");
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
@@ -776,6 +779,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   p.max_pol_rounds = c->prm.max_pol_rounds; p.inter_cut = c->prm.inter_cutoff; p.interact_cut = c->prm.interact_cutoff;
   p.min_sep_numeric = c->prm.min_sep_numeric; p.idiel = c->prm.idiel; p.sdiel = c->prm.sdiel;
   p.exact = c->prm.exact;
+  p.box = c->prm.box_length;
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);
   if (s->adaptive) {
@@ -1185,3 +1189,6 @@ extern "C" int pbsam_system_phase_ms(const pbsam_system *s, double *ms)
 
 // fixed-buffer variant of the IMat builder (uses the helpers above)
 #include "pbsam_static_imat.cu"
+
+// measured device rates for the roofline (uses the helpers above)
+#include "pbsam_probe.cu"

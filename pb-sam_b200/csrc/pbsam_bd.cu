@@ -125,10 +125,11 @@ __device__ __forceinline__ double bd_dt(const BDParams &p, double d)   // comput
   return dt < p.dt_max ? dt : p.dt_max;
 }
 
-__device__ __forceinline__ double c2c_dist(const double *a, const double *b)
+__device__ __forceinline__ double c2c_dist(const double *a, const double *b, double box)   // getC2CDist
 {
-  const double x = a[0] - b[0], y = a[1] - b[1], z = a[2] - b[2];
-  return sqrt(x * x + y * y + z * z);
+  double d[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+  min_image(box, d);
+  return sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
 }
 
 // block-wide test: does molecule i, its centre at P and its sphere centres
@@ -145,7 +146,7 @@ __device__ bool bd_collides(const Ctx &c, const BDView &v, int b, int i, const d
   int hit = 0;
   for (int j = 0; j < nmol; j++) {
     if (j == i) continue;
-    if (c2c_dist(P, pos + 3 * j) - maxRi - c.tv.maxR[bv.mol_type[j]] > 0) continue;
+    if (c2c_dist(P, pos + 3 * j, c.prm.box) - maxRi - c.tv.maxR[bv.mol_type[j]] > 0) continue;
     const int i0 = bv.mol_off[i], ni = bv.mol_off[i + 1] - i0;
     const int j0 = bv.mol_off[j], nj = bv.mol_off[j + 1] - j0;
     for (int u = threadIdx.x; u < ni * nj && !hit; u += blockDim.x) {
@@ -155,6 +156,7 @@ __device__ bool bd_collides(const Ctx &c, const BDView &v, int b, int i, const d
       const double ri = c.tv.rad[bv.sph_ts[ki]], rj = c.tv.rad[bv.sph_ts[kj]];
       double d[3];
       for (int a = 0; a < 3; a++) d[a] = ((P[a] + ci[a]) - pj[a]) - cj[a];
+      min_image(c.prm.box, d);
       const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
       if (form == 0 ? ((dist - ri) - rj < 0.0) : ((ri + rj) - dist > 0.0)) hit = 1;
     }
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_kernel(Ctx c, B
   const double *pos = bv.pos + (size_t)b * nmol * 3;
   if (p.mode == BD_NAM) {
     if (threadIdx.x == 0) {
-      const double cc = c2c_dist(pos, pos + 3);
+      const double cc = c2c_dist(pos, pos + 3, c.prm.box);
       const double d = cc - c.tv.maxR[bv.mol_type[0]] - c.tv.maxR[bv.mol_type[1]];
       v.dt[b] = bd_dt(p, d);
       v.need[b] = cc < p.force_dist;
@@ -204,7 +206,7 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_kernel(Ctx c, B
   int track = 0;
   for (int i = 0; i < nmol; i++)
     for (int j = i + 1; j < nmol; j++) {
-      const double dm = c2c_dist(pos + 3 * i, pos + 3 * j) - c.tv.maxR[bv.mol_type[i]] - c.tv.maxR[bv.mol_type[j]];
+      const double dm = c2c_dist(pos + 3 * i, pos + 3 * j, c.prm.box) - c.tv.maxR[bv.mol_type[i]] - c.tv.maxR[bv.mol_type[j]];
       if (dm < maxd) {
         track = 1;
         const int i0 = bv.mol_off[i], ni = bv.mol_off[i + 1] - i0;
@@ -213,6 +215,7 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_kernel(Ctx c, B
           const int ki = i0 + u / nj, kj = j0 + u % nj;
           double d[3];
           for (int a = 0; a < 3; a++) d[a] = ((pos[3 * i + a] + cen[3 * ki + a]) - pos[3 * j + a]) - cen[3 * kj + a];
+          min_image(c.prm.box, d);
           const double g = (sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) - c.tv.rad[bv.sph_ts[ki]]) -
                            c.tv.rad[bv.sph_ts[kj]];
           smin = g < smin ? g : smin;
@@ -299,6 +302,7 @@ __device__ int bd_translate(const Ctx &c, const BDParams &p, const BDView &v, in
       double d[3];
       bd_kick(p, v, b, drift, sd, d);
       for (int a = 0; a < 3; a++) sm[a] = pos[a] + d[a];
+      min_image(c.prm.box, sm);   // CMolecule::translate wraps into the box
     }
     __syncthreads();
     done = !bd_collides(c, v, b, i, sm, nullptr, 0);
@@ -367,18 +371,18 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_move_kernel(Ctx c, 
       const double f1 = ((v.drot[0] * dt) * p.ikbt) * p.coul_k, f2 = ((v.drot[1] * dt) * p.ikbt) * p.coul_k;
       for (int a = 0; a < 3; a++) { dR[a] = ft * F[3 + a]; dO1[a] = f1 * T[a]; dO2[a] = f2 * T[3 + a]; }
     }
-    const double bdist = c2c_dist(pos, pos + 3);
+    const double bdist = c2c_dist(pos, pos + 3, c.prm.box);
     const int ct = bd_translate(c, p, v, b, 1, dR, sqrt(2 * dt * v.dtr[1]), sm);
     if (threadIdx.x == 0) {
       if (ct == p.max_tries) s_status = BD_STUCK;
-      else if (c2c_dist(pos, pos + 3) > p.escape_dist) s_status = BD_ESCAPED;
+      else if (c2c_dist(pos, pos + 3, c.prm.box) > p.escape_dist) s_status = BD_ESCAPED;
     }
     __syncthreads();
     if (s_status == BD_RUNNING) {
       double *rot = v.rot + (size_t)b * nmol * 4;
       double *q = v.quat + (size_t)b * nmol * 4;
       const double s1 = sqrt(2 * dt * v.drot[0]), s2 = sqrt(2 * dt * v.drot[1]);
-      const double adist = c2c_dist(pos, pos + 3);
+      const double adist = c2c_dist(pos, pos + 3, c.prm.box);
       if (threadIdx.x == 0) {
         double o1[3], o2[3], Q1[4], Q2[4];
         bd_kick(p, v, b, dO1, s1, o1);

@@ -1274,7 +1274,8 @@ __device__ void reexpand_LS(const Team &tm, const Sys &y, int s, bool fromSelf)
     const int s2 = lst[e];
     double cj[3];
     y.cen_lab(s2, cj);
-    const double P[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+    double P[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+    min_image(y.c->prm.box, P);
     const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
     const double TQ = fromSelf ? y.c->tv.tHself[y.ts(s2)] : y.c->bv.tH[y.sc1(s2)];
     const int p = compute_order(y.NP, rho, TQ, y.rad(s2));
@@ -1451,7 +1452,8 @@ __device__ __noinline__ void grad_xform_from(const Team &tm, const Sys &y, int s
   double ci[3], cm[3];
   y.cen_lab(s, ci);
   y.cen_lab(sm, cm);
-  const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+  double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+  min_image(y.c->prm.box, P);
   const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
   const double TQ = self ? y.c->tv.tHself[y.ts(sm)] : y.c->bv.tH[y.sc1(sm)];
   const int p = compute_order(y.NP, rho, TQ, y.rad(sm));
@@ -1468,7 +1470,8 @@ __device__ __forceinline__ int pair_order(const Sys &y, int s, int sm, bool self
   double ci[3], cm[3];
   y.cen_lab(s, ci);
   y.cen_lab(sm, cm);
-  const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+  double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+  min_image(y.c->prm.box, P);
   const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
   const double TQ = self ? y.c->tv.tHself[y.ts(sm)] : y.c->bv.tH[y.sc1(sm)];
   return compute_order(y.NP, rho, TQ, y.rad(sm));
@@ -1482,7 +1485,8 @@ __device__ __noinline__ void grad_xform_warp(const WarpTeam &tw, const Sys &y, c
   double ci[3], cm[3];
   y.cen_lab(s, ci);
   y.cen_lab(sm, cm);
-  const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+  double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+  min_image(y.c->prm.box, P);
   const int p = pair_order(y, s, sm, self);
   PairXf X;
   prep_pair(tw, T, ws, P, p, 0, y.rad(sm), y.rad(s), true, X);
@@ -1627,7 +1631,8 @@ __device__ __noinline__ void grad_share(const Team &tm, const Sys &y, int s, int
       if ((cnt++ % size) != rank) continue;
       double cm[3];
       y.cen_lab(sm, cm);
-      const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+      double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
+      min_image(y.c->prm.box, P);
       const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
       const int p = compute_order(y.NP, rho, bv.maxgH[y.sc1(sm)], y.rad(sm));
       PairXf X;
@@ -1909,8 +1914,9 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
     double a[3], d[3];
     y.cen_lab(s1, a);
     y.cen_lab(s2, d);
-    const double dx = a[0] - d[0], dy = a[1] - d[1], dz = a[2] - d[2];
-    sep[u] = sqrt(dx * dx + dy * dy + dz * dz) - y.rad(s1) - y.rad(s2);
+    double dd[3] = {a[0] - d[0], a[1] - d[1], a[2] - d[2]};
+    min_image(c.prm.box, dd);
+    sep[u] = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]) - y.rad(s1) - y.rad(s2);
   }
   tm.sync();
   if (tm.rank == 0) {
@@ -1922,8 +1928,9 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
       int nn = 0;
       for (int i = 0; i < j; i++) {
         const double *pi = bv.pos + 3 * ((size_t)b * nmol + i), *pj = bv.pos + 3 * ((size_t)b * nmol + j);
-        const double dx = pi[0] - pj[0], dy = pi[1] - pj[1], dz = pi[2] - pj[2];
-        const double c2c = sqrt(dx * dx + dy * dy + dz * dz);
+        double dd[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
+        min_image(c.prm.box, dd);
+        const double c2c = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
         const double ms = c2c - c.tv.maxR[bv.mol_type[i]] - c.tv.maxR[bv.mol_type[j]];
         if (ms < c.prm.interact_cut && nn < 64) neigh[nn++] = i;
       }
@@ -2281,8 +2288,9 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c, int lab
           const double *ci = lab ? y.cenRot(si) : y.cen(si);
           for (int sj = bv.mol_off[j]; sj < bv.mol_off[j + 1]; sj++) {
             const double *cj = lab ? y.cenRot(sj) : y.cen(sj);
-            const double P[3] = {(pi[0] + ci[0]) - (pj[0] + cj[0]), (pi[1] + ci[1]) - (pj[1] + cj[1]),
-                                 (pi[2] + ci[2]) - (pj[2] + cj[2])};
+            double P[3] = {(pi[0] + ci[0]) - (pj[0] + cj[0]), (pi[1] + ci[1]) - (pj[1] + cj[1]),
+                           (pi[2] + ci[2]) - (pj[2] + cj[2])};
+            min_image(c.prm.box, P);
             const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
             const int pi2j = compute_order(y.NP, rho, bv.tH[y.sc1(si)], y.rad(si));
             const int pj2i = compute_order(y.NP, rho, bv.tH[y.sc1(sj)], y.rad(sj));
@@ -2357,7 +2365,9 @@ __global__ void pbsam_potential_kernel(Ctx c, int npts, const double *pts, int p
     for (int s = bv.mol_off[i]; s < bv.mol_off[i + 1]; s++) {
       const int ts = bv.sph_ts[s];
       const double *cs = lab ? bv.cenRot + 3 * ((size_t)b * bv.S + s) : c.tv.cen + 3 * ts;
-      const Sph sp = cart2sph(P[0] - pi[0] - cs[0], P[1] - pi[1] - cs[1], P[2] - pi[2] - cs[2]);
+      double dq[3] = {P[0] - pi[0] - cs[0], P[1] - pi[1] - cs[1], P[2] - pi[2] - cs[2]};
+      min_image(c.prm.box, dq);
+      const Sph sp = cart2sph(dq[0], dq[1], dq[2]);
       const double r = c.tv.rad[ts];
       const int p = compute_order(NP, sp.rho, bv.tH[(size_t)b * bv.S + s], r);
       radial_factors(T, sp.rho, 1.0, true, true, p, r, rad);

@@ -19,7 +19,16 @@ struct SolveParams {
   double min_sep_numeric;  // intra pairs closer than this re-expand numerically
   double idiel, sdiel;
   int exact;               // 1: exact form (direct inner solves, full sweeps, adjoint forces)
+  double box;              // > 0: edge of a cubic periodic box (minimum-image displacements)
 };
+
+// minimum image of a displacement in a cubic periodic box of edge box
+// (CSystem::pbcPos, src/system.cpp:46-55); box <= 0: no periodic box
+__device__ __forceinline__ void min_image(double box, double *d)
+{
+  if (box > 0.0)
+    for (int k = 0; k < 3; k++) d[k] = d[k] - box * round(d[k] / box);
+}
 
 // Per-sphere constant block layout inside TypeView::cst (NP doubles each).
 enum { CST_H1 = 0, CST_F1, CST_H2, CST_F2, CST_LH1, CST_LF1, CST_LH2, CST_LF2, CST_INVH, CST_CHGH, CST_N };

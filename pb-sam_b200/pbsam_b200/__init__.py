@@ -37,7 +37,8 @@ class pbsam_params(ctypes.Structure):
                 ("solve_max_ct", ctypes.c_int), ("max_pol_rounds", ctypes.c_int),
                 ("inter_cutoff", ctypes.c_double), ("interact_cutoff", ctypes.c_double),
                 ("intra_cutoff", ctypes.c_double), ("min_sep_numeric", ctypes.c_double),
-                ("num_points_x", ctypes.c_int), ("cluster_size", ctypes.c_int), ("exact", ctypes.c_int)]
+                ("num_points_x", ctypes.c_int), ("cluster_size", ctypes.c_int), ("exact", ctypes.c_int),
+                ("box_length", ctypes.c_double)]
 
 
 PBSAM_BD_NAM = 0
@@ -87,6 +88,7 @@ SIGNATURES = {
     "pbsam_system_bd_init": (ctypes.c_int, [_P, ctypes.POINTER(pbsam_bd_params), _DP, _DP]),
     "pbsam_system_bd_run": (ctypes.c_int, [_P, ctypes.c_int]),
     "pbsam_system_bd_state": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, ctypes.c_int]),
+    "pbsam_device_peaks": (ctypes.c_int, [ctypes.c_int, _DP, _DP]),
     "pbsam_last_error": (ctypes.c_char_p, []),
 }
 
@@ -140,6 +142,13 @@ def bd_params(mode=PBSAM_BD_NAM, **kw):
 
 def _dptr(a):
     return a.ctypes.data_as(_DP)
+
+
+def device_peaks(device=0):
+    """(FP64 TFLOP/s, L2 read GB/s) of a device, timed in place."""
+    f, l2 = ctypes.c_double(), ctypes.c_double()
+    _check(lib().pbsam_device_peaks(device, ctypes.byref(f), ctypes.byref(l2)))
+    return f.value, l2.value
 
 
 class CSystem:

@@ -21,10 +21,10 @@ DTR = (0.0, 0.03)          # the reference's m_Dtr (src/BDnam.cpp:145), molecule
 DROT = (4.5e-5, 4e-5)      # m_Dr1, m_Dr2
 
 
-def tiny_ctx(cluster_size=0):
+def tiny_ctx(cluster_size=0, **kw):
     import pbsam_b200 as pb
     P = json.load(open(os.path.join(golden_dir("tiny"), "poses.json")))
-    ctx = pb.CSystem(poles=P["poles"], salt=P["salt"], idiel=P["idiel"], cluster_size=cluster_size)
+    ctx = pb.CSystem(poles=P["poles"], salt=P["salt"], idiel=P["idiel"], cluster_size=cluster_size, **kw)
     d = golden_dir("tiny")
     ta = ctx.load_moltype(d + "/molA.pqr", d + "/imA", d + "/expA", "molA.0")
     tb = ctx.load_moltype(d + "/molB.pqr", d + "/imB", d + "/expB", "molB.0")
