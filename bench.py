@@ -366,6 +366,7 @@ def run_bd(args, local, rank, world, dist, exact=False, specs=None):
     ms = e0.elapsed_time(e1)
     clocks = clk.summary()
     s1 = sysb.bd_state()
+    st_timed = sysb.stats()          # counters of the last timed step
     ms_max = replicas.max_over_ranks(ms, dist if world > 1 else None)
     units = int(np.sum(s1["steps"] - s0["steps"]))
     fe = int(np.sum(s1["fevals"] - s0["fevals"]))
@@ -394,9 +395,32 @@ def run_bd(args, local, rank, world, dist, exact=False, specs=None):
            "e2e": {"value": e2e_units / (e2e_ms * 1e-3), "unit": "BD steps/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": d2h, "note": "one step per call, state read back to the host each step"},
            "gpu_launches": 3 * args.bd_steps, "clocks": clocks, "prep": prep_t}
+    if not exact:
+        # roofline of the force kernel (99.99 % of a step): the IMat bytes of the last
+        # timed step's inner iterations (16 p^4 bytes each, re-read from L2) over the
+        # average step time, and its FP64 rate; the solve is only part of a BD
+        # evaluation (mean_phase_ms), the rest being latency-bound re-expansions
+        import pbsam_b200 as pb
+        fp64_peak, l2_peak = pb.device_peaks(local)
+        P = cfg["poles"]
+        its = float(np.sum(st_timed[:, 1]))
+        step_ms = ms / args.bd_steps
+        nbytes, nflops = its * 16.0 * P ** 4, its * 4.0 * P ** 4
+        out_roof = {"bound": "l2", "achieved": nbytes / (step_ms * 1e-3) / 1e9, "peak": l2_peak, "unit": "GB/s",
+                    "frac": nbytes / (step_ms * 1e-3) / 1e9 / l2_peak, "traffic": None,
+                    "peak_kind": "measured in place (L2 read bandwidth over every SM, pbsam_device_peaks)",
+                    "kernel": "pbsam_forces_kernel", "launch_ms": step_ms, "algorithmic_bytes_per_launch": nbytes,
+                    "units": "inner F/H iterations of the last timed step (%d) stand for every step" % int(its),
+                    "fp64": {"achieved_tflops": nflops / (step_ms * 1e-3) / 1e12, "peak_tflops": fp64_peak,
+                             "frac": nflops / (step_ms * 1e-3) / 1e12 / fp64_peak}}
     ph = sysb.phase_ms()
     names = ["solve", "surface", "numeric", "intra", "LS", "DTA", "grad_or_backward", "total"]
     out["mean_phase_ms"] = {k: round(float(v), 2) for k, v in zip(names, ph[:, :8].mean(axis=0))}
+    if not exact:
+        out["roofline"] = out_roof
+    if exact:
+        out["mean_phase_ms"].update({k: round(float(v), 2) for k, v in zip(
+            ["backward_energy", "backward_sweeps", "backward_first_round"], ph[:, 12:15].mean(axis=0))})
     st_last = sysb.stats()
     out["mean_sweeps"] = float(st_last[:, 0].mean())
     out["mean_inner_solves"] = float(st_last[:, 2].mean())

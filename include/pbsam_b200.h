@@ -70,19 +70,33 @@ typedef struct pbsam_params {
                              sphere type at the first system (the reference's iteration of it
                              does not converge on every sphere: its spectral radius can exceed
                              one, and its result then moves with solve_max_ct), every polarized
-                             sphere swept until its change is below 1e-14 relative, and forces
+                             sphere swept until its change is below exact_tol, and forces
                              and torques taken as the exact negative gradient of the lab-frame
                              energy (pbsam_system_compute_energy_lab) by the adjoint of that state,
                              in the lab frame (pbsam_system_backward).  One CTA per system; pole
                              order <= 32.  No reference counterpart. */
   double box_length;      /* 0 (default): no periodic box.  > 0: a cubic periodic box of this
                              edge in A, as CSystem::initConstants(kappa, sdiel, T, true, L)
-                             (src/system.h:18-20) sets it for bdm: every displacement between
-                             molecules (pair lists, re-expansions, energy, potential, minimum
-                             separations, overlap tests) is taken to its minimum image
-                             (CSystem::pbcPos, src/system.cpp:46-55), and BD moves wrap
-                             positions into the box (CMolecule::translate,
-                             src/molecule.h:327). */
+                             (src/system.h:18-20) sets it for bdm.  Molecule centres are wrapped
+                             into the box at each evaluation and BD move (CMolecule::setPos,
+                             translate, src/molecule.h:325-327); the pair lists, the
+                             polarization and gradient re-expansions, the potential, the minimum
+                             separations and the overlap tests take the minimum image of each
+                             displacement (CSystem::pbcPos, src/system.cpp:46-55), while the
+                             gradient lists of prepareDTA (src/molecule.cpp:1515-1619) and the
+                             energy (src/molecule.cpp:1873) take the plain difference of the
+                             wrapped centres, as the reference does.  The lab-frame energy and
+                             the exact form take the minimum image everywhere. */
+  int exact_tables;       /* exact form only.  1 (default): the numeric near-field re-expansions
+                             of each molecule type's overlapping sphere pairs are prepared once
+                             as p^2 x p^2 operators when they fit in 4 GB (p = 10: about 32 MB
+                             per 35-sphere type) and applied as products in the sweeps and in
+                             the backward pass; 0: evaluated from the surface charges each time.
+                             The two agree to rounding. */
+  double exact_tol;       /* exact form only: the sweeps, and the backward pass's transposed
+                             sweeps, stop once the root-mean-square relative change of the
+                             polarized spheres' H (their adjoint) is below it.  Default 1e-14;
+                             the error of the state, and so of the forces, is of this order. */
 } pbsam_params;
 
 typedef struct pbsam_context pbsam_context;
@@ -189,7 +203,9 @@ int pbsam_system_set_stream(pbsam_system *sys, void *stream);
  * [9] set-up (pair lists, molecule rotations), [10] gradient-phase bookkeeping,
  * [11] force and torque sums; sub-phases: [12]-[14] the inter, intra analytic and
  * intra numeric parts of [6], [15] the IMat products within [0].  The phases
- * [0]-[6] and [8]-[11] do not overlap; [7] includes everything. */
+ * [0]-[6] and [8]-[11] do not overlap; [7] includes everything.  In the exact form
+ * (pbsam_params.exact) [6] is the backward pass and [12]-[14] are its energy
+ * adjoint, its transposed sweeps and its first-round and rotation terms. */
 int pbsam_system_phase_ms(const pbsam_system *sys, double *ms);
 
 /* Device time in milliseconds of the last force-kernel launch (CUDA events). */

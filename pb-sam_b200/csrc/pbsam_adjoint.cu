@@ -14,8 +14,8 @@
 //     IMat and C3, CI the degree scalings; (F, H) = G (fb, hb) then costs one
 //     2p^2 x 2p^2 product per solve instead of up to SOLVE_MAX_CT pairs of p^2 x p^2
 //     IMat products (pbsam_direct_kernel, Gauss-Jordan elimination);
-//   * every polarized sphere is swept until the average squared change is below
-//     1e-28, so the state is the fixed point of the reference's equations (the first
+//   * every polarized sphere is swept until the root-mean-square relative change is
+//     below exact_tol (1e-14 by default), so the state is the fixed point of the reference's equations (the first
 //     round from self values, its rotated H kept for the later rounds, the
 //     intra-molecular coupling, as polarize_mutual, src/molecule.cpp:1988-2263);
 //   * the forces and torques are the exact negative gradient of the lab-frame
@@ -311,6 +311,61 @@ __device__ void pair_adjoint(const Team &tm, const Sys &y, int kt, int ks, int p
   tm.sync();
 }
 
+__device__ __forceinline__ double warp_dot(const WarpTeam &tw, const double *a, const double *b, int n)
+{
+  double s = 0.0;
+  for (int k = tw.rank; k < n; k += tw.size) s += a[k] * b[k];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// One pair (si <- sj) of the energy adjoint transformed by a single warp with its own
+// scratch ws (pair_adjoint's arithmetic): part += a . T Hlab_sj (this warp's share of
+// dU/dHlab_si), gHl_sj += W T(sj <- si)(wi / W), and the pose terms <wi, dT/dP Hlab_sj>
+// summed on lane 0 into pose[9]: d/dpos_i (3), d/domega_i (3), d/domega_j (3).
+__device__ __noinline__ void energy_pair_warp(const WarpTeam &tw, const Sys &y, const Scr &ws, int si, int sj, int p,
+                                              const double *Hj, const double *wi, const double *a, double *gHj,
+                                              double *part, double *pose)
+{
+  const Tab &T = y.c->T;
+  const int NP2 = y.NP2;
+  double ct[3], cs[3];
+  y.cen_lab(si, ct);
+  y.cen_lab(sj, cs);
+  double P[3] = {ct[0] - cs[0], ct[1] - cs[1], ct[2] - cs[2]};
+  min_image(y.c->prm.box, P);
+  const double Pm[3] = {-P[0], -P[1], -P[2]};
+  PairXf X;
+  prep_pair(tw, T, ws, P, p, 0, y.rad(sj), y.rad(si), true, X);
+  double *fwd = ws.misc + NP2, *gw = ws.misc + 2 * NP2;
+  pair_apply(tw, T, ws, X, false, Hj, fwd);
+  double *G = ws.G(0);
+  pair_apply_grad(tw, T, ws, X, Hj, G);
+  double gP[3];
+  for (int c = 0; c < 3; c++) gP[c] = warp_dot(tw, wi, G + (size_t)c * NP2, NP2);
+  if (tw.rank == 0) {
+    const double *rt = y.cenRot(si), *rs = y.cenRot(sj);
+    for (int d = 0; d < 3; d++) pose[d] += gP[d];
+    pose[3] += rt[1] * gP[2] - rt[2] * gP[1];
+    pose[4] += rt[2] * gP[0] - rt[0] * gP[2];
+    pose[5] += rt[0] * gP[1] - rt[1] * gP[0];
+    pose[6] -= rs[1] * gP[2] - rs[2] * gP[1];
+    pose[7] -= rs[2] * gP[0] - rs[0] * gP[2];
+    pose[8] -= rs[0] * gP[1] - rs[1] * gP[0];
+  }
+  for (int k = tw.rank; k < NP2; k += tw.size) {
+    part[k] += a[k] * fwd[k];
+    gw[k] = wi[k] / wgt(k);
+  }
+  tw.sync();
+  prep_pair(tw, T, ws, Pm, p, 0, y.rad(si), y.rad(sj), false, X);
+  double *o = ws.G(0);
+  pair_apply(tw, T, ws, X, false, gw, o);
+  for (int k = tw.rank; k < NP2; k += tw.size) gHj[k] += wgt(k) * o[k];
+  tw.sync();
+}
+
 // molecule rotation state of molecule i (the forward prepares it only for molecules
 // with inter-molecular work; the energy needs every molecule)
 __device__ RotState mol_rot(const Team &tm, const Sys &y, int i)
@@ -334,6 +389,15 @@ __device__ RotState mol_rot(const Team &tm, const Sys &y, int i)
     tm.sync();
   }
   return y.molrot(i);
+}
+
+// entry of type sphere kv (index within the type) in the near list of type sphere tsu
+// whose numeric operator exists, or -1
+__device__ __forceinline__ int num_entry(const TypeView &tv, int tsu, int kv)
+{
+  for (int e = tv.near_off[tsu]; e < tv.near_off[tsu + 1]; e++)
+    if (tv.near[e] == kv) return tv.nslot[e] >= 0 ? e : -1;
+  return -1;
 }
 
 __device__ __forceinline__ bool polarized(const Sys &y, int s)
@@ -379,8 +443,31 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
     }
   }
   // ---- the energy: U = sum_{i<j} sum_{si, sj} <a_si . Hlab_si, T(si <- sj) Hlab_sj>
+  // At pole orders up to PBSAM_WARP_MAX_NP the pairs of order <= PBSAM_WARP_P are
+  // dealt round-robin to the CTA's warps, each transforming its pairs alone (a pair
+  // at p = 10 is too narrow to keep 512 threads busy); their shares of dU/dHlab_si
+  // and of the pose terms are added in warp order.  The other pairs are transformed
+  // one by one by the whole CTA.
+  PhaseClock pe{y.tph, 0};
+  pe.start(tm);
+  const bool warps = NP <= PBSAM_WARP_MAX_NP;
+  const int lane = tm.rank & 31, w = tm.rank >> 5, nw = tm.size >> 5;
+  const WarpTeam tw{lane, 32};
+  const Scr ws = warps ? warp_scr(wscr_of(bv, b, 0, w), NP) : sc;
+  auto pair_order_E = [&](int si, int sj) {
+    double ci[3], cj[3];
+    y.cen_lab(si, ci);
+    y.cen_lab(sj, cj);
+    double dd[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
+    min_image(c.prm.box, dd);
+    const double rho = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+    const int pi2j = compute_order(NP, rho, bv.tH[y.sc1(si)], y.rad(si));
+    const int pj2i = compute_order(NP, rho, bv.tH[y.sc1(sj)], y.rad(sj));
+    return pi2j < pj2i ? pi2j : pj2i;
+  };
   for (int i = 0; i < nmol; i++)
-    for (int j = i + 1; j < nmol; j++)
+    for (int j = i + 1; j < nmol; j++) {
+      double pose[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};   // this warp's pose terms (lane 0)
       for (int si = bv.mol_off[i]; si < bv.mol_off[i + 1]; si++) {
         const double fact = 1.0 / (bv.hscale[y.sc1(si)] * y.rad(si));
         double *a = t0, *wi = t1;
@@ -389,21 +476,50 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
           wi[k] = a[k] * Hlab(si)[k];
         }
         tm.sync();
+        if (warps) {
+          double *part = ws.misc;
+          tzero(tw, part, NP2);
+          tw.sync();
+          int q = 0;
+          for (int sj = bv.mol_off[j]; sj < bv.mol_off[j + 1]; sj++) {
+            const int p = pair_order_E(si, sj);
+            if (p > PBSAM_WARP_P) continue;
+            if ((q++ % nw) != w) continue;
+            energy_pair_warp(tw, y, ws, si, sj, p, Hlab(sj), wi, a, gHl(sj), part, pose);
+          }
+          tm.sync();
+          const size_t moff = (size_t)(warp_scr(wscr_of(bv, b, 0, 0), NP).misc - wscr_of(bv, b, 0, 0));
+          for (int k = tm.rank; k < NP2; k += tm.size) {
+            double v = 0.0;
+            for (int u = 0; u < nw; u++) v += wscr_of(bv, b, 0, u)[moff + k];
+            gHl(si)[k] += v;
+          }
+          tm.sync();
+        }
         for (int sj = bv.mol_off[j]; sj < bv.mol_off[j + 1]; sj++) {
-          double ci[3], cj[3];
-          y.cen_lab(si, ci);
-          y.cen_lab(sj, cj);
-          double dd[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
-          min_image(c.prm.box, dd);
-          const double rho = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
-          const int pi2j = compute_order(NP, rho, bv.tH[y.sc1(si)], y.rad(si));
-          const int pj2i = compute_order(NP, rho, bv.tH[y.sc1(sj)], y.rad(sj));
-          const int minp = pi2j < pj2i ? pi2j : pj2i;
-          pair_adjoint(tm, y, si, sj, minp, Hlab(sj), wi, gHl(sj), t2);
+          const int p = pair_order_E(si, sj);
+          if (warps && p <= PBSAM_WARP_P) continue;
+          pair_adjoint(tm, y, si, sj, p, Hlab(sj), wi, gHl(sj), t2);
           for (int k = tm.rank; k < NP2; k += tm.size) gHl(si)[k] += a[k] * t2[k];
           tm.sync();
         }
       }
+      if (warps) {
+        // the warps' pose terms in warp order
+        double *dp = bv.dpos + (size_t)b * nmol * 3, *dr = bv.drot + (size_t)b * nmol * 3;
+        for (int u = 0; u < nw; u++) {
+          if (w == u && lane == 0)
+            for (int d = 0; d < 3; d++) {
+              dp[3 * i + d] += pose[d];
+              dp[3 * j + d] -= pose[d];
+              dr[3 * i + d] += pose[3 + d];
+              dr[3 * j + d] += pose[6 + d];
+            }
+          tm.sync();
+        }
+      }
+    }
+  pe.stop(tm, PH_GX_INTER);
   // ---- Hlab = RF H: rotation terms, then dU/dH in the molecule frame
   for (int i = 0; i < nmol; i++) {
     const RotState mr = y.molrot(i);
@@ -423,7 +539,9 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
     tm.sync();
     solve_direct_T(tm, T, c.tv, sc, y.ts(s), lamF(s), lamH(s), muF(s), muH(s));
   }
-  const double tol2 = 1e-28;
+  PhaseClock pt{y.tph, 0};
+  pt.start(tm);
+  const double tol2 = c.prm.exact_tol * c.prm.exact_tol;
   bool conv = false;
   for (int sweep = 0; sweep < c.prm.max_pol_rounds && !conv; sweep++) {
     double dn = 0.0, nn = 0.0;
@@ -458,6 +576,19 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
           V.in[1] = wH; V.out[1] = oH; V.useF[1] = false;
           pair_apply_multi(tm, T, sc, X, V, false);
           for (int k = tm.rank; k < NP2; k += tm.size) { nF[k] += wgt(k) * oF[k]; nH[k] += wgt(k) * oH[k]; }
+          tm.sync();
+        } else if (c.tv.nslot && num_entry(c.tv, y.ts(u), v - mo) >= 0) {
+          // numeric, precomputed: N^T restricted to the rows of degree < p
+          const double *NF = c.tv.Nmat + (size_t)c.tv.nslot[num_entry(c.tv, y.ts(u), v - mo)] * 2 * NP2 * NP2;
+          const double *NH = NF + (size_t)NP2 * NP2;
+          const double *mF = muF(u), *mH = muH(u);
+          for (int j = tm.rank; j < NP2; j += tm.size) {
+            double sF = 0.0, sH = 0.0;
+            for (int k = 0; k < pF * pF; k++) sF += NF[(size_t)k * NP2 + j] * mF[k];
+            for (int k = 0; k < pH * pH; k++) sH += NH[(size_t)k * NP2 + j] * mH[k];
+            nF[j] += sF;
+            nH[j] += sH;
+          }
           tm.sync();
         } else {
           // numeric: the expansion at u of v's surface charges q = dA W c_n E . Y
@@ -495,6 +626,9 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
     }
     conv = !(dn > tol2 * nn);
   }
+  pt.stop(tm, PH_GX_ANALYTIC);
+  PhaseClock ps{y.tph, 0};
+  ps.start(tm);
   // ---- stage 2: LS = RB(sum over interPol neighbours T(u <- s2) Hrot_s2)
   for (int u = 0; u < S; u++) {
     if (!polarized(y, u)) continue;
@@ -569,6 +703,7 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
     if (!bv.interX[(size_t)b * nmol + i] || (y.nipol(s) == 0 && y.niact(s) == 0)) continue;
     add_rot_grad(tm, y, i, gHsr(s), y.HselfRot(s), 1.0, t2);
   }
+  ps.stop(tm, PH_GX_NUMERIC);
   return conv;
 }
 

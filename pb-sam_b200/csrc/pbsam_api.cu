@@ -199,6 +199,8 @@ extern "C" void pbsam_params_default(pbsam_params *p)
   p->cluster_size = 0;
   p->exact = 0;
   p->box_length = 0.0;
+  p->exact_tables = 1;
+  p->exact_tol = 1e-14;
 }
 
 static double kappa_of(const pbsam_params &p)
@@ -215,6 +217,8 @@ extern "C" int pbsam_context_create(const pbsam_params *prm, int device, pbsam_c
   if (prm->cluster_size < -1 || prm->cluster_size > PBSAM_MAX_CREW)
     return fail(PBSAM_E_BADARG, "cluster_size must be -1 (adaptive), 0 (automatic) or 1..16");
   if (prm->exact != 0 && prm->exact != 1) return fail(PBSAM_E_BADARG, "exact must be 0 or 1");
+  if (prm->exact_tables != 0 && prm->exact_tables != 1) return fail(PBSAM_E_BADARG, "exact_tables must be 0 or 1");
+  if (!(prm->exact_tol > 0.0 && prm->exact_tol < 1.0)) return fail(PBSAM_E_BADARG, "exact_tol must be in (0, 1)");
   if (!(prm->box_length >= 0.0) || !std::isfinite(prm->box_length))
     return fail(PBSAM_E_BADARG, "box_length must be 0 (no periodic box) or a positive edge");
   if (prm->exact && prm->poles > 32) return fail(PBSAM_E_BADARG, "the exact form supports pole orders up to 32");
@@ -553,10 +557,69 @@ static int set_smem_attrs(int NP)
   CK(cudaFuncSetAttribute(pbsam_setup2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   CK(cudaFuncSetAttribute(pbsam_setup3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   CK(cudaFuncSetAttribute(pbsam_selfpol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(pbsam_nummat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   return PBSAM_OK;
 }
 
 // upload all molecule types and run the per-type setup kernels
+// Exact form: the numeric near-field operators of every intra near pair that
+// re-expands numerically (pbsam_nummat_kernel), when they fit in 4 GB; tv.nslot and
+// tv.Nmat stay null otherwise and the kernels evaluate those pairs from the surface
+// charges.  A pair that the device classifies otherwise than this host test (a
+// separation within rounding of 0 or min_sep_numeric) falls back the same way.
+static int build_numeric_operators(std::vector<void *> &B, pbsam_context *c, TypeView &tv, Ctx cx, int NP,
+                                   const std::vector<int> &type_off, const std::vector<int> &near_off,
+                                   const std::vector<int> &near, const std::vector<int> &spx_off,
+                                   const std::vector<double> &cen, const std::vector<double> &rad)
+{
+  const long long NP2 = (long long)NP * NP;
+  const int TS = type_off.back();
+  std::vector<int> nslot(near.size(), -1), slot_e, slot_u;
+  int maxpts = 1;
+  for (int ts = 0, t = 0; ts < TS; ts++) {
+    while (type_off[t + 1] <= ts) t++;
+    for (int e = near_off[ts]; e < near_off[ts + 1]; e++) {
+      const int v = type_off[t] + near[e];
+      const double P[3] = {cen[3 * ts] - cen[3 * v], cen[3 * ts + 1] - cen[3 * v + 1], cen[3 * ts + 2] - cen[3 * v + 2]};
+      const double sep = std::sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]) - rad[ts] - rad[v];
+      if (sep > 0 && !(sep < c->prm.min_sep_numeric)) continue;
+      nslot[e] = (int)slot_e.size();
+      slot_e.push_back(e);
+      slot_u.push_back(ts);
+      maxpts = std::max(maxpts, spx_off[v + 1] - spx_off[v]);
+    }
+  }
+  const size_t per = (size_t)2 * NP2 * NP2 * sizeof(double);
+  if (slot_e.empty() || per * slot_e.size() > (4ULL << 30)) return PBSAM_OK;
+  double *N = nullptr;
+  TRY(dalloc(B, &N, slot_e.size() * 2 * NP2 * NP2));
+  const int *dslot = nullptr, *de = nullptr, *du = nullptr;
+  TRY(dput(B, &dslot, nslot));
+  std::vector<void *> tmp;
+  auto release = [&]() { for (void *q : tmp) cudaFree(q); };
+  int r = dput(tmp, &de, slot_e);
+  if (!r) r = dput(tmp, &du, slot_u);
+  const int CH = 256, ns = (int)slot_e.size();
+  const long long stride = scr_doubles(NP, 1), qstride = 2 * ((maxpts + 1) & ~1LL);
+  double *scr = nullptr, *qw = nullptr;
+  if (!r) r = dalloc(tmp, &scr, (size_t)stride * CH);
+  if (!r) r = dalloc(tmp, &qw, (size_t)qstride * CH);
+  if (r) { release(); return r; }
+  tv.Nmat = N;
+  tv.nslot = dslot;
+  cx.tv = tv;
+  cudaError_t e = cudaSuccess;
+  for (int s0 = 0; e == cudaSuccess && s0 < ns; s0 += CH) {
+    const int n = ns - s0 < CH ? ns - s0 : CH;
+    pbsam_nummat_kernel<<<n, PBSAM_TEAM, team_smem_bytes(NP)>>>(cx, de, du, s0, n, scr, stride, qw, qstride, N);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  }
+  release();
+  if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("numeric near-field operators: ") + cudaGetErrorString(e));
+  return PBSAM_OK;
+}
+
 static int finalize_types(pbsam_context *c)
 {
   if (c->finalized) return PBSAM_OK;
@@ -689,6 +752,7 @@ static int finalize_types(pbsam_context *c)
     cudaFree(derr);
     if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("exact-form operators: ") + cudaGetErrorString(e));
     if (herr) return fail(PBSAM_E_BADARG, "a sphere's inner fixed point is singular; the exact form cannot be used");
+    if (c->prm.exact_tables) TRY(build_numeric_operators(B, c, tv, cx, NP, type_off, near_off, near, spx_off, cen, rad));
   }
   c->finalized = true;
   return PBSAM_OK;
@@ -779,6 +843,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   p.max_pol_rounds = c->prm.max_pol_rounds; p.inter_cut = c->prm.inter_cutoff; p.interact_cut = c->prm.interact_cutoff;
   p.min_sep_numeric = c->prm.min_sep_numeric; p.idiel = c->prm.idiel; p.sdiel = c->prm.sdiel;
   p.exact = c->prm.exact;
+  p.exact_tol = c->prm.exact_tol;
   p.box = c->prm.box_length;
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);

@@ -309,7 +309,8 @@ __device__ __forceinline__ int intra_pair(const TypeView &tv, int ts, int ki, in
 }
 
 // rotate -> translate -> rotate back (src/xforms.cpp:122-132, 260-270); Mout zero-padded to NP
-__device__ void pair_apply(const Team &tm, const Tab &T, const Scr &sc, const PairXf &X, bool useF, const double *Min,
+template <class TM>
+__device__ void pair_apply(const TM &tm, const Tab &T, const Scr &sc, const PairXf &X, bool useF, const double *Min,
                            double *Mout)
 {
   const int p = useF ? X.pF : X.pH;
@@ -1391,21 +1392,54 @@ __device__ double recompute_from_self(const Team &tm, const Sys &y, int s)   // 
   return solve_surface(tm, y, s, true);
 }
 
-// intra near re-expansion with the latest values (src/molecule.cpp:1413-1473)
-__device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s)
+// y = (rows of degree < p of N) x, zero beyond (N: NP2 x NP2 row-major); a warp per row
+__device__ void num_apply(const Team &tm, const double *N, int p, const double *x, double *out, int NP2)
+{
+  const int lane = tm.rank & 31, w = tm.rank >> 5, nw = tm.size >> 5, rows = p * p;
+  for (int r = w; r < NP2; r += nw) {
+    double acc = 0.0;
+    if (r < rows) {
+      const double *row = N + (size_t)r * NP2;
+      for (int j = lane; j < NP2; j += 32) acc += row[j] * x[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    }
+    if (lane == 0) out[r] = acc;
+  }
+  tm.sync();
+}
+
+// intra near re-expansion with the latest values (src/molecule.cpp:1413-1473).
+// part 0: every near neighbour, LFS = sum, LHS = LS + sum.  The exact form splits the
+// sum: its sweeps update only the polarized spheres, so the terms of the other
+// neighbours (F, H and surface charges fixed for the whole solve) are summed once per
+// evaluation (part 1, into slots 0 and 1 of the sphere's gradient work set gLHN,
+// which the exact form does not use otherwise) and every sweep adds the polarized
+// neighbours' terms to them (part 2).
+__device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s, int part = 0)
 {
   const Tab &T = y.c->T;
   const int ts = y.ts(s), i = y.mol(s);
   const int mo = y.c->bv.mol_off[i];
   const int to = y.c->tv.type_off[y.c->bv.mol_type[i]];
   double *a = y.sc.E(7), *bq = y.sc.E(8);
-  tzero(tm, y.LFS(s), y.NP2);
-  tcopy(tm, y.LHS(s), y.LS(s), y.NP2);
+  double *LF = part == 1 ? y.gLHN(s) : y.LFS(s), *LH = part == 1 ? y.gLHN(s) + y.NP2 : y.LHS(s);
+  if (part == 1) {
+    tzero(tm, LF, y.NP2);
+    tzero(tm, LH, y.NP2);
+  } else if (part == 2) {
+    const double *cF = y.gLHN(s), *cH = y.gLHN(s) + y.NP2, *ls = y.LS(s);
+    for (int t = tm.rank; t < y.NP2; t += tm.size) { LF[t] = cF[t]; LH[t] = ls[t] + cH[t]; }
+  } else {
+    tzero(tm, LF, y.NP2);
+    tcopy(tm, LH, y.LS(s), y.NP2);
+  }
   tm.sync();
   const double *ci = y.cen(s);
   for (int e = y.c->tv.near_off[ts]; e < y.c->tv.near_off[ts + 1]; e++) {
     const int kj = y.c->tv.near[e];
     const int s2 = mo + kj;
+    if (part != 0 && (y.nipol(s2) > 0) != (part == 2)) continue;
     const double *cj = y.c->tv.cen + 3 * (to + kj);
     const double P[3] = {ci[0] - cj[0], ci[1] - cj[1], ci[2] - cj[2]};
     const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
@@ -1424,12 +1458,18 @@ __device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s)
       V.in[1] = y.H(s2); V.out[1] = bq; V.useF[1] = false;
       pair_apply_multi(tm, T, y.sc, X, V, false);
       pc.stop(tm, PH_INTRA);
+    } else if (part != 0 && y.c->tv.nslot && y.c->tv.nslot[e] >= 0) {
+      // the exact form's precomputed operators: the same map from F and H of s2
+      const double *NF = y.c->tv.Nmat + (size_t)y.c->tv.nslot[e] * 2 * y.NP2 * y.NP2;
+      num_apply(tm, NF, pF, y.F(s2), a, y.NP2);
+      num_apply(tm, NF + (size_t)y.NP2 * y.NP2, pH, y.H(s2), bq, y.NP2);
+      pc.stop(tm, PH_NUMERIC);
     } else {
       crew_numeric_expand2<1>(tm, y.cw, T, y.sc, y.spx(s2), y.npts(s2), P, y.rad(s),
                               NumSet{y.qF(s2), true, false, pF, a}, NumSet{y.qH(s2), true, true, pH, bq});
       pc.stop(tm, PH_NUMERIC);
     }
-    for (int t = tm.rank; t < y.NP2; t += tm.size) { y.LFS(s)[t] += a[t]; y.LHS(s)[t] += bq[t]; }
+    for (int t = tm.rank; t < y.NP2; t += tm.size) { LF[t] += a[t]; LH[t] += bq[t]; }
     tm.sync();
   }
 }
@@ -1437,8 +1477,10 @@ __device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s)
 __device__ double recompute(const Team &tm, const Sys &y, int s)             // src/molecule.cpp:1168-1229
 {
   const int ts = y.ts(s);
-  reexpand_LS(tm, y, s, false);
-  reexpand_intra_near(tm, y, s);
+  // the exact form computes LS once before its sweeps (its sources, the Hrot of the
+  // first round, stay fixed)
+  if (!y.c->prm.exact) reexpand_LS(tm, y, s, false);
+  reexpand_intra_near(tm, y, s, y.c->prm.exact ? 2 : 0);
   const double *LHf = y.c->tv.LHfar + (size_t)ts * y.NP2, *LFf = y.c->tv.LFfar + (size_t)ts * y.NP2;
   for (int i = tm.rank; i < y.NP2; i += tm.size) { y.LHS(s)[i] += LHf[i]; y.LFS(s)[i] += LFf[i]; }
   tm.sync();
@@ -1452,8 +1494,9 @@ __device__ __noinline__ void grad_xform_from(const Team &tm, const Sys &y, int s
   double ci[3], cm[3];
   y.cen_lab(s, ci);
   y.cen_lab(sm, cm);
+  // prepareDTA takes the plain difference of the (wrapped) centres, no minimum image
+  // (src/molecule.cpp:1515, 1546, 1562, 1602, 1619)
   double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
-  min_image(y.c->prm.box, P);
   const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
   const double TQ = self ? y.c->tv.tHself[y.ts(sm)] : y.c->bv.tH[y.sc1(sm)];
   const int p = compute_order(y.NP, rho, TQ, y.rad(sm));
@@ -1470,8 +1513,7 @@ __device__ __forceinline__ int pair_order(const Sys &y, int s, int sm, bool self
   double ci[3], cm[3];
   y.cen_lab(s, ci);
   y.cen_lab(sm, cm);
-  double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
-  min_image(y.c->prm.box, P);
+  double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};   // as grad_xform_from
   const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
   const double TQ = self ? y.c->tv.tHself[y.ts(sm)] : y.c->bv.tH[y.sc1(sm)];
   return compute_order(y.NP, rho, TQ, y.rad(sm));
@@ -1485,8 +1527,7 @@ __device__ __noinline__ void grad_xform_warp(const WarpTeam &tw, const Sys &y, c
   double ci[3], cm[3];
   y.cen_lab(s, ci);
   y.cen_lab(sm, cm);
-  double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};
-  min_image(y.c->prm.box, P);
+  const double P[3] = {ci[0] - cm[0], ci[1] - cm[1], ci[2] - cm[2]};   // as grad_xform_from
   const int p = pair_order(y, s, sm, self);
   PairXf X;
   prep_pair(tw, T, ws, P, p, 0, y.rad(sm), y.rad(s), true, X);
@@ -1897,6 +1938,16 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
       return;
     }
   }
+  // with a periodic box the molecule centres are wrapped into it as CMolecule::setPos
+  // does (src/molecule.h:325): pair distances take the minimum image, but the
+  // reference's energy and prepareDTA use the plain difference of the wrapped centres
+  if (c.prm.box > 0.0) {
+    for (int t = tm.rank; t < nmol * 3; t += tm.size) {
+      double *v = const_cast<double *>(bv.pos) + (size_t)b * nmol * 3 + t;   // the system's own pose buffer
+      *v = *v - c.prm.box * round(*v / c.prm.box);
+    }
+    tm.sync();
+  }
   // sphere centres for this pose (CMolecule::rotate / rotateCenters)
   for (int s = tm.rank; s < S; s += tm.size) {
     const double *q = bv.quat + 4 * ((size_t)b * nmol + y.mol(s));
@@ -2028,11 +2079,21 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
     }
     for (int i = 0; i < nmol; i++) if (maxdevs[i] > MAXDEV) MAXDEV = maxdevs[i];
   }
+  // the exact form, once before its sweeps: the inter-molecular LS (its sources, the
+  // rotated H of the first round, are not updated by the sweeps) and the near terms of
+  // the neighbours the sweeps leave fixed
+  if (c.prm.exact)
+    for (int i = 0; i < nmol; i++)
+      if (bv.interX[(size_t)b * nmol + i])
+        for (int s = bv.mol_off[i]; s < bv.mol_off[i + 1]; s++)
+          if (y.nipol(s) > 0) {
+            reexpand_LS(tm, y, s, false);
+            reexpand_intra_near(tm, y, s, 1);
+          }
   int ct = 1;
   const double itot = (mtotal > 0 ? 1.0 / mtotal : 0);
-  // the exact form sweeps to the fixed point whatever max_polar_dev says
-  const double tol2 = c.prm.exact ? fmin(c.prm.max_polar_dev * c.prm.max_polar_dev, 1e-28)
-                                  : c.prm.max_polar_dev * c.prm.max_polar_dev;
+  // the exact form sweeps to the fixed point (exact_tol) whatever max_polar_dev says
+  const double tol2 = c.prm.exact ? c.prm.exact_tol * c.prm.exact_tol : c.prm.max_polar_dev * c.prm.max_polar_dev;
   while (dev * itot > tol2 && ct < c.prm.max_pol_rounds) {
     dev = 0.0;
     double maxdevs[32];
@@ -2290,7 +2351,9 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_energy_kernel(Ctx c, int lab
             const double *cj = lab ? y.cenRot(sj) : y.cen(sj);
             double P[3] = {(pi[0] + ci[0]) - (pj[0] + cj[0]), (pi[1] + ci[1]) - (pj[1] + cj[1]),
                            (pi[2] + ci[2]) - (pj[2] + cj[2])};
-            min_image(c.prm.box, P);
+            // the reference's energy takes the plain difference of the wrapped centres
+            // (src/molecule.cpp:1873); the lab-frame form the minimum image
+            if (lab) min_image(c.prm.box, P);
             const double rho = sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
             const int pi2j = compute_order(y.NP, rho, bv.tH[y.sc1(si)], y.rad(si));
             const int pj2i = compute_order(y.NP, rho, bv.tH[y.sc1(sj)], y.rad(sj));
@@ -2620,6 +2683,62 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup3_kernel(Ctx c, int e0,
   tm.sync();
   trans_compute(tm, T, S.rho, 0.0, NP, tv.rad[tj], tv.rad[ts], false, ts1, TH, nullptr, kbuf);
   for (int i = tm.rank; i < tr_off(NP); i += tm.size) tv.pTF[(size_t)e * tr_off(NP) + i] = TH[i];
+}
+
+
+// Numeric near-field operators of the exact form.  For intra near entry e (target type
+// sphere u, source v = near[e]) whose pair re-expands numerically, the full-order maps
+// LF_u += N_F F_v and LH_u += N_H H_v (NP2 x NP2, row-major): column j is the numeric
+// expansion about u (numeric_expand2) of the surface charges (surface_q2) of a unit
+// F_j (H_j) of v.  Both steps are linear in the coefficients and a truncation order p
+// of the forward only drops output degrees >= p, so the rows of degree < p of N give
+// the forward's expansion at that order.  One CTA per slot.
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_nummat_kernel(Ctx c, const int *slot_e, const int *slot_u, int s0,
+                                                                  int ns, double *scr, long long stride, double *qw,
+                                                                  long long qstride, double *Nmat)
+{
+  extern __shared__ double2 dsm[];
+  __shared__ double red[PBSAM_TEAM];
+  const Team tm{(int)threadIdx.x, (int)blockDim.x};
+  const int k = blockIdx.x;
+  if (k >= ns) return;
+  const Tab &T = c.T;
+  const TypeView &tv = c.tv;
+  const int NP = T.NP, NP2 = NP * NP;
+  const int slot = s0 + k, e = slot_e[slot], u = slot_u[slot];
+  Scr sc = make_scr(scr + (size_t)k * stride, NP, dsm);
+  int t = 0;
+  while (tv.type_off[t + 1] <= u) t++;
+  const int v = tv.type_off[t] + tv.near[e];
+  const double *cu = tv.cen + 3 * u, *cv = tv.cen + 3 * v;
+  const double P[3] = {cu[0] - cv[0], cu[1] - cv[1], cu[2] - cv[2]};
+  const double *pts = tv.spx + 3 * (size_t)tv.spx_off[v];
+  const int npt = tv.spx_off[v + 1] - tv.spx_off[v];
+  const double dA = 4 * PB_PI / double(tv.nspx[v]);
+  const double *cstv = tv.cst + (size_t)v * CST_N * NP;
+  double *unit = sc.E(12), *outF = sc.E(10), *outH = sc.E(11);
+  double *qF = qw + (size_t)k * qstride, *qH = qF + qstride / 2;
+  double *NF = Nmat + (size_t)slot * 2 * NP2 * NP2, *NH = NF + (size_t)NP2 * NP2;
+  tzero(tm, unit, NP2);
+  tm.sync();
+  for (int j = 0; j < NP2; j++) {
+    if (tm.rank == 0) {
+      unit[j] = 1.0;
+      if (j > 0) unit[j - 1] = 0.0;
+    }
+    tm.sync();
+    double t1[1], t2[1];
+    surface_q2<1>(tm, T, sc, pts, npt, dA, unit, T.CONST2, qF, unit, cstv + CST_CHGH * NP, qH, 0, 1, t1, t2, red);
+    tm.sync();
+    numeric_expand2<1>(tm, T, sc, pts, npt, P, tv.rad[u], NumSet{qF, true, false, NP, outF},
+                       NumSet{qH, true, true, NP, outH});
+    tm.sync();
+    for (int r = tm.rank; r < NP2; r += tm.size) {
+      NF[(size_t)r * NP2 + j] = outF[r];
+      NH[(size_t)r * NP2 + j] = outH[r];
+    }
+    tm.sync();
+  }
 }
 
 }  // namespace pbsam

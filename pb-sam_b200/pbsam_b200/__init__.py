@@ -38,7 +38,8 @@ class pbsam_params(ctypes.Structure):
                 ("inter_cutoff", ctypes.c_double), ("interact_cutoff", ctypes.c_double),
                 ("intra_cutoff", ctypes.c_double), ("min_sep_numeric", ctypes.c_double),
                 ("num_points_x", ctypes.c_int), ("cluster_size", ctypes.c_int), ("exact", ctypes.c_int),
-                ("box_length", ctypes.c_double)]
+                ("box_length", ctypes.c_double), ("exact_tables", ctypes.c_int),
+                ("exact_tol", ctypes.c_double)]
 
 
 PBSAM_BD_NAM = 0

@@ -10,7 +10,9 @@ negative gradient of the lab-frame energy by the adjoint.  Checked:
     h = 1e-3 A and 1e-4 rad (1e-6 relative), every perturbed pose one system of a
     batch;
   * compute_forces = -dU/dpos and -dU/domega, and dU/dquat along a tangent direction;
-  * an 8-molecule case (40 spheres each, p = 10) against central differences.
+  * an 8-molecule case (40 spheres each, p = 10) against central differences;
+  * the precomputed numeric near-field operators against their evaluation from the
+    surface charges.
 The reference's own forces (per-coordinate gradient solves) are printed beside the
 adjoint's, not gated: they differentiate a different function (the reference's
 energy ignores the orientation, and its sweeps stop short of the fixed point).
@@ -69,10 +71,10 @@ def fd_grad(E, n):
     return (E[:, :, 0] - E[:, :, 1]) / (2 * H_POS), (E[:, :, 2] - E[:, :, 3]) / (2 * H_ROT)
 
 
-def exact_ctx(case):
+def exact_ctx(case, **kw):
     import pbsam_b200 as pb
     P = json.load(open(os.path.join(golden_dir(case), "poses.json")))
-    ctx = pb.CSystem(poles=P["poles"], salt=P["salt"], idiel=P["idiel"], exact=1, max_pol_rounds=400)
+    ctx = pb.CSystem(poles=P["poles"], salt=P["salt"], idiel=P["idiel"], exact=1, max_pol_rounds=400, **kw)
     d = golden_dir(case)
     types = [ctx.load_moltype(d + "/mol%s.pqr" % t, d + "/im" + t, d + "/exp" + t, "mol%s.0" % t) for t in "AB"]
     return ctx, types, P
@@ -131,6 +133,31 @@ def test_exact_backward_vs_oracle_and_central_differences(case, pose, tmp_path):
         ctx.close()
 
 
+@pytest.mark.parametrize("case", ["tiny", "cfg0"])
+def test_exact_tables_agree_with_surface_charges(case):
+    """The numeric near-field operators prepared once per type (exact_tables = 1) against
+    their evaluation from the surface charges at every use (0): every pose of the case,
+    forces, torques, lab-frame energy and the backward pass to 1e-11 relative."""
+    res = []
+    for tables in (1, 0):
+        ctx, types, P = exact_ctx(case, exact_tables=tables)
+        try:
+            fr = [frame_of(P, k) for k in range(len(P["poses"]))]
+            mol = ctx.molecules(types, n_systems=len(fr))
+            mol.set_poses(np.array([f[0] for f in fr]), np.array([f[1] for f in fr]))
+            f, t, st = mol.compute_forces()
+            assert np.all(st == 0), st
+            res.append((f, t, mol.compute_energy(lab=True), mol.stats()[:, 2].copy()))
+            mol.close()
+        finally:
+            ctx.close()
+    (f1, t1, e1, n1), (f0, t0, e0, n0) = res
+    assert np.sum(n1) > 0
+    ef, et, ee = rel(f1, f0), rel(t1, t0), rel(e1, e0)
+    print("%s: tables vs surface charges: force %.2e torque %.2e energy %.2e" % (case, ef, et, ee))
+    assert ef < 1e-11 and et < 1e-11 and ee < 1e-11, (ef, et, ee)
+
+
 def test_exact_reference_forces_reported():
     """The reference's forces (the plain drop-in: its per-coordinate gradient solves)
     beside the adjoint's, reported only."""
@@ -179,29 +206,34 @@ def test_exact_eight_molecules_central_differences():
     ctx = pb.CSystem(poles=10, salt=0.05, exact=1, max_pol_rounds=400)
     try:
         types = [ctx.create_moltype(*sp) for sp in specs]
-        ext = max(m.extent() for m in mols)
         quat = np.array([synth.random_quat(rng) for _ in range(8)])
-        ok = False
-        for spacing in np.arange(2 * ext - 8.0, 2 * ext + 30.0, 1.0):
-            pos = np.array([[x, y, z] for x in (0, 1) for y in (0, 1) for z in (0, 1)], float) * spacing
-            pos += rng.uniform(-1.0, 1.0, pos.shape)
-            ok = all(synth.min_gap((mols[a].centres, mols[a].radii), pos[a], quat[a], (mols[b].centres, mols[b].radii),
-                                   pos[b], quat[b]) > 1.0 for a in range(8) for b in range(a + 1, 8))
-            if ok:
+        jitter = rng.uniform(-1.0, 1.0, (8, 3))
+        corners = np.array([[x, y, z] for x in (0, 1) for y in (0, 1) for z in (0, 1)], float)
+        # the tightest cube (0.5 A steps) whose molecules keep every gap above 1.5 A: the
+        # molecules are elongated (extents 31-47 A), so several pairs sit inside the
+        # 10 A polarization cutoff
+        gaps = None
+        for spacing in np.arange(10.0, 120.0, 0.5):
+            pos = corners * spacing + jitter
+            gaps = [synth.min_gap((mols[a].centres, mols[a].radii), pos[a], quat[a], (mols[b].centres, mols[b].radii),
+                                  pos[b], quat[b]) for a in range(8) for b in range(a + 1, 8)]
+            if min(gaps) > 1.5:
                 break
-        assert ok
+        assert min(gaps) > 1.5 and sum(g < 10.0 for g in gaps) >= 2, gaps
         Pb, Qb = fd_batch(pos, quat)
         mol = ctx.molecules(types, n_systems=len(Pb))
-        mol.set_poses(Pb, Qb)
-        f, t, st = mol.compute_forces()
-        assert np.all(st == 0), st
-        assert mol.stats()[0, 2] > 0, "neighbours must polarize"
-        E = mol.compute_energy(lab=True)
-        dp, dq, dr = mol.backward()
-        fdp, fdr = fd_grad(E, 8)
-        ep, er = rel(dp[0], fdp), rel(dr[0], fdr)
-        print("8 molecules: backward vs central differences %.2e (pos) %.2e (rot)" % (ep, er))
-        assert ep < 1e-6 and er < 1e-6, (ep, er)
-        mol.close()
+        try:
+            mol.set_poses(Pb, Qb)
+            f, t, st = mol.compute_forces()
+            assert np.all(st == 0), st
+            assert mol.stats()[0, 2] > 0, "neighbours must polarize"
+            E = mol.compute_energy(lab=True)
+            dp, dq, dr = mol.backward()
+            fdp, fdr = fd_grad(E, 8)
+            ep, er = rel(dp[0], fdp), rel(dr[0], fdr)
+            print("8 molecules: backward vs central differences %.2e (pos) %.2e (rot)" % (ep, er))
+            assert ep < 1e-6 and er < 1e-6, (ep, er)
+        finally:
+            mol.close()
     finally:
         ctx.close()

@@ -1,14 +1,19 @@
 """The periodic box (pbsam_params.box_length) against the reference with its box on.
 
 bdm runs the reference with CSystem::initConstants(kappa, sdiel, T, true, L)
-(src/BDmulti_main.cpp:67): every displacement between molecules goes through
-CSystem::pbcPos (src/system.cpp:46-55) and moves wrap positions into the box.  The
-reference's own harnesses take a `box` entry; the GPU must reproduce them:
-  * forces, torques and energy of a pose whose molecules interact only across a face
-    of the box (1e-8 relative), and the same numbers as the unwrapped pose without a
-    box;
+(src/BDmulti_main.cpp:67).  CMolecule::setPos and translate wrap the molecule centres
+into the box (src/molecule.h:325-327); the pair lists, the polarization
+re-expansions, reexpandGrad, the collision tests and the BD distances take the
+minimum image of each displacement (CSystem::pbcPos, src/system.cpp:46-55), while
+prepareDTA (src/molecule.cpp:1515-1619) and the energy (src/molecule.cpp:1873) take
+the plain difference of the wrapped centres.  The plain drop-in reproduces that; the
+lab-frame energy takes the minimum image everywhere.  Against the reference's own
+harnesses with a `box` entry:
+  * forces, torques and energy of a pose whose molecules meet only across a face of
+    the box (1e-8 relative); the lab-frame energy equal to that of the same pose
+    unwrapped without a box;
   * multi-molecule BD steps with the reference's noise stream against CBDmulti,
-    molecules straddling the box faces (positions 1e-9 A).
+    molecules straddling the box faces, one carried through a face (positions 1e-9 A).
 """
 import json
 import os
@@ -48,10 +53,12 @@ def test_pbc_forces_across_the_box_face(tmp_path):
     P = json.load(open(os.path.join(golden_dir("tiny"), "poses.json")))
     fr = P["poses"][0]["frame"]
     pa, pb_ = np.array(fr[0]["pos"]), np.array(fr[1]["pos"])
-    # molecule A near the -x face, B's image one box length away: they meet only across the face
-    shift = np.array([-L / 2 + 9.0, 0.0, 0.0]) - pa
+    # A 2 A inside the -x face; B (5 A further in -x) lies beyond it and is wrapped to the
+    # +x side: the two meet only across the face
+    shift = np.array([-L / 2 + 2.0, 0.0, 0.0]) - pa
     a = pa + shift
-    b = pb_ + shift + np.array([L, 0.0, 0.0])
+    b = pb_ + shift
+    assert b[0] < -L / 2
     frame = [(0, list(a), fr[0]["quat"]), (1, list(b), fr[1]["quat"])]
     ref = _ref_forces(str(tmp_path), P, frame, L)
     assert ref["ok"]
@@ -67,12 +74,17 @@ def test_pbc_forces_across_the_box_face(tmp_path):
         e = m.compute_energy()
         assert st[0] == 0 and m.stats()[0, 2] > 0, "the pose must polarize across the face"
         assert rel(f[0], ref["force"]) < 1e-8 and rel(t[0], ref["torque"]) < 1e-8, (rel(f[0], ref["force"]),)
-        assert abs(e[0] - ref["energy"]) <= 1e-8 * abs(ref["energy"])
-        # the same geometry unwrapped, without a box
+        # the energy takes the plain difference of the wrapped centres (B wrapped as
+        # setPos does, 65 A from A) where the forces see the 17 A minimum image
+        assert abs(e[0] - ref["energy"]) <= 1e-8 * abs(ref["energy"]), (e[0], ref["energy"])
+        # the same geometry unwrapped, without a box: the polarization is the same, so
+        # the lab-frame energy (minimum image) is too
         mp = plain.molecules(ptypes, 1)
         mp.set_poses(np.array([[pa, pb_]]), np.array([[fr[0]["quat"], fr[1]["quat"]]]))
         f2, t2, st2 = mp.compute_forces()
-        assert st2[0] == 0 and rel(f[0], f2[0]) < 1e-9 and rel(t[0], t2[0]) < 1e-9
+        assert st2[0] == 0
+        el, el2 = m.compute_energy(lab=True), mp.compute_energy(lab=True)
+        assert abs(el[0] - el2[0]) <= 1e-9 * abs(el2[0]), (el[0], el2[0])
         m.close()
         mp.close()
     finally:
@@ -82,16 +94,20 @@ def test_pbc_forces_across_the_box_face(tmp_path):
 
 def test_pbc_bdm_vs_reference(tmp_path):
     """Three molecules straddling the faces of the box, the reference's noise stream:
-    six CBDmulti steps (moves wrap into the box)."""
+    six CBDmulti steps, one of which carries a molecule through a face (moves wrap
+    into the box)."""
     import pbsam_b200 as pb
     exe = oracle.ref_bdm_harness()
     if exe is None:
         pytest.skip("reference BD harness not built")
     fr = gap5_frame()
     posb = np.array(fr[1][1])
-    a = np.array([-L / 2 + 4.0, 1.0, 0.0])
-    # A near the -x face with B beside it; C near the +x face, nearest to A through the face
-    frame = [(0, list(a), fr[0][2]), (1, list(a + posb), fr[1][2]), (0, [L / 2 - 20.0, -3.0, 2.0], [0.5, 0.5, -0.5, 0.5])]
+    a = np.array([-L / 2 + 0.02, 1.0, 0.0])
+    # A on the -x face (it wraps to the +x side in the second step) with B beside it; C near
+    # the +x face, nearest to A through the face.  CBDmulti holds the copies of species 0
+    # first (src/BDmulti.cpp constructor), so C (species 0) comes before B.
+    frame = [(0, list(a), fr[0][2]), (0, [L / 2 - 20.0, -3.0, 2.0], [0.5, 0.5, -0.5, 0.5]),
+             (1, list(a + posb), fr[1][2])]
     ctx, types, P = tiny_ctx(box_length=L)
     dtr, drot = (0.015, 0.015, 0.015), (4.5e-5, 4.5e-5, 4e-5)
     spec = os.path.join(str(tmp_path), "m.txt")
@@ -112,6 +128,7 @@ def test_pbc_bdm_vs_reference(tmp_path):
             ref[-1]["pos"].append(v[:3])
             ref[-1]["quat"].append(v[3:])
     assert len(ref) == 6 and ref[-1]["fevals"] > 0
+    assert ref[0]["pos"][0][0] < 0 < ref[-1]["pos"][0][0], "A must wrap through the -x face"
     mol = ctx.molecules([types[m[0]] for m in frame], n_systems=1)
     mol.set_poses(np.array([[m[1] for m in frame]]), np.array([[m[2] for m in frame]]))
     mol.bd_init(dtr, drot, mode=pb.PBSAM_BD_MULTI, seed=777, noise=pb.PBSAM_BD_NOISE_DRAND48)
