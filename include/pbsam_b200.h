@@ -87,16 +87,22 @@ typedef struct pbsam_params {
                              energy (src/molecule.cpp:1873) take the plain difference of the
                              wrapped centres, as the reference does.  The lab-frame energy and
                              the exact form take the minimum image everywhere. */
-  int exact_tables;       /* exact form only.  1 (default): the numeric near-field re-expansions
-                             of each molecule type's overlapping sphere pairs are prepared once
-                             as p^2 x p^2 operators when they fit in 4 GB (p = 10: about 32 MB
-                             per 35-sphere type) and applied as products in the sweeps and in
-                             the backward pass; 0: evaluated from the surface charges each time.
-                             The two agree to rounding. */
+  int exact_tables;       /* exact form only.  1 (default): the intra-molecular near-field
+                             re-expansions of each molecule type (numeric for overlapping sphere
+                             pairs, rotation + translation for the others) are prepared once as
+                             full-order p^2 x p^2 operators when they fit in 4 GB (else those of
+                             the numeric pairs alone when they fit; p = 10: about 150 MB per
+                             35-sphere type) and applied as products in the sweeps and in the
+                             backward pass; 0: transformed as the plain drop-in does.  The two
+                             agree to rounding. */
   double exact_tol;       /* exact form only: the sweeps, and the backward pass's transposed
                              sweeps, stop once the root-mean-square relative change of the
                              polarized spheres' H (their adjoint) is below it.  Default 1e-14;
                              the error of the state, and so of the forces, is of this order. */
+  double exact_relax;     /* exact form only: the sweeps' updates (after the first round) and the
+                             transposed sweeps' are over-relaxed by this factor in (0, 2),
+                             x += w (x_swept - x).  Default 1 (plain Gauss-Seidel); the fixed
+                             point does not depend on it, the number of sweeps does. */
 } pbsam_params;
 
 typedef struct pbsam_context pbsam_context;
@@ -308,6 +314,37 @@ int pbsam_selfpol(pbsam_context *ctx, int type_id, int max_rounds, double *fself
  * the denominators of the force kernel's roofline, whose IMat rows stay in L2 and whose
  * arithmetic is FP64. */
 int pbsam_device_peaks(int device, double *fp64_tflops, double *l2_gbs);
+
+/* Single-expansion operations, batched, with the semantics of the reference's
+ * rotation, translation and re-expansion classes, for callers that drive expansions
+ * one by one (the CRotCoeff / CTransCoeff / CXFormA classes of
+ * pb-sam_b200/cpp/pbsam_b200.hpp).  n items; in, out: [n][poles^2] packed real
+ * expansions (degrees >= p of in are ignored, those of out are zero); host pointers
+ * (on_device = 0) or device pointers of the context's device (1).  One CTA per item. */
+
+/* CRotCoeff::reset(theta, phi, xi, p) (src/rotcoeff.cpp:155-171) then rotate
+ * (with_xi = 0, src/rotcoeff.cpp:357-441) or rotateWithXi (with_xi = 1, :250-350), forward
+ * (1) or back (0).  rot: [n][3] = theta, phi, xi. */
+int pbsam_expan_rotate(pbsam_context *c, int n, const double *rot, int p, int with_xi, int forward,
+                       const double *in, double *out, int on_device);
+
+/* CTransCoeff::reset(rho, kappa, p, scalei, scaleo) (src/transcoeff.cpp:172-203) then
+ * translate (deriv = 0, :211-286) or dTranslate (deriv = 1, :294-364), with the context's
+ * kappa (screened = 1) or 0.  args: [n][3] = rho > 0, scale in, scale out. */
+int pbsam_expan_translate(pbsam_context *c, int n, const double *args, int p, int screened, int deriv,
+                          const double *in, double *out, int on_device);
+
+/* CXFormA(source, target).reset(P, p) then xformH (screened = 1, src/xforms.cpp:122-132)
+ * or xformF (0, :260-270); grad (nullable, screened only): [n][3][poles^2], the x, y, z
+ * derivatives w.r.t. the target position (CGradExpan, src/xforms.cpp:85-115).  args:
+ * [n][5] = P = target centre - source centre (3), source scale, target scale (the
+ * spheres' radii). */
+int pbsam_expan_reexpand(pbsam_context *c, int n, const double *args, int p, int screened, const double *in,
+                         double *out, double *grad, int on_device);
+
+/* CRotCoeff::reset(const CQuat &, p)'s Euler angles (theta, phi, xi) of a quaternion
+ * (w, x, y, z), normalised first (src/rotcoeff.cpp:181-201). */
+int pbsam_quat_angles(const double *q, double *angles);
 
 /* Text of the last error on the calling thread. */
 const char *pbsam_last_error(void);

@@ -99,6 +99,23 @@ def liboracle():
     return _lib
 
 
+def expan_op(np_, kappa, op, args, p, f1, f2, x, grad=False):
+    """The oracle's single-expansion operations (pbsam_oracle_expan): op 0 rotate,
+    1 translate, 2 re-expand; x [n][np_^2].  Returns out (and the gradient [n][3][np_^2])."""
+    lib = liboracle()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    a = np.ascontiguousarray(args, dtype=np.float64)
+    n = x.shape[0]
+    out = np.zeros_like(x)
+    g = np.zeros((n, 3, np_ * np_)) if grad else None
+    r = lib.pbsam_oracle_expan(ctypes.c_int(np_), ctypes.c_double(kappa), ctypes.c_int(op), ctypes.c_int(n), _dp(a),
+                               ctypes.c_int(p), ctypes.c_int(f1), ctypes.c_int(f2), _dp(x), _dp(out),
+                               _dp(g) if grad else None)
+    if r != 0:
+        raise RuntimeError("pbsam_oracle_expan failed")
+    return (out, g) if grad else out
+
+
 def write_spec(path, moltypes, frames, salt=0.05, idiel=4.0, poles=10, tol=DEFAULT_TOL, dump=0, energy=1,
                backward=0, nograd=0, exact=0, potpoints=(), potlab=0):
     """moltypes: list of (pqr, imatdir, expdir, expname); frames: list of lists

@@ -2702,3 +2702,58 @@ extern "C" void pbsam_oracle_philox(unsigned long long *c, unsigned long long k0
 {
   orc::System::philox(c, k0, k1);
 }
+
+// Single-expansion operations (the tests of the CUDA pbsam_expan_* entry points):
+// op 0 rotate (Rot::reset(theta, phi, xi) + rotate, or rotate_xi when f1; forward when f2;
+// src/rotcoeff.cpp:155-171, 250-441), op 1 translate (Trans::reset with kappa or 0 when
+// f1 is 0, translate or its derivative when f2; src/transcoeff.cpp:172-364), op 2
+// re-expand (XForm::reset + xformH, or reset_intra + xformF when f1 is 0, with the
+// gradient xformH_grad when grad is given; src/xforms.cpp:50-132, 213-270).  args as
+// the CUDA entry points; in, out [n][np^2], grad [n][3][np^2].
+extern "C" int pbsam_oracle_expan(int np, double kappa, int op, int n, const double *args, int p, int f1, int f2,
+                                  const double *in, double *out, double *grad)
+{
+  using namespace orc;
+  if (np < 1 || p < 1 || p > np || op < 0 || op > 2) return 1;
+  Tables T;
+  T.init(np, kappa);
+  const int NP2 = np * np;
+  auto put = [&](const vec &v, double *dst) {
+    for (int k = 0; k < NP2; k++) dst[k] = k < (int)v.size() ? v[k] : 0.0;
+  };
+  for (int i = 0; i < n; i++) {
+    const vec x(in + (size_t)i * NP2, in + (size_t)(i + 1) * NP2);
+    vec y;
+    if (op == 0) {
+      const double *a = args + 3 * (size_t)i;
+      Rot R;
+      R.reset(T, a[0], a[1], a[2], p, false);
+      if (f1) R.rotate_xi(x, y, p, f2 != 0);
+      else R.rotate(x, y, p, f2 != 0);
+    } else if (op == 1) {
+      const double *a = args + 3 * (size_t)i;
+      Trans Tr;
+      Tr.init_scale(np, a[1], a[2]);
+      Tr.reset(T, a[0], f1 ? T.kappa : 0.0, p, f2 != 0);
+      Tr.translate(x, y, f2 != 0);
+    } else {
+      const double *a = args + 5 * (size_t)i;
+      const P3 P(a[0], a[1], a[2]);
+      XForm X;
+      if (f1) {
+        X.reset(T, P, p, a[3], a[4], grad != nullptr);
+        X.xformH(x, y);
+        if (grad) {
+          vec G[3];
+          X.xformH_grad(x, G);
+          for (int c = 0; c < 3; c++) put(G[c], grad + ((size_t)i * 3 + c) * NP2);
+        }
+      } else {
+        X.reset_intra(T, P, p, p, a[3], a[4]);
+        X.xformF(x, y);
+      }
+    }
+    put(y, out + (size_t)i * NP2);
+  }
+  return 0;
+}

@@ -12,6 +12,12 @@
 //   CMolecule::computeForces(mols, force, torque)        src/molecule.h:179 (false on overlap)
 //   CMolecule::computeTotalIntEnergy(mols)               src/molecule.h:180
 //
+// and the expansion classes a driver uses around them: CExpan / CMulExpan /
+// CLocalExpan (src/expansion.h:96-494), CGradExpan (src/triexpan.h:253), CRotCoeff
+// (src/rotcoeff.h:10-266), CTransCoeff (src/transcoeff.h:9-182) and CXFormA
+// (src/xforms.h:58-104): host containers of packed expansions whose rotations,
+// translations and re-expansions run on the GPU through pbsam_expan_* (each call one
+// item; the *Batch functions send many at once).
 // Header-only; link with pb-sam_b200/lib/libpbsam_b200.so.  The solver state the
 // reference keeps in its molecules lives in one device system per list of
 // molecules (created by initMutualConstants, or by the first computeForces on
@@ -19,6 +25,7 @@
 // the reference does.  Errors are reported the reference's way (false / -1), with
 // the library's message on stderr; nothing exits the process.
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <map>
@@ -94,7 +101,15 @@ class CSystem {
     prm.idiel = idiel;
     const double *t = tolerances();
     prm.max_polar_dev = t[0]; prm.solve_tol = t[1]; prm.solve_max_ct = (int)t[2]; prm.max_pol_rounds = (int)t[3];
+    polesRef() = poles;
     return check(pbsam_context_create(&prm, device, &ctx()));
+  }
+  // the context's pole order (the reference's N_POLES)
+  static int poles() { return polesRef(); }
+  static int &polesRef()
+  {
+    static int p = 10;
+    return p;
   }
   // The reference's compile-time tolerances MAX_POLAR_DEV, SOLVE_TOL, SOLVE_MAX_CT,
   // MAX_POL_ROUNDS (src/molecule.cpp:6-13, src/expcenter.cpp:16-22); set before initConstants.
@@ -235,3 +250,220 @@ inline void CSystem::clear()
   if (ctx()) pbsam_context_destroy(ctx());
   ctx() = nullptr;
 }
+
+// ---------------------------------------------------------------- expansions
+// Packed real expansion of degrees < p (entries n^2, n^2 + 2m - 1, n^2 + 2m: the
+// m = 0 term, then Re and Im of m = 1..n) with its scale, as CExpan.
+class CExpan {
+ public:
+  explicit CExpan(int p = 0, double scale = 1.0) : m_scale(scale), m_c((size_t)p * p, 0.0) {}
+  CExpan(const std::vector<double> &c, double scale) : m_scale(scale), m_c(c)
+  {
+    const int p = order();
+    m_c.resize((size_t)p * p, 0.0);
+  }
+  int order() const { return (int)std::lround(std::sqrt((double)m_c.size())); }   // getRange().p2()
+  double getScale() const { return m_scale; }
+  void setScale(double s) { m_scale = s; }
+  void setOrder(int p) { m_c.resize((size_t)p * p, 0.0); }                        // setRange(p)
+  double &operator[](int i) { return m_c[i]; }
+  double operator[](int i) const { return m_c[i]; }
+  const std::vector<double> &coeffs() const { return m_c; }
+  // range union, as CExpan::operator+= (src/expansion.h:509-560)
+  CExpan &operator+=(const CExpan &o)
+  {
+    if (o.m_c.size() > m_c.size()) m_c.resize(o.m_c.size(), 0.0);
+    for (size_t i = 0; i < o.m_c.size(); i++) m_c[i] += o.m_c[i];
+    return *this;
+  }
+  CExpan &operator-=(const CExpan &o)
+  {
+    if (o.m_c.size() > m_c.size()) m_c.resize(o.m_c.size(), 0.0);
+    for (size_t i = 0; i < o.m_c.size(); i++) m_c[i] -= o.m_c[i];
+    return *this;
+  }
+  CExpan &operator*=(double s)
+  {
+    for (double &v : m_c) v *= s;
+    return *this;
+  }
+  // the coefficients zero-padded to the context's pole order (the C ABI's layout)
+  std::vector<double> padded(int NP) const
+  {
+    std::vector<double> v((size_t)NP * NP, 0.0);
+    for (size_t i = 0; i < m_c.size() && i < v.size(); i++) v[i] = m_c[i];
+    return v;
+  }
+  void assign(const double *v, int p, double scale)
+  {
+    m_c.assign(v, v + (size_t)p * p);
+    m_scale = scale;
+  }
+
+ protected:
+  double m_scale;
+  std::vector<double> m_c;
+};
+class CMulExpan : public CExpan {   // multipole: M-scale
+ public:
+  using CExpan::CExpan;
+};
+class CLocalExpan : public CExpan {  // local: L-scale
+ public:
+  using CExpan::CExpan;
+};
+// x, y, z derivatives of an expansion (CGradExpan)
+class CGradExpan {
+ public:
+  CExpan &operator[](int c) { return m_e[c]; }
+  const CExpan &operator[](int c) const { return m_e[c]; }
+
+ private:
+  CExpan m_e[3];
+};
+
+// <M, L> with the scales of a multipole and a local expansion: sum over n of
+// (1 / (M scale * L scale))^n times the degree-n products, the m > 0 terms twice
+// (inprod, src/expansion.h:706-741)
+inline double inprod(const CExpan &M, const CExpan &L)
+{
+  const int p = std::min(M.order(), L.order());
+  const double fact = 1.0 / (M.getScale() * L.getScale());
+  double sum = 0.0, scale = 1.0;
+  for (int n = 0; n < p; n++) {
+    double s = 0.0;
+    for (int mm = 1; mm < 2 * n + 1; mm++) s += M[n * n + mm] * L[n * n + mm];
+    sum += scale * (2.0 * s + M[n * n] * L[n * n]);
+    scale *= fact;
+  }
+  return sum;
+}
+
+
+// Rotation of expansions by Euler angles (theta, phi, xi).
+class CRotCoeff {
+ public:
+  CRotCoeff() : m_p(0), m_a{0.0, 0.0, 0.0} {}
+  void reset(double theta, double phi, double xi, int p) { m_a[0] = theta; m_a[1] = phi; m_a[2] = xi; m_p = p; }
+  void reset(const CQuat &Q, int p)
+  {
+    const double q[4] = {Q.real(), Q.imag().x(), Q.imag().y(), Q.imag().z()};
+    CSystem::check(pbsam_quat_angles(q, m_a));
+    m_p = p;
+  }
+  int getOrder() const { return m_p; }
+  // rotate (src/rotcoeff.cpp:357-441); the output keeps the input's scale
+  bool rotate(const CExpan &Min, CExpan &Mout, bool bFor) const { return apply(Min, Mout, bFor, 0); }
+  // rotateWithXi (src/rotcoeff.cpp:250-350), for molecule rotations
+  bool rotateWithXi(const CExpan &Min, CExpan &Mout, bool bFor) const { return apply(Min, Mout, bFor, 1); }
+  // many expansions, each with its own rotation
+  static bool rotateBatch(const std::vector<CRotCoeff> &rot, const std::vector<CExpan> &in, std::vector<CExpan> &out,
+                          bool bFor, bool withXi = false)
+  {
+    const int NP = CSystem::poles(), n = (int)in.size();
+    if ((int)rot.size() != n || n == 0) return n == 0;
+    int p = NP;
+    std::vector<double> a, x, y((size_t)n * NP * NP);
+    for (int i = 0; i < n; i++) {
+      p = std::min(p, std::min(rot[i].m_p, in[i].order()));
+      a.insert(a.end(), rot[i].m_a, rot[i].m_a + 3);
+      const std::vector<double> v = in[i].padded(NP);
+      x.insert(x.end(), v.begin(), v.end());
+    }
+    if (!CSystem::check(pbsam_expan_rotate(CSystem::ctx(), n, a.data(), p, withXi, bFor, x.data(), y.data(), 0)))
+      return false;
+    out.assign(n, CExpan());
+    for (int i = 0; i < n; i++) out[i].assign(y.data() + (size_t)i * NP * NP, p, in[i].getScale());
+    return true;
+  }
+
+ private:
+  bool apply(const CExpan &Min, CExpan &Mout, bool bFor, int withXi) const
+  {
+    const int NP = CSystem::poles(), p = std::min(m_p, Min.order());
+    const std::vector<double> x = Min.padded(NP);
+    std::vector<double> y((size_t)NP * NP);
+    if (!CSystem::check(pbsam_expan_rotate(CSystem::ctx(), 1, m_a, p, withXi, bFor, x.data(), y.data(), 0)))
+      return false;
+    Mout.assign(y.data(), p, Min.getScale());
+    return true;
+  }
+  int m_p;
+  double m_a[3];
+};
+
+// Coaxial translation along z by rho: screened by the context's kappa or unscreened
+// (kappa = 0), from scale_in to scale_out.
+class CTransCoeff {
+ public:
+  CTransCoeff() : m_rho(0.0), m_screened(1), m_p(0), m_si(1.0), m_so(1.0) {}
+  // reset(rho, kappa, p, scalei, scaleo): kappa must be the context's or 0
+  bool reset(double rho, double kappa, int p, double scalei, double scaleo)
+  {
+    const double k = CSystem::getKappa();
+    if (kappa != 0.0 && std::fabs(kappa - k) > 1e-12 * k) {
+      std::fprintf(stderr, "pbsam-b200: translations are screened by the context's kappa or not at all\n");
+      return false;
+    }
+    m_rho = rho; m_screened = kappa != 0.0; m_p = p; m_si = scalei; m_so = scaleo;
+    return true;
+  }
+  // translate (src/transcoeff.cpp:211-286; tpose is not supported there either)
+  bool translate(const CExpan &Min, CExpan &Mout, bool tpose = false) const { return apply(Min, Mout, tpose, 0); }
+  // dTranslate (src/transcoeff.cpp:294-364)
+  bool dTranslate(const CExpan &Min, CExpan &Mout, bool tpose = false) const { return apply(Min, Mout, tpose, 1); }
+
+ private:
+  bool apply(const CExpan &Min, CExpan &Mout, bool tpose, int deriv) const
+  {
+    if (tpose) {
+      std::fprintf(stderr, "pbsam-b200: transposed translation is not supported (src/transcoeff.cpp:216-218)\n");
+      return false;
+    }
+    const int NP = CSystem::poles(), p = std::min(m_p, Min.order());
+    const double a[3] = {m_rho, m_si, m_so};
+    const std::vector<double> x = Min.padded(NP);
+    std::vector<double> y((size_t)NP * NP);
+    if (!CSystem::check(pbsam_expan_translate(CSystem::ctx(), 1, a, p, m_screened, deriv, x.data(), y.data(), 0)))
+      return false;
+    Mout.assign(y.data(), p, m_so);
+    return true;
+  }
+  double m_rho;
+  int m_screened, m_p;
+  double m_si, m_so;
+};
+
+// Re-expansion of a source sphere's multipole into a local expansion about a target
+// sphere (CXFormA(source, target)): the spheres' radii are the scales.
+class CXFormA {
+ public:
+  CXFormA(double radSource, double radTarget) : m_rs(radSource), m_rt(radTarget), m_P(), m_p(0) {}
+  // reset(P, p), P = target centre - source centre
+  void reset(const CPnt &P, int p) { m_P = P; m_p = p; }
+  // xformH (screened; src/xforms.cpp:122-132)
+  bool xformH(const CExpan &Min, CExpan &Mout) const { return apply(Min, Mout, nullptr, 1); }
+  // xformH with its gradient w.r.t. the target position (src/xforms.cpp:85-115)
+  bool xformH(const CExpan &Min, CExpan &Mout, CGradExpan &G) const { return apply(Min, Mout, &G, 1); }
+  // xformF (unscreened; src/xforms.cpp:260-270)
+  bool xformF(const CExpan &Min, CExpan &Mout) const { return apply(Min, Mout, nullptr, 0); }
+
+ private:
+  bool apply(const CExpan &Min, CExpan &Mout, CGradExpan *G, int screened) const
+  {
+    const int NP = CSystem::poles(), p = std::min(m_p, Min.order());
+    const double a[5] = {m_P.x(), m_P.y(), m_P.z(), m_rs, m_rt};
+    const std::vector<double> x = Min.padded(NP);
+    std::vector<double> y((size_t)NP * NP), g(G ? 3 * (size_t)NP * NP : 0);
+    if (!CSystem::check(pbsam_expan_reexpand(CSystem::ctx(), 1, a, p, screened, x.data(), y.data(),
+                                             G ? g.data() : nullptr, 0)))
+      return false;
+    Mout.assign(y.data(), p, m_rt);
+    if (G)
+      for (int c = 0; c < 3; c++) (*G)[c].assign(g.data() + (size_t)c * NP * NP, p, m_rt);
+    return true;
+  }
+  double m_rs, m_rt;
+  CPnt m_P;
+  int m_p;
+};

@@ -206,10 +206,16 @@ __device__ void solve_direct_T(const Team &tm, const Tab &T, const TypeView &tv,
   double *x = sc.xs, *y = sc.sol;
   for (int k = tm.rank; k < NP2; k += tm.size) { x[k] = gF[k]; x[NP2 + k] = gH[k]; }
   tm.sync();
+  // a thread per column, eight rows in flight
   for (int j = tm.rank; j < n2; j += tm.size) {
-    double s = 0.0;
-    for (int r = 0; r < n2; r++) s += G[(size_t)r * n2 + j] * x[r];
-    y[j] = s;
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int r = 0;
+    for (; r + 7 < n2; r += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; u++) a[u] += G[(size_t)(r + u) * n2 + j] * x[r + u];
+    }
+    for (; r < n2; r++) a[0] += G[(size_t)r * n2 + j] * x[r];
+    y[j] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
   }
   tm.sync();
   for (int k = tm.rank; k < NP2; k += tm.size) {
@@ -391,12 +397,11 @@ __device__ RotState mol_rot(const Team &tm, const Sys &y, int i)
   return y.molrot(i);
 }
 
-// entry of type sphere kv (index within the type) in the near list of type sphere tsu
-// whose numeric operator exists, or -1
-__device__ __forceinline__ int num_entry(const TypeView &tv, int tsu, int kv)
+// entry of type sphere kv (index within the type) in the near list of type sphere tsu, or -1
+__device__ __forceinline__ int near_entry(const TypeView &tv, int tsu, int kv)
 {
   for (int e = tv.near_off[tsu]; e < tv.near_off[tsu + 1]; e++)
-    if (tv.near[e] == kv) return tv.nslot[e] >= 0 ? e : -1;
+    if (tv.near[e] == kv) return e;
   return -1;
 }
 
@@ -563,7 +568,15 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
         const int pF = compute_order(NP, rho, bv.tF[y.sc1(v)], y.rad(v));
         const int pH = compute_order(NP, rho, bv.tH[y.sc1(v)], y.rad(v));
         double *oF = t6, *oH = sc.E(10);
-        if (sep > 0 && !(sep < c.prm.min_sep_numeric)) {
+        const bool analytic = sep > 0 && !(sep < c.prm.min_sep_numeric);
+        const int ent = c.tv.nslot ? near_entry(c.tv, y.ts(u), v - mo) : -1;
+        const int slot = ent >= 0 ? c.tv.nslot[ent] : -1;
+        if (slot >= 0 && c.tv.nkind[slot] == (analytic ? 0 : 1)) {
+          // the precomputed operators of the forward map v -> u, transposed
+          const double *NF = c.tv.Nmat + (size_t)slot * 2 * NP2 * NP2;
+          num_apply_T(tm, NF, pF, analytic ? pF : NP, muF(u), nF, NP2);
+          num_apply_T(tm, NF + (size_t)NP2 * NP2, pH, analytic ? pH : NP, muH(u), nH, NP2);
+        } else if (analytic) {
           // analytic: T(u <- v)^T = W T(v <- u) W^-1, from the intra table of target v
           double *wF = t4, *wH = t5;
           for (int k = tm.rank; k < NP2; k += tm.size) { wF[k] = muF(u)[k] / wgt(k); wH[k] = muH(u)[k] / wgt(k); }
@@ -576,19 +589,6 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
           V.in[1] = wH; V.out[1] = oH; V.useF[1] = false;
           pair_apply_multi(tm, T, sc, X, V, false);
           for (int k = tm.rank; k < NP2; k += tm.size) { nF[k] += wgt(k) * oF[k]; nH[k] += wgt(k) * oH[k]; }
-          tm.sync();
-        } else if (c.tv.nslot && num_entry(c.tv, y.ts(u), v - mo) >= 0) {
-          // numeric, precomputed: N^T restricted to the rows of degree < p
-          const double *NF = c.tv.Nmat + (size_t)c.tv.nslot[num_entry(c.tv, y.ts(u), v - mo)] * 2 * NP2 * NP2;
-          const double *NH = NF + (size_t)NP2 * NP2;
-          const double *mF = muF(u), *mH = muH(u);
-          for (int j = tm.rank; j < NP2; j += tm.size) {
-            double sF = 0.0, sH = 0.0;
-            for (int k = 0; k < pF * pF; k++) sF += NF[(size_t)k * NP2 + j] * mF[k];
-            for (int k = 0; k < pH * pH; k++) sH += NH[(size_t)k * NP2 + j] * mH[k];
-            nF[j] += sF;
-            nH[j] += sH;
-          }
           tm.sync();
         } else {
           // numeric: the expansion at u of v's surface charges q = dA W c_n E . Y
@@ -619,8 +619,11 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
       }
       dn += team_sum(tm, ld, y.red);
       nn += team_sum(tm, ln, y.red);
-      tcopy(tm, lamF(v), nF, NP2);
-      tcopy(tm, lamH(v), nH, NP2);
+      const double om = c.prm.exact_relax;   // over-relaxed as the forward sweeps
+      for (int k = tm.rank; k < NP2; k += tm.size) {
+        lamF(v)[k] += om * (nF[k] - lamF(v)[k]);
+        lamH(v)[k] += om * (nH[k] - lamH(v)[k]);
+      }
       tm.sync();
       solve_direct_T(tm, T, c.tv, sc, tsv, lamF(v), lamH(v), muF(v), muH(v));
     }

@@ -201,6 +201,7 @@ extern "C" void pbsam_params_default(pbsam_params *p)
   p->box_length = 0.0;
   p->exact_tables = 1;
   p->exact_tol = 1e-14;
+  p->exact_relax = 1.0;
 }
 
 static double kappa_of(const pbsam_params &p)
@@ -219,6 +220,7 @@ extern "C" int pbsam_context_create(const pbsam_params *prm, int device, pbsam_c
   if (prm->exact != 0 && prm->exact != 1) return fail(PBSAM_E_BADARG, "exact must be 0 or 1");
   if (prm->exact_tables != 0 && prm->exact_tables != 1) return fail(PBSAM_E_BADARG, "exact_tables must be 0 or 1");
   if (!(prm->exact_tol > 0.0 && prm->exact_tol < 1.0)) return fail(PBSAM_E_BADARG, "exact_tol must be in (0, 1)");
+  if (!(prm->exact_relax > 0.0 && prm->exact_relax < 2.0)) return fail(PBSAM_E_BADARG, "exact_relax must be in (0, 2)");
   if (!(prm->box_length >= 0.0) || !std::isfinite(prm->box_length))
     return fail(PBSAM_E_BADARG, "box_length must be 0 (no periodic box) or a positive edge");
   if (prm->exact && prm->poles > 32) return fail(PBSAM_E_BADARG, "the exact form supports pole orders up to 32");
@@ -562,11 +564,12 @@ static int set_smem_attrs(int NP)
 }
 
 // upload all molecule types and run the per-type setup kernels
-// Exact form: the numeric near-field operators of every intra near pair that
-// re-expands numerically (pbsam_nummat_kernel), when they fit in 4 GB; tv.nslot and
-// tv.Nmat stay null otherwise and the kernels evaluate those pairs from the surface
-// charges.  A pair that the device classifies otherwise than this host test (a
-// separation within rounding of 0 or min_sep_numeric) falls back the same way.
+// Exact form: the near-field operators of the intra near pairs (pbsam_nummat_kernel):
+// of every pair when they fit in 4 GB, else of the numeric pairs alone when those fit,
+// else none (tv.nslot and tv.Nmat stay null and the kernels transform the pairs as
+// the plain drop-in does).  A pair that the device classifies otherwise than this host
+// test (a separation within rounding of 0 or min_sep_numeric) finds an operator of the
+// other kind and is transformed the plain way too.
 static int build_numeric_operators(std::vector<void *> &B, pbsam_context *c, TypeView &tv, Ctx cx, int NP,
                                    const std::vector<int> &type_off, const std::vector<int> &near_off,
                                    const std::vector<int> &near, const std::vector<int> &spx_off,
@@ -574,27 +577,35 @@ static int build_numeric_operators(std::vector<void *> &B, pbsam_context *c, Typ
 {
   const long long NP2 = (long long)NP * NP;
   const int TS = type_off.back();
-  std::vector<int> nslot(near.size(), -1), slot_e, slot_u;
+  const size_t per = (size_t)2 * NP2 * NP2 * sizeof(double), budget = 4ULL << 30;
+  std::vector<int> nslot, slot_e, slot_u, slot_k;
   int maxpts = 1;
-  for (int ts = 0, t = 0; ts < TS; ts++) {
-    while (type_off[t + 1] <= ts) t++;
-    for (int e = near_off[ts]; e < near_off[ts + 1]; e++) {
-      const int v = type_off[t] + near[e];
-      const double P[3] = {cen[3 * ts] - cen[3 * v], cen[3 * ts + 1] - cen[3 * v + 1], cen[3 * ts + 2] - cen[3 * v + 2]};
-      const double sep = std::sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]) - rad[ts] - rad[v];
-      if (sep > 0 && !(sep < c->prm.min_sep_numeric)) continue;
-      nslot[e] = (int)slot_e.size();
-      slot_e.push_back(e);
-      slot_u.push_back(ts);
-      maxpts = std::max(maxpts, spx_off[v + 1] - spx_off[v]);
+  for (int with_analytic = 1; with_analytic >= 0; with_analytic--) {
+    nslot.assign(near.size(), -1);
+    slot_e.clear(); slot_u.clear(); slot_k.clear();
+    for (int ts = 0, t = 0; ts < TS; ts++) {
+      while (type_off[t + 1] <= ts) t++;
+      for (int e = near_off[ts]; e < near_off[ts + 1]; e++) {
+        const int v = type_off[t] + near[e];
+        const double P[3] = {cen[3 * ts] - cen[3 * v], cen[3 * ts + 1] - cen[3 * v + 1], cen[3 * ts + 2] - cen[3 * v + 2]};
+        const double sep = std::sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2]) - rad[ts] - rad[v];
+        const bool analytic = sep > 0 && !(sep < c->prm.min_sep_numeric);
+        if (analytic && !with_analytic) continue;
+        nslot[e] = (int)slot_e.size();
+        slot_e.push_back(e);
+        slot_u.push_back(ts);
+        slot_k.push_back(analytic ? 0 : 1);
+        if (!analytic) maxpts = std::max(maxpts, spx_off[v + 1] - spx_off[v]);
+      }
     }
+    if (per * slot_e.size() <= budget) break;
   }
-  const size_t per = (size_t)2 * NP2 * NP2 * sizeof(double);
-  if (slot_e.empty() || per * slot_e.size() > (4ULL << 30)) return PBSAM_OK;
+  if (slot_e.empty() || per * slot_e.size() > budget) return PBSAM_OK;
   double *N = nullptr;
   TRY(dalloc(B, &N, slot_e.size() * 2 * NP2 * NP2));
-  const int *dslot = nullptr, *de = nullptr, *du = nullptr;
+  const int *dslot = nullptr, *dkind = nullptr, *de = nullptr, *du = nullptr;
   TRY(dput(B, &dslot, nslot));
+  TRY(dput(B, &dkind, slot_k));
   std::vector<void *> tmp;
   auto release = [&]() { for (void *q : tmp) cudaFree(q); };
   int r = dput(tmp, &de, slot_e);
@@ -607,6 +618,7 @@ static int build_numeric_operators(std::vector<void *> &B, pbsam_context *c, Typ
   if (r) { release(); return r; }
   tv.Nmat = N;
   tv.nslot = dslot;
+  tv.nkind = dkind;
   cx.tv = tv;
   cudaError_t e = cudaSuccess;
   for (int s0 = 0; e == cudaSuccess && s0 < ns; s0 += CH) {
@@ -844,6 +856,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   p.min_sep_numeric = c->prm.min_sep_numeric; p.idiel = c->prm.idiel; p.sdiel = c->prm.sdiel;
   p.exact = c->prm.exact;
   p.exact_tol = c->prm.exact_tol;
+  p.exact_relax = c->prm.exact_relax;
   p.box = c->prm.box_length;
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);
@@ -1257,3 +1270,4 @@ extern "C" int pbsam_system_phase_ms(const pbsam_system *s, double *ms)
 
 // measured device rates for the roofline (uses the helpers above)
 #include "pbsam_probe.cu"
+#include "pbsam_expan.cu"

@@ -294,7 +294,7 @@ __device__ void rot_compute(const TM &tm, const Tab &T, double theta, double phi
 }
 
 // Euler angles of a molecule orientation (src/rotcoeff.cpp:180-201)
-__device__ __forceinline__ void quat_angles(const double *q, double &th, double &ph, double &xi)
+__host__ __device__ __forceinline__ void quat_angles(const double *q, double &th, double &ph, double &xi)
 {
   const double w = q[0], x = q[1], y = q[2], z = q[3];
   th = acos(1.0 - 2 * x * x - 2 * y * y);

@@ -54,7 +54,9 @@ __host__ __device__ inline long long scr_doubles(int NP, long long S)
   n += 6 * 3 * NP2;             // sol
   n += 12 * NP2;                // mv
   n += 4096 + S * S;            // misc + list building workspace
-  return n;
+  // a multiple of 8 doubles: consecutive blocks stay 64-byte aligned (R and dR are
+  // double2, whose accesses need 16-byte alignment)
+  return (n + 7) & ~7LL;
 }
 
 // IMat rows and matvec operands are stored with an even stride so that every row
@@ -1298,13 +1300,13 @@ __device__ void reexpand_LS(const Team &tm, const Sys &y, int s, bool fromSelf)
 // type by pbsam_direct_kernel.  Returns computeDev2 (src/expcenter.cpp:1336-1370) of H.
 __device__ __noinline__ double solve_direct(const Team &tm, const Tab &T, const TypeView &tv, const Scr &sc, int ts,
                                             double *F, double *H, const double *LF, const double *LH, double *red,
-                                            int *stats)
+                                            int *stats, double omega)
 {
   const int NP = T.NP, NP2 = NP * NP, n2 = 2 * NP2;
   const double *cst = tv.cst + (size_t)ts * CST_N * NP;
   const double *Dfix = tv.Dfix + (size_t)ts * NP2, *Vfix = tv.Vfix + (size_t)ts * NP2;
   const double *G = tv.Gdir + (size_t)ts * n2 * n2;
-  double *x = sc.xs, *Hold = sc.sol;
+  double *x = sc.xs, *Hold = sc.sol, *Fold = sc.sol + NP2;
   for (int k = tm.rank; k < NP2; k += tm.size) {
     int n = (int)sqrt((double)k);
     while (n * n > k) n--;
@@ -1312,18 +1314,29 @@ __device__ __noinline__ double solve_direct(const Team &tm, const Tab &T, const 
     x[k] = Vfix[k] + cst[CST_LH1 * NP + n] * LH[k] + cst[CST_LF1 * NP + n] * LF[k];
     x[NP2 + k] = Dfix[k] + cst[CST_LH2 * NP + n] * LH[k] + cst[CST_LF2 * NP + n] * LF[k];
     Hold[k] = H[k];
+    Fold[k] = F[k];
   }
   tm.sync();
   const int lane = tm.rank & 31, w = tm.rank >> 5, nw = tm.size >> 5;
   for (int r = w; r < n2; r += nw) {
     const double *g = G + (size_t)r * n2;
-    double acc = 0.0;
-    for (int j = lane; j < n2; j += 32) acc += g[j] * x[j];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int j = lane;
+    for (; j + 96 < n2; j += 128) {   // four loads in flight per lane
+      const double g0 = g[j], g1 = g[j + 32], g2 = g[j + 64], g3 = g[j + 96];
+      a0 += g0 * x[j];
+      a1 += g1 * x[j + 32];
+      a2 += g2 * x[j + 64];
+      a3 += g3 * x[j + 96];
+    }
+    for (; j < n2; j += 32) a0 += g[j] * x[j];
+    double acc = (a0 + a1) + (a2 + a3);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) {
-      if (r < NP2) F[r] = acc;
-      else H[r - NP2] = acc;
+      // omega != 1: the sweep's update over-relaxed (the fixed point is the same)
+      if (r < NP2) F[r] = omega == 1.0 ? acc : Fold[r] + omega * (acc - Fold[r]);
+      else H[r - NP2] = omega == 1.0 ? acc : Hold[r - NP2] + omega * (acc - Hold[r - NP2]);
     }
   }
   tm.sync();
@@ -1350,7 +1363,8 @@ __device__ double solve_surface(const Team &tm, const Sys &y, int s, bool rotH)
   PhaseClock pc{y.tph, 0};
   pc.start(tm);
   double dv = y.c->prm.exact
-                  ? solve_direct(tm, T, y.c->tv, y.sc, ts, y.F(s), y.H(s), y.LFS(s), y.LHS(s), y.red, y.stats())
+                  ? solve_direct(tm, T, y.c->tv, y.sc, ts, y.F(s), y.H(s), y.LFS(s), y.LHS(s), y.red, y.stats(),
+                                 rotH ? 1.0 : y.c->prm.exact_relax)
                   : solve_fh(tm, y.cw, y.tph, T, y.c->tv, y.c->prm, y.sc, ts, 1, y.F(s), y.H(s), y.LFS(s), y.LHS(s),
                              y.red, y.stats());
   pc.stop(tm, PH_SOLVE);
@@ -1392,19 +1406,48 @@ __device__ double recompute_from_self(const Team &tm, const Sys &y, int s)   // 
   return solve_surface(tm, y, s, true);
 }
 
-// y = (rows of degree < p of N) x, zero beyond (N: NP2 x NP2 row-major); a warp per row
-__device__ void num_apply(const Team &tm, const double *N, int p, const double *x, double *out, int NP2)
+// out = (rows of degree < p of N) x, zero beyond (N: NP2 x NP2 row-major), reading the
+// columns of degree < pin; a warp per row, four loads in flight per lane
+__device__ void num_apply(const Team &tm, const double *N, int p, int pin, const double *x, double *out, int NP2)
 {
-  const int lane = tm.rank & 31, w = tm.rank >> 5, nw = tm.size >> 5, rows = p * p;
+  const int lane = tm.rank & 31, w = tm.rank >> 5, nw = tm.size >> 5, rows = p * p, cols = pin * pin;
   for (int r = w; r < NP2; r += nw) {
     double acc = 0.0;
     if (r < rows) {
       const double *row = N + (size_t)r * NP2;
-      for (int j = lane; j < NP2; j += 32) acc += row[j] * x[j];
+      int j = lane;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      for (; j + 96 < cols; j += 128) {
+        const double m0 = row[j], m1 = row[j + 32], m2 = row[j + 64], m3 = row[j + 96];
+        a0 += m0 * x[j];
+        a1 += m1 * x[j + 32];
+        a2 += m2 * x[j + 64];
+        a3 += m3 * x[j + 96];
+      }
+      for (; j < cols; j += 32) a0 += row[j] * x[j];
+      acc = (a0 + a1) + (a2 + a3);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     }
     if (lane == 0) out[r] = acc;
+  }
+  tm.sync();
+}
+
+// out[j] += sum over rows k of degree < p of N[k][j] y[k], for the columns j of degree
+// < pin (the transpose of num_apply); a thread per column, eight rows in flight
+__device__ void num_apply_T(const Team &tm, const double *N, int p, int pin, const double *y, double *out, int NP2)
+{
+  const int rows = p * p, cols = pin * pin;
+  for (int j = tm.rank; j < cols; j += tm.size) {
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int k = 0;
+    for (; k + 7 < rows; k += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; u++) a[u] += N[(size_t)(k + u) * NP2 + j] * y[k + u];
+    }
+    for (; k < rows; k++) a[0] += N[(size_t)k * NP2 + j] * y[k];
+    out[j] += ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
   }
   tm.sync();
 }
@@ -1449,7 +1492,17 @@ __device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s, int par
     const int pH = compute_order(y.NP, rho, y.c->bv.tH[y.sc1(s2)], rj);
     PhaseClock pc{y.tph, 0};
     pc.start(tm);
-    if (sep > 0 && !(sep < y.c->prm.min_sep_numeric)) {
+    const bool analytic = sep > 0 && !(sep < y.c->prm.min_sep_numeric);
+    const int slot = (part != 0 && y.c->tv.nslot) ? y.c->tv.nslot[e] : -1;
+    if (slot >= 0 && y.c->tv.nkind[slot] == (analytic ? 0 : 1)) {
+      // the exact form's precomputed operators of the pair, the same maps of F and H of
+      // s2: an analytic transform at order p is the block of degrees < p of its
+      // full-order operator, a numeric one the rows of degree < p
+      const double *NF = y.c->tv.Nmat + (size_t)slot * 2 * y.NP2 * y.NP2;
+      num_apply(tm, NF, pF, analytic ? pF : y.NP, y.F(s2), a, y.NP2);
+      num_apply(tm, NF + (size_t)y.NP2 * y.NP2, pH, analytic ? pH : y.NP, y.H(s2), bq, y.NP2);
+      pc.stop(tm, analytic ? PH_INTRA : PH_NUMERIC);
+    } else if (analytic) {
       PairXf X;
       table_pair(tm, T, y.c->tv, y.sc, intra_pair(y.c->tv, ts, s - mo, kj), pH, pF, rj, y.rad(s), X);
       MultiVec V;
@@ -1458,12 +1511,6 @@ __device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s, int par
       V.in[1] = y.H(s2); V.out[1] = bq; V.useF[1] = false;
       pair_apply_multi(tm, T, y.sc, X, V, false);
       pc.stop(tm, PH_INTRA);
-    } else if (part != 0 && y.c->tv.nslot && y.c->tv.nslot[e] >= 0) {
-      // the exact form's precomputed operators: the same map from F and H of s2
-      const double *NF = y.c->tv.Nmat + (size_t)y.c->tv.nslot[e] * 2 * y.NP2 * y.NP2;
-      num_apply(tm, NF, pF, y.F(s2), a, y.NP2);
-      num_apply(tm, NF + (size_t)y.NP2 * y.NP2, pH, y.H(s2), bq, y.NP2);
-      pc.stop(tm, PH_NUMERIC);
     } else {
       crew_numeric_expand2<1>(tm, y.cw, T, y.sc, y.spx(s2), y.npts(s2), P, y.rad(s),
                               NumSet{y.qF(s2), true, false, pF, a}, NumSet{y.qH(s2), true, true, pH, bq});
@@ -2686,13 +2733,16 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_setup3_kernel(Ctx c, int e0,
 }
 
 
-// Numeric near-field operators of the exact form.  For intra near entry e (target type
-// sphere u, source v = near[e]) whose pair re-expands numerically, the full-order maps
-// LF_u += N_F F_v and LH_u += N_H H_v (NP2 x NP2, row-major): column j is the numeric
-// expansion about u (numeric_expand2) of the surface charges (surface_q2) of a unit
-// F_j (H_j) of v.  Both steps are linear in the coefficients and a truncation order p
-// of the forward only drops output degrees >= p, so the rows of degree < p of N give
-// the forward's expansion at that order.  One CTA per slot.
+// Near-field operators of the exact form.  For intra near entry e (target type sphere
+// u, source v = near[e]) the full-order maps LF_u += N_F F_v and LH_u += N_H H_v
+// (NP2 x NP2, row-major).  Numeric pairs (kind 1): column j is the numeric expansion
+// about u (numeric_expand2) of the surface charges (surface_q2) of a unit F_j (H_j) of
+// v; both steps are linear and a truncation order p only drops output degrees >= p,
+// so the rows of degree < p give the forward's expansion at that order.  Analytic
+// pairs (kind 0): column j is the intra table transform (rotation, coaxial
+// translation, rotation back) of a unit coefficient at full order; rotations keep
+// degrees apart and the translation coefficients of degrees < p do not depend on p,
+// so the block of degrees < p is the transform at order p.  One CTA per slot.
 __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_nummat_kernel(Ctx c, const int *slot_e, const int *slot_u, int s0,
                                                                   int ns, double *scr, long long stride, double *qw,
                                                                   long long qstride, double *Nmat)
@@ -2705,7 +2755,7 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_nummat_kernel(Ctx c, const i
   const Tab &T = c.T;
   const TypeView &tv = c.tv;
   const int NP = T.NP, NP2 = NP * NP;
-  const int slot = s0 + k, e = slot_e[slot], u = slot_u[slot];
+  const int slot = s0 + k, e = slot_e[slot], u = slot_u[slot], kind = tv.nkind[slot];
   Scr sc = make_scr(scr + (size_t)k * stride, NP, dsm);
   int t = 0;
   while (tv.type_off[t + 1] <= u) t++;
@@ -2727,11 +2777,22 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_nummat_kernel(Ctx c, const i
       if (j > 0) unit[j - 1] = 0.0;
     }
     tm.sync();
-    double t1[1], t2[1];
-    surface_q2<1>(tm, T, sc, pts, npt, dA, unit, T.CONST2, qF, unit, cstv + CST_CHGH * NP, qH, 0, 1, t1, t2, red);
-    tm.sync();
-    numeric_expand2<1>(tm, T, sc, pts, npt, P, tv.rad[u], NumSet{qF, true, false, NP, outF},
-                       NumSet{qH, true, true, NP, outH});
+    if (kind == 0) {
+      // analytic pair: the intra table transform at full order (table_pair)
+      PairXf X;
+      table_pair(tm, T, tv, sc, intra_pair(tv, u, u - tv.type_off[t], tv.near[e]), NP, NP, tv.rad[v], tv.rad[u], X);
+      MultiVec V;
+      V.n = 2;
+      V.in[0] = unit; V.out[0] = outF; V.useF[0] = true;
+      V.in[1] = unit; V.out[1] = outH; V.useF[1] = false;
+      pair_apply_multi(tm, T, sc, X, V, false);
+    } else {
+      double t1[1], t2[1];
+      surface_q2<1>(tm, T, sc, pts, npt, dA, unit, T.CONST2, qF, unit, cstv + CST_CHGH * NP, qH, 0, 1, t1, t2, red);
+      tm.sync();
+      numeric_expand2<1>(tm, T, sc, pts, npt, P, tv.rad[u], NumSet{qF, true, false, NP, outF},
+                         NumSet{qH, true, true, NP, outH});
+    }
     tm.sync();
     for (int r = tm.rank; r < NP2; r += tm.size) {
       NF[(size_t)r * NP2 + j] = outF[r];

@@ -20,6 +20,7 @@ struct SolveParams {
   double idiel, sdiel;
   int exact;               // 1: exact form (direct inner solves, full sweeps, adjoint forces)
   double exact_tol;        // exact form: sweep stop (root-mean-square relative change)
+  double exact_relax;      // exact form: over-relaxation factor of the sweeps' updates
   double box;              // > 0: edge of a cubic periodic box (minimum-image displacements)
 };
 
@@ -67,9 +68,10 @@ struct TypeView {
   double *pS;              // [TE][16] rotation scalars
   const double *Gdir;      // [TS][2NP2][2NP2] row-major or null: the inner fixed point solved for
                            // (fb, hb) -> (F, H) (exact form, pbsam_direct_kernel)
-  const int *nslot;        // [near entries] numeric operator slot of each intra near entry, -1 if none
-  const double *Nmat;      // [slots][2][NP2][NP2] row-major or null: the numeric near-field
-                           // operators N_F, N_H (exact form, pbsam_nummat_kernel)
+  const int *nslot;        // [near entries] operator slot of each intra near entry, -1 if none
+  const int *nkind;        // [slots] 0: analytic pair (rotation + translation), 1: numeric
+  const double *Nmat;      // [slots][2][NP2][NP2] row-major or null: the near-field operators
+                           // N_F, N_H of the intra near pairs (exact form, pbsam_nummat_kernel)
 };
 
 // Batch of B independent systems with the same list of molecules.

@@ -39,7 +39,7 @@ class pbsam_params(ctypes.Structure):
                 ("intra_cutoff", ctypes.c_double), ("min_sep_numeric", ctypes.c_double),
                 ("num_points_x", ctypes.c_int), ("cluster_size", ctypes.c_int), ("exact", ctypes.c_int),
                 ("box_length", ctypes.c_double), ("exact_tables", ctypes.c_int),
-                ("exact_tol", ctypes.c_double)]
+                ("exact_tol", ctypes.c_double), ("exact_relax", ctypes.c_double)]
 
 
 PBSAM_BD_NAM = 0
@@ -90,6 +90,13 @@ SIGNATURES = {
     "pbsam_system_bd_run": (ctypes.c_int, [_P, ctypes.c_int]),
     "pbsam_system_bd_state": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, ctypes.c_int]),
     "pbsam_device_peaks": (ctypes.c_int, [ctypes.c_int, _DP, _DP]),
+    "pbsam_expan_rotate": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P,
+                                          ctypes.c_int]),
+    "pbsam_expan_translate": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P,
+                                             ctypes.c_int]),
+    "pbsam_expan_reexpand": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int, _P, _P, _P,
+                                            ctypes.c_int]),
+    "pbsam_quat_angles": (ctypes.c_int, [_DP, _DP]),
     "pbsam_last_error": (ctypes.c_char_p, []),
 }
 
@@ -143,6 +150,14 @@ def bd_params(mode=PBSAM_BD_NAM, **kw):
 
 def _dptr(a):
     return a.ctypes.data_as(_DP)
+
+
+def quat_angles(q):
+    """Euler angles (theta, phi, xi) of a quaternion (w, x, y, z), as CRotCoeff::reset(CQuat)."""
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    a = np.zeros(3)
+    _check(lib().pbsam_quat_angles(_dptr(q), _dptr(a)))
+    return a
 
 
 def device_peaks(device=0):
@@ -212,6 +227,39 @@ class CSystem:
 
     def molecules(self, mol_types, n_systems=1):
         return Molecules(self, mol_types, n_systems)
+
+    # single-expansion operations (CRotCoeff, CTransCoeff, CXFormA), batched over rows
+    def _expan_io(self, x):
+        P2 = self.params.poles ** 2
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, P2)
+        return x, np.zeros_like(x)
+
+    def expan_rotate(self, rot, p, x, with_xi=False, forward=True):
+        """Rotate each row of x (packed expansions) by Euler angles rot[n][3] = theta, phi, xi."""
+        x, out = self._expan_io(x)
+        rot = np.ascontiguousarray(rot, dtype=np.float64).reshape(-1, 3)
+        _check(lib().pbsam_expan_rotate(self.handle, len(x), rot.ctypes.data, p, int(with_xi), int(forward),
+                                        x.ctypes.data, out.ctypes.data, 0))
+        return out
+
+    def expan_translate(self, args, p, x, screened=True, deriv=False):
+        """Coaxial translation of each row of x; args[n][3] = rho, scale in, scale out."""
+        x, out = self._expan_io(x)
+        args = np.ascontiguousarray(args, dtype=np.float64).reshape(-1, 3)
+        _check(lib().pbsam_expan_translate(self.handle, len(x), args.ctypes.data, p, int(screened), int(deriv),
+                                           x.ctypes.data, out.ctypes.data, 0))
+        return out
+
+    def expan_reexpand(self, args, p, x, screened=True, grad=False):
+        """Re-expansion of each row of x from a source to a target sphere; args[n][5] =
+        target centre - source centre, source radius, target radius.  grad: also the
+        x, y, z derivatives w.r.t. the target position ([n][3][p^2])."""
+        x, out = self._expan_io(x)
+        args = np.ascontiguousarray(args, dtype=np.float64).reshape(-1, 5)
+        g = np.zeros((len(x), 3, x.shape[1])) if grad else None
+        _check(lib().pbsam_expan_reexpand(self.handle, len(x), args.ctypes.data, p, int(screened), x.ctypes.data,
+                                          out.ctypes.data, g.ctypes.data if grad else None, 0))
+        return (out, g) if grad else out
 
     def close(self):
         if self.handle:

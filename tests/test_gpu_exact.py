@@ -11,8 +11,8 @@ negative gradient of the lab-frame energy by the adjoint.  Checked:
     batch;
   * compute_forces = -dU/dpos and -dU/domega, and dU/dquat along a tangent direction;
   * an 8-molecule case (40 spheres each, p = 10) against central differences;
-  * the precomputed numeric near-field operators against their evaluation from the
-    surface charges.
+  * the precomputed intra near-field operators against the plain transforms (numeric
+    expansions of the surface charges, rotation + translation).
 The reference's own forces (per-coordinate gradient solves) are printed beside the
 adjoint's, not gated: they differentiate a different function (the reference's
 energy ignores the orientation, and its sweeps stop short of the fixed point).
@@ -134,10 +134,10 @@ def test_exact_backward_vs_oracle_and_central_differences(case, pose, tmp_path):
 
 
 @pytest.mark.parametrize("case", ["tiny", "cfg0"])
-def test_exact_tables_agree_with_surface_charges(case):
-    """The numeric near-field operators prepared once per type (exact_tables = 1) against
-    their evaluation from the surface charges at every use (0): every pose of the case,
-    forces, torques, lab-frame energy and the backward pass to 1e-11 relative."""
+def test_exact_operators_agree_with_plain_transforms(case):
+    """The intra near-field operators prepared once per type (exact_tables = 1) against
+    the plain transforms at every use (0): every pose of the case, forces and torques
+    (the backward pass) and the lab-frame energy to 1e-11 relative."""
     res = []
     for tables in (1, 0):
         ctx, types, P = exact_ctx(case, exact_tables=tables)
@@ -154,7 +154,7 @@ def test_exact_tables_agree_with_surface_charges(case):
     (f1, t1, e1, n1), (f0, t0, e0, n0) = res
     assert np.sum(n1) > 0
     ef, et, ee = rel(f1, f0), rel(t1, t0), rel(e1, e0)
-    print("%s: tables vs surface charges: force %.2e torque %.2e energy %.2e" % (case, ef, et, ee))
+    print("%s: operators vs plain transforms: force %.2e torque %.2e energy %.2e" % (case, ef, et, ee))
     assert ef < 1e-11 and et < 1e-11 and ee < 1e-11, (ef, et, ee)
 
 
