@@ -68,11 +68,11 @@ __host__ __device__ inline size_t imat_stride(int NP2) { return (size_t)NP2 * im
 // numeric-expansion tile: per point the P^2 harmonics, 2 x P radial factors,
 // 5 geometry words and 2 x 3 weights
 __host__ __device__ inline size_t tile_point_bytes(int NP) { return ((size_t)NP * NP + 2 * NP + 11) * sizeof(double); }
-// F/H solve state kept in shared memory: F, H, new H, F base, H base (3 operands
-// each) and a degree table
+// F/H solve state kept in shared memory: F, H, new H, F base, H base, new F (3
+// operands each) and a degree table
 __host__ __device__ inline size_t solve_state_bytes(int NP)
 {
-  return 5 * 3 * (size_t)NP * NP * sizeof(double) + (size_t)NP * NP * sizeof(short) + 16;
+  return 6 * 3 * (size_t)NP * NP * sizeof(double) + (size_t)NP * NP * sizeof(short) + 16;
 }
 __host__ __device__ inline size_t dyn_region_bytes(int NP)
 {
@@ -835,9 +835,12 @@ __device__ __noinline__ void surface_q2(const Team &tm, const Tab &T, const Scr 
 // time and its lanes stride the rows with 16-byte read-only loads, two column
 // blocks per step, so 128 bytes per lane are in flight; the D operands share every
 // loaded IMat element.  The row sums are reduced across the warp in a fixed order.
+// push > 0: Y is in shared memory and each row result is stored into Y of every CTA
+// of the cluster (ranks 0 .. push-1, distributed shared memory), lane 4 g + j storing
+// row j to ranks g, g + 8, ...; the cluster barrier that follows publishes them.
 template <int D, int U>
 __device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const double *x, int NP2,
-                                          int r_begin, int r_end, double *Y, const double *scale)
+                                          int r_begin, int r_end, double *Y, const double *scale, int push)
 {
   const int lane = tm.rank & 31, warp = tm.rank >> 5, nw = tm.size >> 5;
   const int NV = ld >> 1;
@@ -882,7 +885,29 @@ __device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         acc[j][d] = v;
       }
-    if (lane < 4) {
+    if (push > 0) {
+      const int jj = lane & 3, g = lane >> 2;
+      const int i = r0 + jj;
+      if (i < r_end && g < push) {
+        int n = (int)sqrt((double)i);
+        while (n * n > i) n--;
+        while ((n + 1) * (n + 1) <= i) n++;
+        double v[D];
+#pragma unroll
+        for (int d = 0; d < D; d++) v[d] = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (j == jj)
+#pragma unroll
+            for (int d = 0; d < D; d++) v[d] = acc[j][d] * scale[n];
+        cg::cluster_group cl = cg::this_cluster();
+        for (int q = g; q < push; q += 8) {
+          double *dst = cl.map_shared_rank(Y, q);
+#pragma unroll
+          for (int d = 0; d < D; d++) dst[d * NP2 + i] = v[d];
+        }
+      }
+    } else if (lane < 4) {
       const int i = r0 + lane;
       if (i < r_end) {
         int n = (int)sqrt((double)i);
@@ -899,10 +924,10 @@ __device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int
 }
 
 __device__ __forceinline__ void imat_apply(const Team &tm, const double *IMT, int ld, const double *x, int NP2, int D,
-                                           int r_begin, int r_end, double *Y, const double *scale)
+                                           int r_begin, int r_end, double *Y, const double *scale, int push = 0)
 {
-  if (D == 1) imat_apply_t<1, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
-  else imat_apply_t<3, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale);
+  if (D == 1) imat_apply_t<1, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale, push);
+  else imat_apply_t<3, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale, push);
 }
 
 // ------------------------------------------------------------------ crews (thread-block clusters)
@@ -1057,10 +1082,9 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
   const double *Dfix = tv.Dfix + (size_t)ts * NP2, *Vfix = tv.Vfix + (size_t)ts * NP2;
   const double *IMT = tv.imat + (size_t)ts * imat_stride(NP2);
   const int ld = sc.ld;
-  double *sF = sc.tile, *sH = sF + len, *sHn = sH + len, *sFb = sHn + len, *sHb = sFb + len;
-  short *deg = (short *)(sHb + len);
-  double *xgF = xg, *xgH = xg + 3 * NP2;     // exchange buffers (global, the leader's scratch)
-  double *sOut = xg + 6 * NP2;               // H at entry (leader only)
+  double *sF = sc.tile, *sH = sF + len, *sHn = sH + len, *sFb = sHn + len, *sHb = sFb + len, *sFn = sHb + len;
+  short *deg = (short *)(sFn + len);
+  double *sOut = xg + 6 * NP2;               // H at entry (leader only; the leader's scratch)
   const bool lead = cw.rank == 0, crew = cw.size > 1;
   cg::cluster_group cl = cg::this_cluster();
   for (int k = tm.rank; k < NP2; k += tm.size) {
@@ -1100,26 +1124,30 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
     }
     tm.sync();
     if (crew) {
-      imat_apply(tm, IMT, ld, sc.xs, NP2, D, r0, r1, xgF, T.CONST3);
-      cl.sync();                // every CTA's rows of the new F are in L2
-      for (int k = tm.rank; k < len; k += tm.size) sF[k] = xgF[k];
+      // every CTA pushes its rows of the new F into every CTA's sFn (distributed
+      // shared memory); after the cluster barrier each holds the whole vector.  F is
+      // double-buffered: a CTA still forming its operands from sF is never written to
+      imat_apply(tm, IMT, ld, sc.xs, NP2, D, r0, r1, sFn, T.CONST3, cw.size);
+      cl.sync();
+      { double *t = sF; sF = sFn; sFn = t; }
     } else {
       imat_apply(tm, IMT, ld, sc.xs, NP2, D, 0, NP2, sF, T.CONST3);
+      tm.sync();
     }
-    tm.sync();
     for (int k = tm.rank; k < len; k += tm.size) {
       const int kk = k % NP2, n = deg[kk];
       sc.xs[(k / NP2) * ld + kk] = sHb[k] + cst[CST_H2 * NP + n] * sH[k] + cst[CST_F2 * NP + n] * sF[k];
     }
     tm.sync();
     if (crew) {
-      imat_apply(tm, IMT, ld, sc.xs, NP2, D, r0, r1, xgH, cst + CST_INVH * NP);
+      // the same for the new H, into sHn (read only by computeDev below, after this
+      // barrier, and written again only after the next F barrier)
+      imat_apply(tm, IMT, ld, sc.xs, NP2, D, r0, r1, sHn, cst + CST_INVH * NP, cw.size);
       cl.sync();
-      for (int k = tm.rank; k < len; k += tm.size) sHn[k] = xgH[k];
     } else {
       imat_apply(tm, IMT, ld, sc.xs, NP2, D, 0, NP2, sHn, cst + CST_INVH * NP);
+      tm.sync();
     }
-    tm.sync();
     mv.stop(tm, PH_MATVEC);
     // computeDev over complex entries (d, n, m) of the old and new H
     double part = 0.0;
