@@ -171,7 +171,7 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(gpu_id_for_smi(local)) as clk:
+    with ClockSampler(gpu_id_for_smi(local)) as clk, torch.cuda.nvtx.range("sweep"):   # NVTX: ncu --nvtx-include
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(args.steps):
@@ -402,7 +402,7 @@ def run_bd(args, local, rank, world, dist, exact=False, specs=None):
     if world > 1:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(gpu_id_for_smi(local)) as clk:
+    with ClockSampler(gpu_id_for_smi(local)) as clk, torch.cuda.nvtx.range("bd_exact" if exact else "bd"):
         torch.cuda.synchronize()
         e0.record(stream)
         sysb.bd_run(args.bd_steps)
