@@ -550,7 +550,8 @@ static int pick_crew(K kern, int n_sys, size_t smem, int requested)
 static int set_smem_attrs(int NP)
 {
   const int smem = (int)team_smem_bytes(NP);
-  CK(cudaFuncSetAttribute(pbsam_forces_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(pbsam_forces_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)forces_smem_bytes(NP)));
   // clusters of up to 16 CTAs (beyond the portable 8)
   CK(cudaFuncSetAttribute(pbsam_forces_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   CK(cudaFuncSetAttribute(pbsam_selfpol_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -831,7 +832,7 @@ extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, c
   chk(dalloc(Bf, &bv.sep, B * S * S));
   // the exact form runs one CTA per system (its backward pass is not shared by a crew)
   s->adaptive = c->prm.cluster_size < 0 && !c->prm.exact;
-  s->crew = c->prm.exact ? 1 : pick_crew(pbsam_forces_kernel, B, team_smem_bytes(NP), s->adaptive ? 0 : c->prm.cluster_size);
+  s->crew = c->prm.exact ? 1 : pick_crew(pbsam_forces_kernel, B, forces_smem_bytes(NP), s->adaptive ? 0 : c->prm.cluster_size);
   bv.crew = s->adaptive ? PBSAM_MAX_CREW : s->crew;   // scratch blocks per system: the largest crew it may get
   bv.scr_stride = scr_doubles(NP, S);
   chk(dalloc(Bf, &bv.scr, (size_t)B * bv.crew * bv.scr_stride));
@@ -937,7 +938,7 @@ extern "C" int pbsam_system_compute_forces(pbsam_system *s, double *force, doubl
 {
   if (!s) return fail(PBSAM_E_BADARG, "null system");
   CK(cudaSetDevice(s->ctx->device));
-  const size_t smem = team_smem_bytes(s->ctx->prm.poles);
+  const size_t smem = forces_smem_bytes(s->ctx->prm.poles);
   if (s->adaptive && s->stats_pending) {
     // regroup from the last evaluation's costs, every call: wait for the counters of
     // the previous evaluation, so that the plan depends on the counts alone and not

@@ -121,7 +121,7 @@ static cudaError_t bd_enqueue_step(pbsam_system *s, cudaStream_t st)
   pbsam_bd_pre_kernel<<<s->B, PBSAM_BD_THREADS, 0, st>>>(s->c, h->p, h->v);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  e = launch_crews(pbsam_forces_kernel, s->B, s->crew, team_smem_bytes(s->ctx->prm.poles), st, cb,
+  e = launch_crews(pbsam_forces_kernel, s->B, s->crew, forces_smem_bytes(s->ctx->prm.poles), st, cb,
                    (const int *)nullptr);
   if (e != cudaSuccess) return e;
   pbsam_bd_move_kernel<<<s->B, PBSAM_BD_THREADS, h->move_smem, st>>>(s->c, h->p, h->v);

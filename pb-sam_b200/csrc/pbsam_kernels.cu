@@ -35,6 +35,7 @@ struct Scr {
   double2 *lvA, *lvB;    // shared memory: rotation recursion levels, (2NP-1)^2 each
   double *tile;          // shared memory (aliases the levels): numeric-expansion point tiles
   double *xs;            // shared memory: matvec operands, 3 * ld
+  double *ims;           // shared memory after the team region: the IMat of a single-CTA solve (p <= 12)
   __device__ double *E(int i) const { return e + (size_t)i * NP2; }
   __device__ double *G(int i) const { return g + (size_t)i * 3 * NP2; }
 };
@@ -90,6 +91,16 @@ __host__ __device__ inline size_t team_smem_bytes(int NP)
 {
   return dyn_region_bytes(NP) + 3 * (size_t)imat_ld(NP * NP) * sizeof(double) + 64;
 }
+// The force kernel also reserves, at pole orders up to PBSAM_SMEM_IMAT_NP, room for one
+// IMat after the team region (80 KB at p = 10, 166 KB at p = 12) and its mbarrier: a
+// single-CTA solve copies its sphere's IMat there once (a TMA bulk copy) and its inner
+// iterations read it from shared memory instead of re-reading it from L2.
+#define PBSAM_SMEM_IMAT_NP 12
+__host__ __device__ inline size_t imat_smem_bytes(int NP)
+{
+  return NP <= PBSAM_SMEM_IMAT_NP ? imat_stride(NP * NP) * sizeof(double) + 64 : 0;
+}
+__host__ __device__ inline size_t forces_smem_bytes(int NP) { return team_smem_bytes(NP) + imat_smem_bytes(NP); }
 
 __device__ Scr make_scr(double *base, int NP, void *smem)
 {
@@ -104,6 +115,7 @@ __device__ Scr make_scr(double *base, int NP, void *smem)
     int tp = (int)(lv / tile_point_bytes(NP));
     s.tile_pts = tp > 64 ? 64 : tp;
     s.xs = (double *)((char *)smem + lv);
+    s.ims = (double *)((char *)smem + team_smem_bytes(NP));
   }
   const long long rotE = rot_off(NN), trE = tr_off(NN);
   s.NP2 = NP2;
@@ -169,7 +181,7 @@ __device__ Scr warp_scr(double *base, int NP)
   s.misc = take(3LL * s.NP2);     // the warp's running sum
   s.lvA = (double2 *)take(2LL * NN * NN);
   s.lvB = (double2 *)take(2LL * NN * NN);
-  s.sol = nullptr; s.mv = nullptr; s.tile = nullptr; s.xs = nullptr;
+  s.sol = nullptr; s.mv = nullptr; s.tile = nullptr; s.xs = nullptr; s.ims = nullptr;
   return s;
 }
 
@@ -838,7 +850,9 @@ __device__ __noinline__ void surface_q2(const Team &tm, const Tab &T, const Scr 
 // push > 0: Y is in shared memory and each row result is stored into Y of every CTA
 // of the cluster (ranks 0 .. push-1, distributed shared memory), lane 4 g + j storing
 // row j to ranks g, g + 8, ...; the cluster barrier that follows publishes them.
-template <int D, int U>
+// S: IMT is in shared memory (plain loads instead of read-only global loads; the same
+// sums in the same order).
+template <int D, int U, bool S>
 __device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int ld, const double *x, int NP2,
                                           int r_begin, int r_end, double *Y, const double *scale, int push)
 {
@@ -864,7 +878,7 @@ __device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int
       for (int b = 0; b < U; b++)
 #pragma unroll
         for (int j = 0; j < 4; j++)
-          a[b][j] = (k0 + 32 * b < NV) ? __ldg(rp[j] + k0 + 32 * b) : make_double2(0.0, 0.0);
+          a[b][j] = (k0 + 32 * b < NV) ? (S ? rp[j][k0 + 32 * b] : __ldg(rp[j] + k0 + 32 * b)) : make_double2(0.0, 0.0);
 #pragma unroll
       for (int b = 0; b < U; b++) {
         if (k0 + 32 * b >= NV) break;
@@ -924,10 +938,54 @@ __device__ __noinline__ void imat_apply_t(const Team &tm, const double *IMT, int
 }
 
 __device__ __forceinline__ void imat_apply(const Team &tm, const double *IMT, int ld, const double *x, int NP2, int D,
-                                           int r_begin, int r_end, double *Y, const double *scale, int push = 0)
+                                           int r_begin, int r_end, double *Y, const double *scale, int push = 0,
+                                           bool smem = false)
 {
-  if (D == 1) imat_apply_t<1, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale, push);
-  else imat_apply_t<3, 4>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale, push);
+  if (smem) {
+    if (D == 1) imat_apply_t<1, 4, true>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale, push);
+    else imat_apply_t<3, 4, true>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale, push);
+  } else {
+    if (D == 1) imat_apply_t<1, 4, false>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale, push);
+    else imat_apply_t<3, 4, false>(tm, IMT, ld, x, NP2, r_begin, r_end, Y, scale, push);
+  }
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// Copy one IMat (bytes, a multiple of 16, both addresses 16-byte aligned) into shared
+// memory with a TMA bulk copy completed on an mbarrier that sits after it.  The wait is
+// bounded: if the copy has not landed after 2^22 polls the staging is switched off for
+// the rest of the launch (the flag after the mbarrier) and the caller reads the IMat
+// from global memory; the copy, should it land later, writes only into this region.
+__device__ bool stage_imat(const Team &tm, double *dst, const double *src, unsigned bytes)
+{
+  unsigned long long *bar = (unsigned long long *)((char *)dst + bytes);
+  volatile int *off = (volatile int *)(bar + 1);
+  if (*off) return false;
+  const unsigned b = smem_u32(bar), d = smem_u32(dst);
+  if (tm.rank == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(d), "l"(src), "r"(bytes), "r"(b) : "memory");
+  }
+  __syncthreads();
+  int ok = 0;
+  for (int it = 0; it < (1 << 22) && !ok; it++) {
+    unsigned done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(done) : "r"(b) : "memory");
+    ok = done != 0;
+  }
+  ok = __syncthreads_and(ok);
+  if (tm.rank == 0) {
+    if (ok) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(b) : "memory");
+    else *off = 1;
+  }
+  __syncthreads();
+  return ok != 0;
 }
 
 // ------------------------------------------------------------------ crews (thread-block clusters)
@@ -1113,6 +1171,15 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
   tm.sync();
   int r0, r1;
   crew_rows(NP2, cw.rank, cw.size, r0, r1);
+  // a single-CTA solve at p <= 12 reads its IMat from shared memory when the launch
+  // reserved the room (the force kernel does, forces_smem_bytes)
+  bool sim = false;
+  if (!crew && NP <= PBSAM_SMEM_IMAT_NP) {
+    unsigned dsz;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dsz));
+    if (dsz >= forces_smem_bytes(NP)) sim = stage_imat(tm, sc.ims, IMT, (unsigned)(imat_stride(NP2) * sizeof(double)));
+  }
+  const double *IMA = sim ? sc.ims : IMT;
   int ct = 0;
   double dev = 0.0;
   PhaseClock mv{tph, 0};
@@ -1131,7 +1198,7 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
       cl.sync();
       { double *t = sF; sF = sFn; sFn = t; }
     } else {
-      imat_apply(tm, IMT, ld, sc.xs, NP2, D, 0, NP2, sF, T.CONST3);
+      imat_apply(tm, IMA, ld, sc.xs, NP2, D, 0, NP2, sF, T.CONST3, 0, sim);
       tm.sync();
     }
     for (int k = tm.rank; k < len; k += tm.size) {
@@ -1145,7 +1212,7 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
       imat_apply(tm, IMT, ld, sc.xs, NP2, D, r0, r1, sHn, cst + CST_INVH * NP, cw.size);
       cl.sync();
     } else {
-      imat_apply(tm, IMT, ld, sc.xs, NP2, D, 0, NP2, sHn, cst + CST_INVH * NP);
+      imat_apply(tm, IMA, ld, sc.xs, NP2, D, 0, NP2, sHn, cst + CST_INVH * NP, 0, sim);
       tm.sync();
     }
     mv.stop(tm, PH_MATVEC);
@@ -2349,6 +2416,14 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
 __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c, const int *list)
 {
   extern __shared__ double2 dsm[];
+  if (threadIdx.x == 0 && c.T.NP <= PBSAM_SMEM_IMAT_NP) {
+    // the IMat staging region's flag (stage_imat): staging on
+    unsigned dsz;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dsz));
+    if (dsz >= forces_smem_bytes(c.T.NP))
+      *(int *)((char *)dsm + team_smem_bytes(c.T.NP) + imat_stride(c.T.NP * c.T.NP) * sizeof(double) + 8) = 0;
+  }
+  __syncthreads();
   __shared__ double red[PBSAM_TEAM];
   __shared__ CrewCmd cmd;
   const Team tm{(int)threadIdx.x, (int)blockDim.x};
