@@ -227,16 +227,18 @@ int pbsam_system_last_kernel_ms(const pbsam_system *sys, double *ms);
  *   PBSAM_BD_MULTI = CBDmulti::propagate / makeMove / compute_dt / computeMinSepDist
  *                    (src/BDmulti.cpp:396-566): every molecule moves in turn;
  *                    forces while the minimum separation is below the context's
- *                    interaction cutoff (no periodic box); the minimum separation
+ *                    interaction cutoff (the periodic box of pbsam_params.box_length
+ *                    applies, as bdm's); the minimum separation
  *                    is the smallest sphere gap over all molecule pairs, at least
  *                    dt_ref, as the reference's bdm computes it.
  * Time step dt = min(dt_max, dt_min + max(0, d - dt_ref) / dt_div) ps, d the
  * molecule gap (NAM) or the minimum separation (MULTI); drifts D*dt*fact_tr*F and
  * Dr*dt*ikbt*coul_k*torque; noise N(0, 2*D*dt) per component from Philox4x64-10
  * (key = seed, counter = (draw, system)) where the reference uses drand48.
- * Docking (contact lists, PBSAM_BD_DOCKED) is not evaluated.  A force evaluation
- * that finds overlapping spheres ends the trajectory with PBSAM_BD_FAILED, where the
- * reference exits (src/BDnam.cpp:210-212). */
+ * NAM docking (PBSAM_BD_DOCKED) is tested after each move once contact definitions
+ * are set (pbsam_system_bd_set_contacts).  A force evaluation that finds overlapping
+ * spheres ends the trajectory with PBSAM_BD_FAILED, where the reference exits
+ * (src/BDnam.cpp:210-212). */
 #define PBSAM_BD_NAM 0
 #define PBSAM_BD_MULTI 1
 #define PBSAM_BD_RUNNING 0
@@ -282,6 +284,21 @@ int pbsam_system_bd_run(pbsam_system *sys, int n_steps);
  * trajectory.  Any pointer may be NULL. */
 int pbsam_system_bd_state(pbsam_system *sys, double *pos, double *quat, int *status, int *steps, double *time,
                           int *fevals, int on_device);
+/* NAM docking criteria (CBDnam::addMolContact + CBDnam::IsDocked, src/BDnam.cpp:38-41,
+ * 379-399): after each move of a running trajectory it is PBSAM_BD_DOCKED when, for
+ * some definition d with partner[d] == 1 (the species of molecule 1), at least
+ * ncontact[d] >= 1 of its pairs off[d] .. off[d+1]-1 have a surface gap (centre
+ * distance minus both radii, CMolecule::getSepDist) of at most dist[e] between sphere
+ * k1[e] of molecule 0 and sphere k2[e] of molecule 1 (0-based, PQR order).  n_defs = 0
+ * removes them.  After pbsam_system_bd_init; NAM only. */
+int pbsam_system_bd_set_contacts(pbsam_system *sys, int n_defs, const int *partner, const int *ncontact,
+                                 const int *off, const int *k1, const int *k2, const double *dist);
+/* The same from a contactdef file: CMolContact::readMolContact (every pair at distance
+ * sepdist, the bdnam command line's docking distance; src/contact.cpp:53-97) when
+ * sepdist > 0, readMolContactWithDist (a distance on every pair line, :105-145) when
+ * sepdist <= 0.  The molecule-1 type must be 0; a file that ends inside a definition
+ * is PBSAM_E_IO. */
+int pbsam_system_bd_set_contacts_file(pbsam_system *sys, const char *path, double sepdist);
 
 /* Molecule-type preparation (the reference's `pbsam mat` and `pbsam spol`).
  *

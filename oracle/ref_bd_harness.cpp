@@ -6,8 +6,10 @@
 // src/BDnam.cpp:48-150), seeds drand48 with a given seed instead of the clock,
 // places the molecules at the spec's poses, and runs the body of CBDnam::run's
 // loop (src/BDnam.cpp:196-243: compute_dt, computeForces inside f_DIST, the
-// drifts, makeMove) for n steps, writing the poses after every step.  No contact
-// definitions are loaded, so IsDocked is always false.
+// drifts, makeMove) for n steps, writing the poses after every step.  Contact
+// definitions are loaded as bdnam loads them (CContact::setSepDist,
+// CMolContact::readMolContact, CBDnam::addMolContact, src/BDnam_main.cpp:64-69) when
+// the spec has a `contact` entry; without one IsDocked is always false.
 //
 // The class's private members (makeMove, m_mols, the diffusion constants) are
 // reached by compiling this file with `private` defined as
@@ -17,6 +19,7 @@
 //       moltype <pqr> <imat dir> <exp dir> <exp name>     (exactly two)
 //       frame / mol <type> <x> <y> <z> <qw> <qx> <qy> <qz> (two molecules)
 //       bd <mode (0)> <n steps> <seed> <unused>
+//       contact <contactdef file> <docking distance>          (optional)
 // output: BDSTEP <steps> <status> <force evaluations> <time>, then POSE lines,
 // and TIME <wall seconds of the steps after the first> <their count> at the end;
 // statuses numbered 0 running, 1 escaped, 2 stuck, 3 docked; exit status 4 when
@@ -48,6 +51,8 @@ int main(int argc, char **argv)
   std::vector<std::vector<double> > poses;
   int mode = 0, nsteps = 0;
   long seed = 0, unused = 0;
+  std::string contactfile;
+  double dockdist = 0.0;
   std::string tok;
   while (in >> tok) {
     if (tok == "salt") in >> salt;
@@ -56,6 +61,7 @@ int main(int argc, char **argv)
     else if (tok == "frame") {}
     else if (tok == "mol") { int ty; std::vector<double> v(7); in >> ty; for (int k = 0; k < 7; k++) in >> v[k]; poses.push_back(v); }
     else if (tok == "bd") in >> mode >> nsteps >> seed >> unused;
+    else if (tok == "contact") in >> contactfile >> dockdist;
     else if (tok == "poles" || tok == "dump" || tok == "energy") { std::string x; in >> x; }
     else if (tok == "tol") { std::string a, b, c, d; in >> a >> b >> c >> d; }
     else if (tok == "bdp" || tok == "bddiff" || tok == "bdnoise") { std::string rest; std::getline(in, rest); }
@@ -67,6 +73,18 @@ int main(int argc, char **argv)
                                        (sdiel * PERMITTIVITY_VAC * KB * temperature));
   CSystem::initConstants(kappa, sdiel, temperature);
   CBDnam::initConstants(2);
+  if (!contactfile.empty()) {
+    CContact::setSepDist(dockdist);
+    std::vector<CMolContact> molcontactlist;
+    int moltype = -1;
+    std::streambuf *keep0 = std::cout.rdbuf();
+    std::ofstream sink0("/dev/null");
+    std::cout.rdbuf(sink0.rdbuf());
+    CMolContact::readMolContact(contactfile.c_str(), moltype, molcontactlist);
+    std::cout.rdbuf(keep0);
+    if (moltype != 0) return 2;
+    CBDnam::addMolContact(moltype, molcontactlist);
+  }
   std::vector<char *> f1, f2;
   for (int k = 0; k < 4; k++) {
     f1.push_back(const_cast<char *>(types[0][k].c_str()));

@@ -54,6 +54,13 @@ struct BDView {
   unsigned long long *lcg;            // [B] drand48 state (noise 1)
   double *nr_val;                     // [B] the second deviate kept by the polar method (noise 1)
   int *nr_saved;                      // [B]
+  // docking definitions of molecule 0 (NAM; CMolContact lists, src/contact.h): n_dock
+  // definitions, definition d needing dock_ncon[d] of its sphere pairs dock_off[d] ..
+  // dock_off[d+1]-1 (sphere dock_k1 of molecule 0, dock_k2 of molecule 1) within
+  // dock_dist of each other, counted only when dock_partner[d] is 1 (the partner species)
+  int n_dock;
+  const int *dock_partner, *dock_ncon, *dock_off, *dock_k1, *dock_k2;
+  const double *dock_dist;
 };
 
 // ---------------------------------------------------------------- Philox4x64-10
@@ -410,6 +417,33 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_move_kernel(Ctx c, 
           }
           __syncthreads();
         }
+      }
+    }
+    // CBDnam::IsDocked (src/BDnam.cpp:379-399) after a move that left the trajectory
+    // running: a definition is met when ncontact of its pairs have a surface gap
+    // (CMolecule::getSepDist, src/moldynamics.cpp:36-41) of at most their distance;
+    // the reference stops counting at ncontact, which decides the same
+    if (s_status == BD_RUNNING && v.n_dock > 0) {
+      __shared__ int s_hits;
+      const int o0 = bv.mol_off[0], o1 = bv.mol_off[1];
+      const double *cen = v.cen + (size_t)b * bv.S * 3;
+      for (int d = 0; d < v.n_dock && s_status == BD_RUNNING; d++) {
+        if (v.dock_partner[d] != 1 || v.dock_ncon[d] < 1) continue;
+        if (threadIdx.x == 0) s_hits = 0;
+        __syncthreads();
+        for (int e = v.dock_off[d] + threadIdx.x; e < v.dock_off[d + 1]; e += blockDim.x) {
+          const int s1 = o0 + v.dock_k1[e], s2 = o1 + v.dock_k2[e];
+          double dd[3];
+          for (int a = 0; a < 3; a++)
+            dd[a] = (pos[a] + cen[3 * s1 + a]) - (pos[3 + a] + cen[3 * s2 + a]);
+          min_image(c.prm.box, dd);
+          const double g = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]) - c.tv.rad[bv.sph_ts[s1]] -
+                           c.tv.rad[bv.sph_ts[s2]];
+          if (g <= v.dock_dist[e]) atomicAdd(&s_hits, 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && s_hits >= v.dock_ncon[d]) s_status = BD_DOCKED;
+        __syncthreads();
       }
     }
   } else {

@@ -159,6 +159,85 @@ extern "C" int pbsam_system_bd_run(pbsam_system *s, int n_steps)
   return PBSAM_OK;
 }
 
+extern "C" int pbsam_system_bd_set_contacts(pbsam_system *s, int n_defs, const int *partner, const int *ncontact,
+                                            const int *off, const int *k1, const int *k2, const double *dist)
+{
+  if (!s) return fail(PBSAM_E_BADARG, "null system");
+  BDHost *h = s->bd;
+  if (!h) return fail(PBSAM_E_STATE, "pbsam_system_bd_init has not been called");
+  if (h->p.mode != PBSAM_BD_NAM) return fail(PBSAM_E_BADARG, "docking contacts belong to NAM dynamics");
+  if (n_defs < 0 || (n_defs > 0 && (!partner || !ncontact || !off || off[0] != 0)))
+    return fail(PBSAM_E_BADARG, "bad contact definitions");
+  CK(cudaSetDevice(s->ctx->device));
+  int mo[3] = {0, 0, 0};
+  CK(cudaMemcpy(mo, s->c.bv.mol_off, 3 * sizeof(int), cudaMemcpyDeviceToHost));
+  const int n0 = mo[1] - mo[0], n1 = mo[2] - mo[1];
+  for (int d = 0; d < n_defs; d++)
+    if (off[d + 1] < off[d]) return fail(PBSAM_E_BADARG, "contact offsets must not decrease");
+  const int np = n_defs > 0 ? off[n_defs] : 0;
+  if (np > 0 && (!k1 || !k2 || !dist)) return fail(PBSAM_E_BADARG, "null contact pairs");
+  for (int e = 0; e < np; e++) {
+    if (k1[e] < 0 || k1[e] >= n0 || k2[e] < 0 || k2[e] >= n1)
+      return fail(PBSAM_E_BADARG, "a contact names a sphere the molecule does not have");
+    if (!std::isfinite(dist[e])) return fail(PBSAM_E_BADARG, "non-finite contact distance");
+  }
+  CK(cudaStreamSynchronize(h->st));
+  BDView &v = h->v;
+  v.n_dock = 0;
+  if (n_defs > 0) {
+    std::vector<int> hp(partner, partner + n_defs), hn(ncontact, ncontact + n_defs), ho(off, off + n_defs + 1);
+    std::vector<int> h1(k1, k1 + np), h2(k2, k2 + np);
+    std::vector<double> hd(dist, dist + np);
+    TRY(dput(h->bufs, &v.dock_partner, hp));
+    TRY(dput(h->bufs, &v.dock_ncon, hn));
+    TRY(dput(h->bufs, &v.dock_off, ho));
+    TRY(dput(h->bufs, &v.dock_k1, h1));
+    TRY(dput(h->bufs, &v.dock_k2, h2));
+    TRY(dput(h->bufs, &v.dock_dist, hd));
+    v.n_dock = n_defs;
+  }
+  // the step graph holds the view it was captured with: capture again at the next run
+  if (h->exec) { cudaGraphExecDestroy(h->exec); h->exec = nullptr; }
+  if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  return PBSAM_OK;
+}
+
+// contactdef reader (CMolContact::readMolContact, src/contact.cpp:53-97, and
+// readMolContactWithDist, :105-145): molecule-1 type (0 for NAM), the number of
+// definitions, then per definition the partner type, the contacts needed, the number
+// of pairs and the pairs (sphere of molecule 1, sphere of molecule 2, and a distance
+// when sepdist <= 0).  A file that ends inside a definition is refused.
+extern "C" int pbsam_system_bd_set_contacts_file(pbsam_system *s, const char *path, double sepdist)
+{
+  if (!s || !path) return fail(PBSAM_E_BADARG, "null argument");
+  std::ifstream in(path);
+  if (!in) return fail(PBSAM_E_IO, std::string("cannot open contact file ") + path);
+  int mol1type = -1, ndef = 0;
+  if (!(in >> mol1type >> ndef)) return fail(PBSAM_E_IO, std::string("contact file header: ") + path);
+  if (mol1type != 0) return fail(PBSAM_E_BADARG, "NAM contact definitions are for molecule type 0");
+  std::vector<int> partner, ncon, off(1, 0), k1, k2;
+  std::vector<double> dist;
+  int mol2type;
+  while (in >> mol2type) {
+    int nc = 0, npair = 0;
+    if (!(in >> nc >> npair) || npair < 0) return fail(PBSAM_E_IO, std::string("contact definition: ") + path);
+    for (int n = 0; n < npair; n++) {
+      int a, b;
+      double dd = sepdist;
+      if (!(in >> a >> b) || (sepdist <= 0 && !(in >> dd)))
+        return fail(PBSAM_E_IO, std::string("contact file ends inside a definition: ") + path);
+      k1.push_back(a);
+      k2.push_back(b);
+      dist.push_back(dd);
+    }
+    partner.push_back(mol2type);
+    ncon.push_back(nc);
+    off.push_back((int)k1.size());
+  }
+  return pbsam_system_bd_set_contacts(s, (int)partner.size(), partner.data(), ncon.data(), off.data(), k1.data(),
+                                      k2.data(), dist.data());
+}
+
 extern "C" int pbsam_system_bd_state(pbsam_system *s, double *pos, double *quat, int *status, int *steps,
                                      double *time, int *fevals, int on_device)
 {

@@ -46,6 +46,11 @@ PBSAM_BD_NAM = 0
 PBSAM_BD_MULTI = 1
 PBSAM_BD_NOISE_PHILOX = 0
 PBSAM_BD_NOISE_DRAND48 = 1
+PBSAM_BD_RUNNING = 0
+PBSAM_BD_ESCAPED = 1
+PBSAM_BD_STUCK = 2
+PBSAM_BD_DOCKED = 3
+PBSAM_BD_FAILED = 4
 BD_STATUS = {0: "RUNNING", 1: "ESCAPED", 2: "STUCK", 3: "DOCKED", 4: "FAILED"}
 
 
@@ -97,6 +102,8 @@ SIGNATURES = {
     "pbsam_expan_reexpand": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int, _P, _P, _P,
                                             ctypes.c_int]),
     "pbsam_quat_angles": (ctypes.c_int, [_DP, _DP]),
+    "pbsam_system_bd_set_contacts": (ctypes.c_int, [_P, ctypes.c_int, _IP, _IP, _IP, _IP, _IP, _DP]),
+    "pbsam_system_bd_set_contacts_file": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_double]),
     "pbsam_last_error": (ctypes.c_char_p, []),
 }
 
@@ -373,6 +380,23 @@ class Molecules:
     def bd_run(self, n_steps):
         """Queue n_steps steps of every running trajectory (asynchronous)."""
         _check(lib().pbsam_system_bd_run(self.handle, int(n_steps)))
+
+    def bd_set_contacts(self, defs):
+        """NAM docking criteria: defs = [(partner, ncontact, [(k1, k2, dist), ...]), ...]."""
+        partner = np.array([d[0] for d in defs], dtype=np.int32)
+        ncon = np.array([d[1] for d in defs], dtype=np.int32)
+        off = np.concatenate([[0], np.cumsum([len(d[2]) for d in defs])]).astype(np.int32)
+        pairs = [pr for d in defs for pr in d[2]]
+        k1 = np.array([pr[0] for pr in pairs], dtype=np.int32)
+        k2 = np.array([pr[1] for pr in pairs], dtype=np.int32)
+        dist = np.array([pr[2] for pr in pairs], dtype=np.float64)
+        ip = lambda a: a.ctypes.data_as(_IP)
+        _check(lib().pbsam_system_bd_set_contacts(self.handle, len(defs), ip(partner), ip(ncon), ip(off), ip(k1),
+                                                  ip(k2), _dptr(dist)))
+
+    def bd_set_contacts_file(self, path, sepdist):
+        """NAM docking criteria from a contactdef file (sepdist <= 0: per-pair distances)."""
+        _check(lib().pbsam_system_bd_set_contacts_file(self.handle, path.encode(), sepdist))
 
     def bd_state(self):
         """dict(pos[n_sys, n_mol, 3], quat[n_sys, n_mol, 4], status, steps, time, fevals)."""

@@ -198,3 +198,83 @@ def test_reference_stream_vs_reference_bdm(tmp_path, scale):
         check_step(g, 0, dict(ref[k], pos=np.array(ref[k]["pos"]), quat=np.array(ref[k]["quat"])))
     mol.close()
     ctx.close()
+
+
+def _contact_files(tmp_path, dist):
+    """Every sphere pair of the two tiny molecules, one contact needed: a contactdef
+    file for readMolContact (distance from the command line) and the same with a
+    distance on every pair line (readMolContactWithDist)."""
+    na = sum(1 for ln in open(os.path.join(golden_dir("tiny"), "molA.pqr")) if "CEN" in ln)
+    nb = sum(1 for ln in open(os.path.join(golden_dir("tiny"), "molB.pqr")) if "CEN" in ln)
+    pairs = [(i, j) for i in range(na) for j in range(nb)]
+    f1, f2 = os.path.join(tmp_path, "contact.dat"), os.path.join(tmp_path, "contact_dist.dat")
+    with open(f1, "w") as fh:
+        fh.write("0 1\n1 1 %d\n" % len(pairs) + "".join("%d %d\n" % pr for pr in pairs))
+    with open(f2, "w") as fh:
+        fh.write("0 1\n1 1 %d\n" % len(pairs) + "".join("%d %d %r\n" % (pr + (dist,)) for pr in pairs))
+    return f1, f2, pairs
+
+
+def test_docking_vs_reference_bdnam(tmp_path):
+    """NAM docking (CMolContact::readMolContact, CBDnam::IsDocked): the reference's own
+    CBDnam with a contact file (every sphere pair, one contact within 5.5 A) docks at
+    step 30 of this run; the CUDA path with the reference's noise stream repeats every
+    step and docks at the same step.  The same definitions read with per-pair distances
+    and given as arrays agree; without them the trajectory keeps running."""
+    import subprocess
+    import pbsam_b200 as pb
+    exe = oracle.ref_bd_harness()
+    if exe is None:
+        pytest.skip("reference BD harness not built")
+    dist, seed, n = 5.5, 12345, 34
+    f1, f2, pairs = _contact_files(str(tmp_path), dist)
+    fr = gap5_frame()
+    ctx, types, P = tiny_ctx()
+    spec = os.path.join(str(tmp_path), "dock.txt")
+    oracle.write_bd_spec(spec, oracle.golden_moltypes(golden_dir("tiny")), fr, 0, n, seed, 0, DTR, DROT,
+                         salt=P["salt"], idiel=P["idiel"], poles=P["poles"])
+    with open(spec, "a") as fh:
+        fh.write("contact %s %r\n" % (f1, dist))
+    subprocess.check_call([exe, spec, spec + ".out"], env=dict(os.environ, OMP_NUM_THREADS="1"),
+                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    ref = []
+    for ln in open(spec + ".out"):
+        t = ln.split()
+        if t[0] == "BDSTEP":
+            ref.append(dict(status=int(t[2]), fevals=int(t[3]), time=float(t[4]), steps=int(t[1]), pos=[], quat=[]))
+        elif t[0] == "POSE":
+            v = [float(x) for x in t[2:]]
+            ref[-1]["pos"].append(v[:3])
+            ref[-1]["quat"].append(v[3:])
+    assert ref[-1]["status"] == pb.PBSAM_BD_DOCKED and 10 < len(ref) < n, (len(ref), ref[-1]["status"])
+    mols = []
+    try:
+        for how in ("file", "file_dist", "arrays", "none"):
+            m = ctx.molecules(types, n_systems=1)
+            mols.append(m)
+            m.set_poses(np.array([[x[1] for x in fr]]), np.array([[x[2] for x in fr]]))
+            m.bd_init(DTR, DROT, mode=0, seed=seed, noise=pb.PBSAM_BD_NOISE_DRAND48)
+            if how == "file":
+                m.bd_set_contacts_file(f1, dist)
+            elif how == "file_dist":
+                m.bd_set_contacts_file(f2, 0.0)
+            elif how == "arrays":
+                m.bd_set_contacts([(1, 1, [(i, j, dist) for i, j in pairs])])
+            for k in range(len(ref)):
+                m.bd_run(1)
+                g = m.bd_state()
+                r = dict(ref[k], pos=np.array(ref[k]["pos"]), quat=np.array(ref[k]["quat"]))
+                if how == "none" and k == len(ref) - 1:
+                    r["status"] = pb.PBSAM_BD_RUNNING
+                check_step(g, 0, r)
+            m.bd_run(2)                     # a docked trajectory stays as it is
+            g = m.bd_state()
+            if how != "none":
+                assert g["status"][0] == pb.PBSAM_BD_DOCKED and g["steps"][0] == len(ref)
+        # a contact naming a sphere the molecule does not have is refused
+        with pytest.raises(pb.PbsamError):
+            mols[0].bd_set_contacts([(1, 1, [(99, 0, dist)])])
+    finally:
+        for m in mols:
+            m.close()
+        ctx.close()
