@@ -300,6 +300,17 @@ int pbsam_system_bd_set_contacts(pbsam_system *sys, int n_defs, const int *partn
  * is PBSAM_E_IO. */
 int pbsam_system_bd_set_contacts_file(pbsam_system *sys, const char *path, double sepdist);
 
+/* bdm restart configurations, host only (no device needed): readConfigWithMolType
+ * (src/readutil.cpp:835-886, used by CBDmulti::restartConfig, src/BDmulti.cpp:286-316)
+ * and CMolecule::saveConfig (src/molecule.cpp:255-269).  One molecule per line:
+ * "x y z qw qx qy qz type".  pbsam_config_read stores up to max_mol molecules (pos
+ * [3 each], quat [4 each], moltype; any may be NULL) and sets *n_mol to the number in
+ * the file (PBSAM_E_BADARG when it exceeds max_mol; PBSAM_E_IO for a file that ends
+ * inside a molecule or has a field that is not a number).  pbsam_config_write writes
+ * at full precision (the reference's stream default keeps 6 digits). */
+int pbsam_config_read(const char *path, int max_mol, int *n_mol, double *pos, double *quat, int *moltype);
+int pbsam_config_write(const char *path, int n_mol, const double *pos, const double *quat, const int *moltype);
+
 /* Molecule-type preparation (the reference's `pbsam mat` and `pbsam spol`).
  *
  * Surface-integral matrices of a molecule's spheres: replaces the CMolecule IMat

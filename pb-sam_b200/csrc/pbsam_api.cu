@@ -1272,3 +1272,45 @@ extern "C" int pbsam_system_phase_ms(const pbsam_system *s, double *ms)
 // measured device rates for the roofline (uses the helpers above)
 #include "pbsam_probe.cu"
 #include "pbsam_expan.cu"
+
+// bdm restart configurations (host only): readConfigWithMolType (src/readutil.cpp:835-886)
+// and CMolecule::saveConfig (src/molecule.cpp:255-269), one molecule per line,
+// "x y z qw qx qy qz type".  The reader takes whitespace-separated fields, eight per
+// molecule; a file that ends inside a molecule is refused rather than cut short.
+extern "C" int pbsam_config_read(const char *path, int max_mol, int *n_mol, double *pos, double *quat, int *moltype)
+{
+  if (!path || !n_mol || max_mol < 0) return fail(PBSAM_E_BADARG, "bad argument");
+  std::ifstream in(path);
+  if (!in) return fail(PBSAM_E_IO, std::string("cannot open configuration ") + path);
+  int n = 0;
+  double v[7];
+  while (in >> v[0]) {
+    int t;
+    for (int k = 1; k < 7; k++)
+      if (!(in >> v[k])) return fail(PBSAM_E_IO, std::string("configuration ends inside a molecule: ") + path);
+    if (!(in >> t)) return fail(PBSAM_E_IO, std::string("configuration ends inside a molecule: ") + path);
+    if (n < max_mol) {
+      if (pos) for (int k = 0; k < 3; k++) pos[3 * n + k] = v[k];
+      if (quat) for (int k = 0; k < 4; k++) quat[4 * n + k] = v[3 + k];
+      if (moltype) moltype[n] = t;
+    }
+    n++;
+  }
+  if (!in.eof()) return fail(PBSAM_E_IO, std::string("configuration has a field that is not a number: ") + path);
+  *n_mol = n;
+  if (n > max_mol) return fail(PBSAM_E_BADARG, "the configuration holds more molecules than max_mol");
+  return PBSAM_OK;
+}
+
+extern "C" int pbsam_config_write(const char *path, int n_mol, const double *pos, const double *quat,
+                                  const int *moltype)
+{
+  if (!path || n_mol < 0 || (n_mol > 0 && (!pos || !quat || !moltype))) return fail(PBSAM_E_BADARG, "bad argument");
+  FILE *f = std::fopen(path, "w");
+  if (!f) return fail(PBSAM_E_IO, std::string("cannot write configuration ") + path);
+  for (int i = 0; i < n_mol; i++)
+    std::fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g %.17g %d\n", pos[3 * i], pos[3 * i + 1], pos[3 * i + 2],
+                 quat[4 * i], quat[4 * i + 1], quat[4 * i + 2], quat[4 * i + 3], moltype[i]);
+  const bool ok = std::fclose(f) == 0;
+  return ok ? PBSAM_OK : fail(PBSAM_E_IO, std::string("writing configuration ") + path);
+}

@@ -104,6 +104,8 @@ SIGNATURES = {
     "pbsam_quat_angles": (ctypes.c_int, [_DP, _DP]),
     "pbsam_system_bd_set_contacts": (ctypes.c_int, [_P, ctypes.c_int, _IP, _IP, _IP, _IP, _IP, _DP]),
     "pbsam_system_bd_set_contacts_file": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_double]),
+    "pbsam_config_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _IP, _DP, _DP, _IP]),
+    "pbsam_config_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _DP, _DP, _IP]),
     "pbsam_last_error": (ctypes.c_char_p, []),
 }
 
@@ -157,6 +159,25 @@ def bd_params(mode=PBSAM_BD_NAM, **kw):
 
 def _dptr(a):
     return a.ctypes.data_as(_DP)
+
+
+def config_read(path):
+    """bdm restart configuration: (pos [n][3], quat [n][4], moltype [n])."""
+    n = ctypes.c_int()
+    rc = lib().pbsam_config_read(path.encode(), 0, ctypes.byref(n), None, None, None)
+    if rc != 0 and n.value == 0:
+        _check(rc)
+    pos, quat, mt = np.zeros((n.value, 3)), np.zeros((n.value, 4)), np.zeros(n.value, dtype=np.int32)
+    _check(lib().pbsam_config_read(path.encode(), n.value, ctypes.byref(n), _dptr(pos), _dptr(quat),
+                                   mt.ctypes.data_as(_IP)))
+    return pos, quat, mt
+
+
+def config_write(path, pos, quat, moltype):
+    pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+    quat = np.ascontiguousarray(quat, dtype=np.float64).reshape(-1, 4)
+    mt = np.ascontiguousarray(moltype, dtype=np.int32)
+    _check(lib().pbsam_config_write(path.encode(), len(pos), _dptr(pos), _dptr(quat), mt.ctypes.data_as(_IP)))
 
 
 def quat_angles(q):
