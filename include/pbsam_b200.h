@@ -300,6 +300,30 @@ int pbsam_system_bd_set_contacts(pbsam_system *sys, int n_defs, const int *partn
  * is PBSAM_E_IO. */
 int pbsam_system_bd_set_contacts_file(pbsam_system *sys, const char *path, double sepdist);
 
+/* Forces, torques and statuses of the last evaluation of every system, without
+ * evaluating again (after a group evaluation, pbsam_group_compute_forces). */
+int pbsam_system_get_forces(pbsam_system *sys, double *force, double *torque, int *status, int on_device);
+
+/* Groups of system handles (no reference counterpart: the reference runs one
+ * trajectory per process).  The systems of several handles, each with its own
+ * molecule list and sphere counts and possibly its own context (pole order), are
+ * evaluated in one launch, one CTA per system, longest first: at creation by the
+ * square of the sphere count, after pbsam_group_tune by the device time of each
+ * system's last evaluation.  Results stay in each handle (pbsam_system_get_forces,
+ * pbsam_system_bd_state).  Every handle on the same device; a handle belongs to at
+ * most one group at a time and is not used on its own while a group call runs. */
+typedef struct pbsam_group pbsam_group;
+int pbsam_group_create(int n, pbsam_system *const *systems, pbsam_group **out);
+int pbsam_group_destroy(pbsam_group *g);
+/* One launch over every system of every handle (CMolecule::computeForces of each). */
+int pbsam_group_compute_forces(pbsam_group *g);
+/* Reorder the systems by the device time of their last evaluation, longest first. */
+int pbsam_group_tune(pbsam_group *g);
+/* n_steps BD steps of every trajectory of every handle (each pbsam_system_bd_init'ed,
+ * contact lists included): one CUDA graph per step, the same steps as each handle's
+ * own pbsam_system_bd_run. */
+int pbsam_group_bd_run(pbsam_group *g, int n_steps);
+
 /* bdm restart configurations, host only (no device needed): readConfigWithMolType
  * (src/readutil.cpp:835-886, used by CBDmulti::restartConfig, src/BDmulti.cpp:286-316)
  * and CMolecule::saveConfig (src/molecule.cpp:255-269).  One molecule per line:

@@ -1265,6 +1265,7 @@ extern "C" int pbsam_system_phase_ms(const pbsam_system *s, double *ms)
 
 // Brownian dynamics on the force path (uses the helpers above)
 #include "pbsam_bd_host.cu"
+#include "pbsam_group.cu"
 
 // fixed-buffer variant of the IMat builder (uses the helpers above)
 #include "pbsam_static_imat.cu"
@@ -1313,4 +1314,17 @@ extern "C" int pbsam_config_write(const char *path, int n_mol, const double *pos
                  quat[4 * i], quat[4 * i + 1], quat[4 * i + 2], quat[4 * i + 3], moltype[i]);
   const bool ok = std::fclose(f) == 0;
   return ok ? PBSAM_OK : fail(PBSAM_E_IO, std::string("writing configuration ") + path);
+}
+
+extern "C" int pbsam_system_get_forces(pbsam_system *s, double *force, double *torque, int *status, int on_device)
+{
+  if (!s) return fail(PBSAM_E_BADARG, "null system");
+  CK(cudaSetDevice(s->ctx->device));
+  const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const size_t n = (size_t)s->B * s->nmol * 3;
+  if (force) CK(cudaMemcpyAsync(force, s->c.bv.force, n * sizeof(double), k, s->stream));
+  if (torque) CK(cudaMemcpyAsync(torque, s->c.bv.torque, n * sizeof(double), k, s->stream));
+  if (status) CK(cudaMemcpyAsync(status, s->c.bv.status, (size_t)s->B * sizeof(int), k, s->stream));
+  if (!on_device) CK(cudaStreamSynchronize(s->stream));
+  return PBSAM_OK;
 }

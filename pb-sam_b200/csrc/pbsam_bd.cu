@@ -180,10 +180,10 @@ __device__ void bd_rotate_centres(const Ctx &c, const BDView &v, int b, int i)
 }
 
 // time step and force mask of every running system
-__global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_kernel(Ctx c, BDParams p, BDView v)
+__device__ void bd_pre_body(const Ctx &c, const BDParams &p, const BDView &v, int b)
 {
   const BatchView &bv = c.bv;
-  const int b = blockIdx.x, nmol = bv.nmol;
+  const int nmol = bv.nmol;
   if (b >= bv.B) return;
   if (v.status[b] != BD_RUNNING) {
     if (threadIdx.x == 0) v.need[b] = 0;
@@ -245,6 +245,10 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_kernel(Ctx c, B
     v.dt[b] = bd_dt(p, md);
     v.need[b] = md < p.interact_cut;
   }
+}
+__global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_kernel(Ctx c, BDParams p, BDView v)
+{
+  bd_pre_body(c, p, v, blockIdx.x);
 }
 
 // The reference's own stream (noise 1), per system: drand48 (POSIX: X <- (0x5DEECE66D X
@@ -352,13 +356,13 @@ __device__ int bd_rotate(const Ctx &c, const BDParams &p, const BDView &v, int b
   return tries;
 }
 
-__global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_move_kernel(Ctx c, BDParams p, BDView v)
+__device__ void bd_move_body(const Ctx &c, const BDParams &p, const BDView &v, int b)
 {
   extern __shared__ double bd_rel[];          // [max spheres of a molecule][3]
   __shared__ double sm[8];
   __shared__ int s_status;
   const BatchView &bv = c.bv;
-  const int b = blockIdx.x, nmol = bv.nmol;
+  const int nmol = bv.nmol;
   if (b >= bv.B || v.status[b] != BD_RUNNING) return;
   const double dt = v.dt[b];
   const bool need = v.need[b] != 0;
@@ -467,6 +471,25 @@ __global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_move_kernel(Ctx c, 
     v.time[b] += dt;
     if (need) v.fevals[b]++;
   }
+}
+__global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_move_kernel(Ctx c, BDParams p, BDView v)
+{
+  bd_move_body(c, p, v, blockIdx.x);
+}
+
+// Groups of system handles (pbsam_group_*): one launch over every system of every
+// handle, CTA k taking work[k] = (handle, system); handles keep their own views.
+__global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_pre_group_kernel(const Ctx *cs, const BDParams *ps,
+                                                                             const BDView *vs, const int2 *work)
+{
+  const int2 w = work[blockIdx.x];
+  bd_pre_body(cs[w.x], ps[w.x], vs[w.x], w.y);
+}
+__global__ void __launch_bounds__(PBSAM_BD_THREADS) pbsam_bd_move_group_kernel(const Ctx *cs, const BDParams *ps,
+                                                                              const BDView *vs, const int2 *work)
+{
+  const int2 w = work[blockIdx.x];
+  bd_move_body(cs[w.x], ps[w.x], vs[w.x], w.y);
 }
 
 __global__ void pbsam_bd_init_kernel(Ctx c, BDParams p, BDView v)

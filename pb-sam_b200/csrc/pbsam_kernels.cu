@@ -2441,6 +2441,32 @@ __global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_kernel(Ctx c, const i
   crew_finish(tm, cw);
 }
 
+// One launch over the systems of several handles (pbsam_group_*), possibly of
+// different molecule lists, sphere counts and pole orders: CTA k evaluates system
+// work[k].y of handle work[k].x with that handle's context view (one CTA per system;
+// the dynamic shared memory is that of the largest pole order in the group).
+__global__ void __launch_bounds__(PBSAM_TEAM) pbsam_forces_group_kernel(const Ctx *cs, const int2 *work)
+{
+  extern __shared__ double2 dsm[];
+  const int2 w = work[blockIdx.x];
+  const Ctx &c = cs[w.x];
+  if (threadIdx.x == 0 && c.T.NP <= PBSAM_SMEM_IMAT_NP) {
+    unsigned dsz;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dsz));
+    if (dsz >= forces_smem_bytes(c.T.NP))
+      *(int *)((char *)dsm + team_smem_bytes(c.T.NP) + imat_stride(c.T.NP * c.T.NP) * sizeof(double) + 8) = 0;
+  }
+  __syncthreads();
+  __shared__ double red[PBSAM_TEAM];
+  __shared__ CrewCmd cmd;
+  const Team tm{(int)threadIdx.x, (int)blockDim.x};
+  const Crew cw{0, 1, &cmd};
+  const int b = w.y;
+  if (b >= c.bv.B) return;
+  if (c.bv.fmask && c.bv.fmask[b] == 0) return;
+  forces_body(tm, c, cw, b, dsm, red);
+}
+
 // interaction energy on the state left by the last force evaluation.
 // lab == 0: the reference's convention (src/moldynamics.cpp:358-386,
 //   src/molecule.cpp:1850-1890): unrotated sphere centres and molecule-frame H, so

@@ -105,6 +105,12 @@ SIGNATURES = {
     "pbsam_system_bd_set_contacts": (ctypes.c_int, [_P, ctypes.c_int, _IP, _IP, _IP, _IP, _IP, _DP]),
     "pbsam_system_bd_set_contacts_file": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_double]),
     "pbsam_config_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _IP, _DP, _DP, _IP]),
+    "pbsam_system_get_forces": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int]),
+    "pbsam_group_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P), ctypes.POINTER(_P)]),
+    "pbsam_group_destroy": (ctypes.c_int, [_P]),
+    "pbsam_group_compute_forces": (ctypes.c_int, [_P]),
+    "pbsam_group_tune": (ctypes.c_int, [_P]),
+    "pbsam_group_bd_run": (ctypes.c_int, [_P, ctypes.c_int]),
     "pbsam_config_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _DP, _DP, _IP]),
     "pbsam_last_error": (ctypes.c_char_p, []),
 }
@@ -159,6 +165,33 @@ def bd_params(mode=PBSAM_BD_NAM, **kw):
 
 def _dptr(a):
     return a.ctypes.data_as(_DP)
+
+
+class Group:
+    """Several Molecules handles (different molecule lists, sphere counts, contexts)
+    evaluated in one launch, longest systems first (pbsam_group_*)."""
+
+    def __init__(self, handles):
+        self.handles = list(handles)
+        arr = (_P * len(self.handles))(*[h.handle for h in self.handles])
+        g = _P()
+        _check(lib().pbsam_group_create(len(self.handles), arr, ctypes.byref(g)))
+        self.handle = g
+
+    def compute_forces(self):
+        _check(lib().pbsam_group_compute_forces(self.handle))
+        return [h.get_forces() for h in self.handles]
+
+    def tune(self):
+        _check(lib().pbsam_group_tune(self.handle))
+
+    def bd_run(self, n_steps):
+        _check(lib().pbsam_group_bd_run(self.handle, n_steps))
+
+    def close(self):
+        if self.handle:
+            _check(lib().pbsam_group_destroy(self.handle))
+            self.handle = None
 
 
 def config_read(path):
@@ -324,6 +357,14 @@ class Molecules:
         t = np.zeros((self.n_systems, self.n_mol, 3))
         st = np.zeros(self.n_systems, dtype=np.int32)
         _check(lib().pbsam_system_compute_forces(self.handle, f.ctypes.data, t.ctypes.data, st.ctypes.data, 0))
+        return f, t, st
+
+    def get_forces(self):
+        """Forces, torques and statuses of the last evaluation (e.g. by a Group)."""
+        f = np.zeros((self.n_systems, self.n_mol, 3))
+        t = np.zeros((self.n_systems, self.n_mol, 3))
+        st = np.zeros(self.n_systems, dtype=np.int32)
+        _check(lib().pbsam_system_get_forces(self.handle, f.ctypes.data, t.ctypes.data, st.ctypes.data, 0))
         return f, t, st
 
     def compute_forces_device(self, force_ptr, torque_ptr, status_ptr):
