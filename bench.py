@@ -276,6 +276,14 @@ def run_ours(args):
             if out is not None:
                 out["bd_exact"] = bdx
                 out["gpu_launches"] += bdx["gpu_launches"]
+        if args.bd_uneven:
+            try:
+                bdu = run_bd_uneven(args, local, rank, world, dist)
+            except Exception as e:
+                bdu = {"error": "%s: %s" % (type(e).__name__, e), "gpu_launches": 0}
+            if out is not None:
+                out["bd_uneven"] = bdu
+                out["gpu_launches"] += bdu["gpu_launches"]
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -485,6 +493,99 @@ def run_bd(args, local, rank, world, dist, exact=False, specs=None):
     sysb.close()
     ctx.close()
     return out, specs
+
+
+def run_bd_uneven(args, local, rank, world, dist):
+    """BD steps/s of 1024 two-molecule trajectories whose molecules have uneven sphere
+    counts (8 A and 8 B molecules of 10-60 spheres, every A-B pair a handle of 16
+    trajectories), exact form with adjoint forces: every step of every handle in one
+    group launch (one CUDA graph per step, longest systems first), against the same
+    handles stepped by their own graphs on their own streams."""
+    import torch
+    import pbsam_b200 as pb
+    from pbsam_b200 import replicas, workload
+    cfg = dict(workload.BD_UNEVEN)
+    A, B = workload.uneven_molecules(cfg)
+    t0 = time.time()
+    specs, prep_t, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds_p10, mols=A + B)
+    prep_t = {"molecules_s": round(time.time() - t0, 1)}
+    t0 = time.time()
+    ctx, types = workload.open_context(cfg, specs, device=local, exact=1, exact_tol=args.exact_tol)
+    prep_t["context_s"] = round(time.time() - t0, 1)
+    n = cfg["n_types"]
+    stream = torch.cuda.current_stream()
+
+    def handles(streams):
+        hs = []
+        for i in range(n):
+            for j in range(n):
+                h = ctx.molecules([types[i], types[n + j]], n_systems=cfg["per_pair"])
+                h.set_stream(streams[len(hs)].cuda_stream)
+                pcfg = dict(cfg, pose_seed=cfg["pose_seed"] + 64 * i + j)
+                pos, quat = workload.bd_start(pcfg, [A[i], B[j]], cfg["per_pair"], rank=rank)
+                h.set_poses(pos, quat)
+                ext = max(A[i].extent(), B[j].extent())
+                dtr, drot = workload.stokes_einstein(ext, cfg["viscosity"], cfg["temperature"])
+                h.bd_init([0.0, dtr], [drot, drot], mode=0, seed=97 + 64 * i + j + 4096 * rank,
+                          escape_dist=cfg["escape"], dt_min=cfg["dt_min"], dt_max=cfg["dt_max"], dt_ref=0.0,
+                          dt_div=cfg["dt_gap"] / (cfg["dt_max"] - cfg["dt_min"]))
+                hs.append(h)
+        return hs
+
+    def steps_of(hs):
+        return int(sum(int(np.sum(h.bd_state()["steps"])) for h in hs))
+
+    out = {}
+    timings = {}
+    finals = {}
+    for mode in ("group", "own"):
+        # "own": every handle on a stream of its own, so that their graphs run side by side
+        streams = [stream] * (n * n) if mode == "group" else [torch.cuda.Stream() for _ in range(n * n)]
+        hs = handles(streams)
+        g = pb.Group(hs) if mode == "group" else None
+        run = (lambda k: g.bd_run(k)) if mode == "group" else (lambda k: [h.bd_run(k) for h in hs])
+        run(args.warmup)
+        if g is not None:
+            g.tune()
+        torch.cuda.synchronize()
+        s0 = steps_of(hs)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(gpu_id_for_smi(local)) as clk, torch.cuda.nvtx.range("bd_uneven_" + mode):
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for st in set(streams):
+                st.wait_event(e0)
+            run(args.bd_steps)
+            for st in set(streams):
+                stream.wait_stream(st)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = replicas.max_over_ranks(e0.elapsed_time(e1), dist if world > 1 else None)
+        units = replicas.sum_over_ranks(steps_of(hs) - s0, dist if world > 1 else None)
+        timings[mode] = (units / (ms * 1e-3), ms, clk.summary())
+        finals[mode] = [h.bd_state() for h in hs]
+        if g is not None:
+            g.close()
+        for h in hs:
+            h.close()
+    same = all(np.array_equal(a[k], b[k]) for a, b in zip(finals["group"], finals["own"]) for k in a)
+    sizes = [len(m.radii) for m in A + B]
+    out = {"metric": "BD steps/s (two-molecule bdnam trajectories, molecules of 10-60 spheres, p=10), exact form "
+                     "with adjoint forces, one group launch per step",
+           "value": timings["group"][0], "unit": "BD steps/s", "ms_per_step": timings["group"][1] / args.bd_steps,
+           "steps": args.bd_steps, "warmup": args.warmup, "dtype": "f64",
+           "config": {"workload": "%d trajectories: %d x %d molecule pairs x %d, sphere counts %s (A) and %s (B), "
+                                  "300 charges in [-0.6, 0.6] with net +2/-2, start 50 A, escape 150 A; exact_tol %g" % (
+                                      n * n * cfg["per_pair"], n, n, cfg["per_pair"], sizes[:n], sizes[n:],
+                                      args.exact_tol),
+                      "handles": n * n},
+           "own_launches": {"value": timings["own"][0], "ms_per_step": timings["own"][1] / args.bd_steps,
+                            "note": "each handle's own step graph, every handle on a stream of its own"},
+           "vs_own_launches": timings["group"][0] / timings["own"][0],
+           "same_trajectories": bool(same),
+           "gpu_launches": 3 * args.bd_steps, "clocks": timings["group"][2], "prep": prep_t}
+    ctx.close()
+    return out
 
 
 def reference_bd_step_seconds(cfg, files, pos, quat, limit_s, workdir, steps=3, variant="fast", seed=1):
@@ -762,6 +863,8 @@ def main():
     ap.add_argument("--bd-exact", type=int, default=1,
                     help="also time the BD workload in the exact form with adjoint forces")
     ap.add_argument("--bd-steps", type=int, default=20, help="timed BD steps")
+    ap.add_argument("--bd-uneven", type=int, default=1,
+                    help="also time BD of molecules with uneven sphere counts (groups of handles)")
     ap.add_argument("--exact-tol", type=float, default=1e-10,
                     help="exact BD leg: pbsam_params.exact_tol (the leg reports the force error against 1e-14)")
     ap.add_argument("--exact-relax", type=float, default=1.0, help="exact BD leg: pbsam_params.exact_relax")

@@ -36,6 +36,26 @@ BD_P10 = dict(n_sph=35, r=(3.0, 6.0), n_q=1200, q_amp=0.6, nets=(2.0, -2.0), pol
               dt_gap=30.0, viscosity=0.89e-3, temperature=298.15, min_gap=1.0)
 
 
+# Brownian dynamics of molecules with uneven sphere counts (SURVEY config 3's 10..60
+# spheres per molecule, charges as config 0): n_types "A" molecules (net +2) and
+# n_types "B" molecules (net -2), every A-B pair a handle of per_pair trajectories.
+BD_UNEVEN = dict(n_types=8, sizes=(10, 60), r=(3.0, 6.0), n_q=300, q_amp=0.6, nets=(2.0, -2.0), poles=10, salt=0.05,
+                 idiel=4.0, seed=4100, pose_seed=4200, start=50.0, escape=150.0, dt_min=0.02, dt_max=2.0,
+                 dt_gap=30.0, viscosity=0.89e-3, temperature=298.15, min_gap=1.0, per_pair=16)
+
+
+def uneven_molecules(cfg):
+    """(A molecules, B molecules) with sphere counts drawn uniformly from cfg['sizes']."""
+    rng = np.random.default_rng(cfg["seed"])
+    lo, hi = cfg["sizes"]
+    out = []
+    for side, net in enumerate(cfg["nets"]):
+        out.append([synth.make_molecule(int(rng.integers(lo, hi + 1)), cfg["r"][0], cfg["r"][1], cfg["n_q"],
+                                        cfg["q_amp"], net, seed=cfg["seed"] + 100 * (side + 1) + k)
+                    for k in range(cfg["n_types"])])
+    return out[0], out[1]
+
+
 def stokes_einstein(radius_A, viscosity=0.89e-3, temperature=298.15):
     """(translational A^2/ps, rotational rad^2/ps) diffusion constants of a sphere."""
     kT = 1.3806503e-23 * temperature
@@ -136,12 +156,13 @@ def write_inputs(cfg, specs, outdir):
     return files
 
 
-def prepare(cfg, device=0, outdir=None, selfpol_rounds=1700):
-    """Build IMats and self-polarized expansions on the GPU; returns
-    (moltype specs for CSystem.create_moltype, prep timings, file specs or None)."""
+def prepare(cfg, device=0, outdir=None, selfpol_rounds=1700, mols=None):
+    """Build IMats and self-polarized expansions on the GPU (of the config's molecules,
+    or of mols); returns (moltype specs for CSystem.create_moltype, prep timings, file
+    specs or None)."""
     import time
     import pbsam_b200 as pb
-    mols = molecules(cfg)
+    mols = molecules(cfg) if mols is None else mols
     specs, tm = [], {}
     prep = pb.CSystem(poles=cfg["poles"], salt=cfg["salt"], idiel=cfg["idiel"], device=device)
     types = []
