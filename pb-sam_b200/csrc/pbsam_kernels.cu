@@ -70,10 +70,10 @@ __host__ __device__ inline size_t imat_stride(int NP2) { return (size_t)NP2 * im
 // 5 geometry words and 2 x 3 weights
 __host__ __device__ inline size_t tile_point_bytes(int NP) { return ((size_t)NP * NP + 2 * NP + 11) * sizeof(double); }
 // F/H solve state kept in shared memory: F, H, new H, F base, H base, new F (3
-// operands each) and a degree table
+// operands each), a degree table and the four per-degree coefficients of the operands
 __host__ __device__ inline size_t solve_state_bytes(int NP)
 {
-  return 6 * 3 * (size_t)NP * NP * sizeof(double) + (size_t)NP * NP * sizeof(short) + 16;
+  return 6 * 3 * (size_t)NP * NP * sizeof(double) + (size_t)NP * NP * sizeof(short) + 16 + 4 * (size_t)NP * sizeof(double);
 }
 __host__ __device__ inline size_t dyn_region_bytes(int NP)
 {
@@ -1142,6 +1142,8 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
   const int ld = sc.ld;
   double *sF = sc.tile, *sH = sF + len, *sHn = sH + len, *sFb = sHn + len, *sHb = sFb + len, *sFn = sHb + len;
   short *deg = (short *)(sFn + len);
+  // the operands' per-degree coefficients, copied once per solve
+  double *cH1 = (double *)(((size_t)(deg + NP2) + 15) & ~(size_t)15), *cF1 = cH1 + NP, *cH2 = cF1 + NP, *cF2 = cH2 + NP;
   double *sOut = xg + 6 * NP2;               // H at entry (leader only; the leader's scratch)
   const bool lead = cw.rank == 0, crew = cw.size > 1;
   cg::cluster_group cl = cg::this_cluster();
@@ -1153,6 +1155,12 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
   }
   for (int d = tm.rank; d < D; d += tm.size)
     for (int k = NP2; k < ld; k++) sc.xs[d * ld + k] = 0.0;   // pad columns (the IMat's are zero too)
+  for (int n = tm.rank; n < NP; n += tm.size) {
+    cH1[n] = cst[CST_H1 * NP + n];
+    cF1[n] = cst[CST_F1 * NP + n];
+    cH2[n] = cst[CST_H2 * NP + n];
+    cF2[n] = cst[CST_F2 * NP + n];
+  }
   tm.sync();
   for (int k = tm.rank; k < len; k += tm.size) {
     const int kk = k % NP2, n = deg[kk];
@@ -1183,13 +1191,59 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
   int ct = 0;
   double dev = 0.0;
   PhaseClock mv{tph, 0};
+  const int lane = tm.rank & 31, warp = tm.rank >> 5, nwarp = tm.size >> 5;
+  const int ncx = D * NP * (NP + 1) / 2;
   for (;;) {
     mv.start(tm);
+    // the F operands of this iteration and, from the second iteration on, the last
+    // iteration's computeDev over complex entries (d, n, m) of its old (sHn) and new
+    // (sH) H: the per-thread sums and their reduction are those of team_sum, taken at
+    // the operands' barrier; the stop test then comes before this iteration's products
+    double part = 0.0;
     for (int k = tm.rank; k < len; k += tm.size) {
       const int kk = k % NP2, n = deg[kk];
-      sc.xs[(k / NP2) * ld + kk] = sFb[k] + cst[CST_H1 * NP + n] * sH[k] + cst[CST_F1 * NP + n] * sF[k];
+      sc.xs[(k / NP2) * ld + kk] = sFb[k] + cH1[n] * sH[k] + cF1[n] * sF[k];
+    }
+    if (ct > 0) {
+      for (int u = tm.rank; u < ncx; u += tm.size) {
+        const int d = u / (NP * (NP + 1) / 2), r = u % (NP * (NP + 1) / 2);
+        int n = (int)((sqrt(8.0 * r + 1.0) - 1.0) * 0.5);
+        while (n * (n + 1) / 2 > r) n--;
+        while ((n + 1) * (n + 2) / 2 <= r) n++;
+        const int m = r - n * (n + 1) / 2;
+        const int base = d * NP2 + IDX(n);
+        double ar, ai = 0.0, br, bi = 0.0;
+        if (m == 0) { ar = sHn[base]; br = sH[base]; }
+        else { ar = sHn[base + 2 * m - 1]; ai = sHn[base + 2 * m]; br = sH[base + 2 * m - 1]; bi = sH[base + 2 * m]; }
+        const double PL = 1e-30;
+        double sv;
+        if (fabs(ar) < PL && fabs(ai) < PL) {
+          if (fabs(br) < PL && fabs(bi) < PL) continue;
+          sv = 1.0;
+        } else if (fabs(br) < PL && fabs(bi) < PL) sv = 1.0;
+        else {
+          const double dr = ar - br, di = ai - bi;
+          const double top = dr * dr + di * di;
+          const double bot = ar * ar + ai * ai + br * br + bi * bi;
+          sv = (m != 0) ? 2 * top / bot : top / bot;
+        }
+        part += sv;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      if (lane == 0) red[warp] = part;
     }
     tm.sync();
+    if (ct > 0) {
+      double r = 0.0;
+      for (int w = 0; w < nwarp; w++) r += red[w];
+      dev = r / (4 * NP * NP);
+      // red is written again only at the next iteration's operands, two barriers on
+      if (!(dev > prm.solve_tol && ct < prm.solve_max_ct)) {
+        mv.stop(tm, PH_MATVEC);
+        break;
+      }
+    }
     if (crew) {
       // every CTA pushes its rows of the new F into every CTA's sFn (distributed
       // shared memory); after the cluster barrier each holds the whole vector.  F is
@@ -1203,7 +1257,7 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
     }
     for (int k = tm.rank; k < len; k += tm.size) {
       const int kk = k % NP2, n = deg[kk];
-      sc.xs[(k / NP2) * ld + kk] = sHb[k] + cst[CST_H2 * NP + n] * sH[k] + cst[CST_F2 * NP + n] * sF[k];
+      sc.xs[(k / NP2) * ld + kk] = sHb[k] + cH2[n] * sH[k] + cF2[n] * sF[k];
     }
     tm.sync();
     if (crew) {
@@ -1216,37 +1270,8 @@ __device__ __noinline__ double solve_core(const Team &tm, const Crew &cw, double
       tm.sync();
     }
     mv.stop(tm, PH_MATVEC);
-    // computeDev over complex entries (d, n, m) of the old and new H
-    double part = 0.0;
-    const int ncx = D * NP * (NP + 1) / 2;
-    for (int u = tm.rank; u < ncx; u += tm.size) {
-      const int d = u / (NP * (NP + 1) / 2), r = u % (NP * (NP + 1) / 2);
-      int n = (int)((sqrt(8.0 * r + 1.0) - 1.0) * 0.5);
-      while (n * (n + 1) / 2 > r) n--;
-      while ((n + 1) * (n + 2) / 2 <= r) n++;
-      const int m = r - n * (n + 1) / 2;
-      const int base = d * NP2 + IDX(n);
-      double ar, ai = 0.0, br, bi = 0.0;
-      if (m == 0) { ar = sH[base]; br = sHn[base]; }
-      else { ar = sH[base + 2 * m - 1]; ai = sH[base + 2 * m]; br = sHn[base + 2 * m - 1]; bi = sHn[base + 2 * m]; }
-      const double PL = 1e-30;
-      double s;
-      if (fabs(ar) < PL && fabs(ai) < PL) {
-        if (fabs(br) < PL && fabs(bi) < PL) continue;
-        s = 1.0;
-      } else if (fabs(br) < PL && fabs(bi) < PL) s = 1.0;
-      else {
-        const double dr = ar - br, di = ai - bi;
-        const double top = dr * dr + di * di;
-        const double bot = ar * ar + ai * ai + br * br + bi * bi;
-        s = (m != 0) ? 2 * top / bot : top / bot;
-      }
-      part += s;
-    }
-    dev = team_sum(tm, part, red) / (4 * NP * NP);
     { double *t = sH; sH = sHn; sHn = t; }
     ct++;
-    if (!(dev > prm.solve_tol && ct < prm.solve_max_ct)) break;
   }
   if (!lead) return 0.0;
   if (tm.rank == 0 && stats) { stats[1] += ct; stats[2] += 1; }
