@@ -137,8 +137,8 @@ int pbsam_moltype_info(const pbsam_context *ctx, int type_id, int *n_sph, int *n
 /* Replaces constructing the CMolecule objects of a run (src/molecule.h:67-77)
  * followed by CMolecule::initMutualConstants(mols, inter, interact, true)
  * (src/molecule.cpp:77-95), for n_systems independent copies of the same
- * molecule list (mol_types[n_mol]).  Each system keeps its own solver state
- * between calls, as the reference's molecules do. */
+ * molecule list (mol_types[n_mol], 1 <= n_mol <= 64).  Each system keeps its own
+ * solver state between calls, as the reference's molecules do. */
 int pbsam_system_create(pbsam_context *ctx, int n_systems, int n_mol, const int *mol_types,
                         pbsam_system **sys);
 int pbsam_system_destroy(pbsam_system *sys);

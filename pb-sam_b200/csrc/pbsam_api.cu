@@ -773,7 +773,7 @@ static int finalize_types(pbsam_context *c)
 
 extern "C" int pbsam_system_create(pbsam_context *c, int n_systems, int n_mol, const int *mol_types, pbsam_system **out)
 {
-  if (!c || n_systems <= 0 || n_mol <= 0 || n_mol > 32 || !mol_types || !out) return fail(PBSAM_E_BADARG, "bad argument");
+  if (!c || n_systems <= 0 || n_mol <= 0 || n_mol > 64 || !mol_types || !out) return fail(PBSAM_E_BADARG, "bad argument");
   for (int i = 0; i < n_mol; i++)
     if (mol_types[i] < 0 || mol_types[i] >= (int)c->types.size()) return fail(PBSAM_E_BADARG, "bad molecule type");
   TRY(finalize_types(c));

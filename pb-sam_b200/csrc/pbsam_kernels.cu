@@ -2176,13 +2176,13 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
     else {
       for (int i = 0; i < nmol; i++) bv.interMol_n[(size_t)b * nmol + i] = 0;
       for (int s = 0; s < S; s++) {
-        int added = 0;   // molecules already credited (bit mask; nmol <= 32 here)
+        unsigned long long added = 0;   // molecules already credited (bit mask; nmol <= 64)
         for (int e = 0; e < y.nipol(s); e++) {
           const int j = y.mol(y.ipol(s)[e]);
-          if (added & (1 << j)) continue;
+          if (added & (1ULL << j)) continue;
           int &n = bv.interMol_n[(size_t)b * nmol + j];
           bv.interMol[((size_t)b * nmol + j) * S + n++] = s;
-          added |= (1 << j);
+          added |= (1ULL << j);
         }
       }
       for (int j = 0; j < nmol; j++) {
@@ -2230,8 +2230,8 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
   double dev = 0.0, MAXDEV = 0.0;
   int mtotal = 0;
   {
-    double maxdevs[32];
-    for (int i = 0; i < nmol && i < 32; i++) maxdevs[i] = 0.0;
+    // MAXDEV: the largest change of any sphere (the reference takes the largest of the
+    // molecules' largest, the same number)
     for (int i = 0; i < nmol; i++) {
       double dmol = 0.0;
       if (bv.interX[(size_t)b * nmol + i])
@@ -2239,12 +2239,11 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
           if (y.nipol(s) == 0) continue;
           const double d = recompute_from_self(tm, y, s);
           dmol += d;
-          if (maxdevs[i] < d) maxdevs[i] = d;
+          if (MAXDEV < d) MAXDEV = d;
           mtotal++;
         }
       dev += dmol;
     }
-    for (int i = 0; i < nmol; i++) if (maxdevs[i] > MAXDEV) MAXDEV = maxdevs[i];
   }
   // the exact form, once before its sweeps: the inter-molecular LS (its sources, the
   // rotated H of the first round, are not updated by the sweeps) and the near terms of
@@ -2263,8 +2262,7 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
   const double tol2 = c.prm.exact ? c.prm.exact_tol * c.prm.exact_tol : c.prm.max_polar_dev * c.prm.max_polar_dev;
   while (dev * itot > tol2 && ct < c.prm.max_pol_rounds) {
     dev = 0.0;
-    double maxdevs[32];
-    for (int i = 0; i < nmol && i < 32; i++) maxdevs[i] = 0.0;
+    double next_max = 0.0;
     for (int i = 0; i < nmol; i++) {
       double dmol = 0.0;
       if (bv.interX[(size_t)b * nmol + i])
@@ -2274,13 +2272,12 @@ __device__ void forces_body(const Team &tm, const Ctx &c, const Crew &cw, int b,
           // the exact form recomputes every sphere (the selective update can leave a
           // sphere whose last change was small out of date)
           if (c.prm.exact || d > 0.1 * MAXDEV) d = recompute(tm, y, s);
-          if (maxdevs[i] < d) maxdevs[i] = d;
+          if (next_max < d) next_max = d;
           dmol += d;
         }
       dev += dmol;
     }
-    MAXDEV = 0.0;
-    for (int i = 0; i < nmol; i++) if (maxdevs[i] > MAXDEV) MAXDEV = maxdevs[i];
+    MAXDEV = next_max;
     ct++;
   }
   if (tm.rank == 0) {

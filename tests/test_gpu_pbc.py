@@ -139,3 +139,88 @@ def test_pbc_bdm_vs_reference(tmp_path):
     assert np.all(np.abs(g["pos"]) <= L / 2 + 1e-9)
     mol.close()
     ctx.close()
+
+
+def _lattice64():
+    """64 molecules (32 copies of each golden p = 6 molecule, species 0 first as
+    CBDmulti holds them) on a 4 x 4 x 4 lattice of 24 A, jittered and randomly
+    turned, in a periodic box of 96 A: minimum gap 4 A, 115 molecule pairs inside the
+    polarization cutoff, many of them across a face."""
+    from pbsam_b200 import synth
+    rng = np.random.default_rng(64)
+    quat = np.array([synth.random_quat(rng) for _ in range(64)])
+    jit = rng.uniform(-1.5, 1.5, (64, 3))
+    perm = rng.permutation(64)
+    grid = np.array([[x, y, z] for x in range(4) for y in range(4) for z in range(4)], float)
+    s, box = 24.0, 96.0
+    pos = grid[perm] * s + jit - box / 2 + s / 2
+    types = [0] * 32 + [1] * 32
+    return types, pos, quat, box
+
+
+def test_pbc_64_molecules_vs_reference(tmp_path):
+    """A 64-molecule periodic system (the molecule count of the reference's periodic bdm
+    example): forces, torques and energy of one evaluation against the reference's
+    (1e-8 relative)."""
+    import pbsam_b200 as pb
+    P = json.load(open(os.path.join(golden_dir("tiny"), "poses.json")))
+    types, pos, quat, box = _lattice64()
+    ref = _ref_forces(str(tmp_path), P, list(zip(types, pos.tolist(), quat.tolist())), box)
+    assert ref["ok"]
+    ctx = pb.CSystem(poles=P["poles"], salt=P["salt"], idiel=P["idiel"], box_length=box)
+    try:
+        d = golden_dir("tiny")
+        ts = [ctx.load_moltype(d + "/mol%s.pqr" % t, d + "/im" + t, d + "/exp" + t, "mol%s.0" % t) for t in "AB"]
+        m = ctx.molecules([ts[t] for t in types], 1)
+        m.set_poses(pos[None], quat[None])
+        f, t, st = m.compute_forces()
+        e = m.compute_energy()
+        assert st[0] == 0 and m.stats()[0, 2] > 0
+        ef, et = rel(f[0], ref["force"]), rel(t[0], ref["torque"])
+        print("64 molecules: force %.2e torque %.2e energy %.2e" % (ef, et, abs(e[0] - ref["energy"]) / abs(ref["energy"])))
+        assert ef < 1e-8 and et < 1e-8 and abs(e[0] - ref["energy"]) <= 1e-8 * abs(ref["energy"])
+        m.close()
+    finally:
+        ctx.close()
+
+
+def test_pbc_bdm_64_molecules_vs_reference(tmp_path):
+    """Three CBDmulti steps of the 64-molecule periodic system with the reference's
+    noise stream against the reference's own bdm (positions 1e-9 A)."""
+    import pbsam_b200 as pb
+    exe = oracle.ref_bdm_harness()
+    if exe is None:
+        pytest.skip("reference BD harness not built")
+    types, pos, quat, box = _lattice64()
+    frame = list(zip(types, pos.tolist(), quat.tolist()))
+    ctx, ts, P = tiny_ctx(box_length=box)
+    # CBDmulti's per-species coefficients (src/BDmulti.cpp:204-205)
+    dtr, drot = tuple([0.015] * 64), tuple([4.5e-5] * 32 + [4e-5] * 32)
+    spec = os.path.join(str(tmp_path), "m64.txt")
+    oracle.write_bd_spec(spec, oracle.golden_moltypes(golden_dir("tiny")), frame, 1, 3, 2024, 0, dtr, drot,
+                         salt=P["salt"], idiel=P["idiel"], poles=P["poles"], noise=(1, 1))
+    with open(spec, "a") as fh:
+        fh.write("box %r\n" % box)
+    subprocess.check_call([exe, spec, spec + ".out"], env=dict(os.environ, OMP_NUM_THREADS="1"),
+                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    ref = []
+    for ln in open(spec + ".out"):
+        t = ln.split()
+        if t[0] == "BDSTEP":
+            ref.append(dict(status=0, steps=int(t[1]), fevals=int(t[3]), time=float(t[4]), pos=[], quat=[]))
+        elif t[0] == "POSE":
+            v = [float(x) for x in t[2:]]
+            ref[-1]["pos"].append(v[:3])
+            ref[-1]["quat"].append(v[3:])
+    assert len(ref) == 3 and ref[-1]["fevals"] > 0
+    mol = ctx.molecules([ts[t] for t in types], n_systems=1)
+    try:
+        mol.set_poses(pos[None], quat[None])
+        mol.bd_init(dtr, drot, mode=pb.PBSAM_BD_MULTI, seed=2024, noise=pb.PBSAM_BD_NOISE_DRAND48)
+        for k in range(3):
+            mol.bd_run(1)
+            g = mol.bd_state()
+            check_step(g, 0, dict(ref[k], pos=np.array(ref[k]["pos"]), quat=np.array(ref[k]["quat"])))
+    finally:
+        mol.close()
+        ctx.close()
