@@ -15,7 +15,12 @@ The same line carries a Brownian-dynamics leg ("bd", --bd 1): 1024 independent
 two-molecule bdnam trajectories at p = 10 (35 + 35 spheres), each step a force
 evaluation where the pair is inside the force distance plus the Ermak-McCammon
 move, one CUDA graph per step of the whole batch; BD steps/s with its own e2e,
-clocks and the reference's computeForces timed on the host cores.
+clocks and the reference's computeForces timed on the host cores.  Further legs:
+"bd_exact" (the same trajectories, exact form with adjoint forces, checked against
+central differences), "bd_uneven" (1024 trajectories of molecules of 10-60 spheres in
+64 handles, one group launch per step against the handles' own launches) and
+"bd_many" (bdm dynamics of 148 systems of 64 molecules x 30 spheres in a periodic
+300 A cube, with the reference's own bdm timed on the host cores).
 
 Multi-GPU: one process per GPU (torchrun), each rank solves its own batch of 26
 poses and its own 1024 trajectories (weak scaling, no data-path collective); rank 0
@@ -284,6 +289,14 @@ def run_ours(args):
             if out is not None:
                 out["bd_uneven"] = bdu
                 out["gpu_launches"] += bdu["gpu_launches"]
+        if args.bd_many:
+            try:
+                bdm = run_bd_many(args, local, rank, world, dist)
+            except Exception as e:
+                bdm = {"error": "%s: %s" % (type(e).__name__, e), "gpu_launches": 0}
+            if out is not None:
+                out["bd_many"] = bdm
+                out["gpu_launches"] += bdm["gpu_launches"]
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -588,6 +601,149 @@ def run_bd_uneven(args, local, rank, world, dist):
     return out
 
 
+BD_MANY_METRIC = "BD steps/s (bdm: 64 molecules x 30 spheres in a periodic 300 A cube, p=10)"
+
+
+def run_bd_many(args, local, rank, world, dist):
+    """BD steps per second of independent many-body systems: 64 molecules of 30
+    spheres (32 of each species) in a periodic 300 A cube, the reference bdm's
+    multi-molecule dynamics (forces of every molecule whenever two are inside the
+    interaction cutoff, then every molecule moved in turn), plain FP64 drop-in.  Every
+    system starts from the same configuration with its own noise stream; every step of
+    every system counts as one unit."""
+    import torch
+    from pbsam_b200 import replicas, workload
+    cfg = dict(workload.BD_MANY)
+    t0 = time.time()
+    specs, prep_t, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds_p10)
+    ctx, types = workload.open_context(cfg, specs, device=local, box_length=cfg["box"])
+    mols = workload.molecules(cfg)
+    kinds, pos, quat = workload.many_start(cfg, mols, rank=rank)
+    B = args.bd_many_systems
+    sysb = ctx.molecules([types[k] for k in kinds], n_systems=B)
+    prep_t["total_s"] = round(time.time() - t0, 1)
+    stream = torch.cuda.current_stream()
+    sysb.set_stream(stream.cuda_stream)
+    sysb.set_poses(np.repeat(pos[None], B, 0), np.repeat(quat[None], B, 0))
+    n = len(kinds)
+    dtr = [cfg["dtr"]] * n
+    drot = [cfg["drot"][k] for k in kinds]
+    sysb.bd_init(dtr, drot, mode=1, seed=2718 + rank)
+    sysb.bd_run(args.warmup)
+    torch.cuda.synchronize()
+    s0 = sysb.bd_state()
+    if world > 1:
+        dist.barrier()
+    steps = args.bd_many_steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_id_for_smi(local)) as clk, torch.cuda.nvtx.range("bd_many"):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sysb.bd_run(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clocks = clk.summary()
+    s1 = sysb.bd_state()
+    ms_max = replicas.max_over_ranks(ms, dist if world > 1 else None)
+    units = int(np.sum(s1["steps"] - s0["steps"]))
+    fe = int(np.sum(s1["fevals"] - s0["fevals"]))
+    units_all = replicas.sum_over_ranks(units, dist if world > 1 else None)
+    st_last = sysb.stats()
+    ph = sysb.phase_ms()
+    # e2e: one step per call through the public API, the state read back every step
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_e2e = max(1, steps // 2)
+    torch.cuda.synchronize()
+    ee0.record(stream)
+    for _ in range(n_e2e):
+        sysb.bd_run(1)
+        st = sysb.bd_state()
+    ee1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = replicas.max_over_ranks(ee0.elapsed_time(ee1), dist if world > 1 else None)
+    e2e_units = replicas.sum_over_ranks(int(np.sum(st["steps"] - s1["steps"])), dist if world > 1 else None)
+    d2h = sum(int(v.nbytes) for v in st.values())
+    L = cfg["box"]
+    d = pos[:, None] - pos[None]
+    d -= L * np.round(d / L)
+    r = np.linalg.norm(d, axis=2) + np.eye(n) * 1e9
+    names = ["solve", "surface", "numeric", "intra", "LS", "DTA", "grad_or_backward", "total"]
+    out = {"metric": BD_MANY_METRIC, "value": units_all / (ms_max * 1e-3), "unit": "BD steps/s",
+           "ms_per_step": ms_max / steps, "steps": steps, "warmup": args.warmup, "dtype": "f64",
+           "config": {"workload": "bdm p=10: %d systems of 64 molecules x 30 spheres (r 3-6 A, 900 charges in "
+                                  "[-0.6, 0.6], net +2 x 32 / -2 x 32) in a periodic 300 A cube, random start with "
+                                  "a 2 A minimum gap (%d molecule pairs within 100 A), D 0.015 A^2/ps, Dr 4.5e-5 / "
+                                  "4e-5 rad^2/ps, bdm time steps, Philox noise per system; plain FP64 form" % (
+                                      B, int(np.sum(r < 100) // 2)),
+                      "systems_per_gpu": B, "spheres_per_system": int(sum(len(mols[k].radii) for k in kinds))},
+           "force_evaluations_fraction": fe / max(units, 1),
+           "status_counts": {name: int(np.sum(s1["status"] == k)) for k, name in
+                             ((0, "running"), (2, "stuck"), (4, "failed"))},
+           "e2e": {"value": e2e_units / (e2e_ms * 1e-3), "unit": "BD steps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": d2h, "note": "one step per call, state read back to the host each step"},
+           "gpu_launches": 3 * steps, "clocks": clocks, "prep": prep_t,
+           "mean_phase_ms": {k: round(float(v), 2) for k, v in zip(names, ph[:, :8].mean(axis=0))},
+           "mean_sweeps": float(st_last[:, 0].mean()), "mean_inner_solves": float(st_last[:, 2].mean())}
+    if rank == 0 and args.cpu_baseline:
+        out["cpu_baseline"] = bd_many_cpu_baseline(cfg, kinds, pos, quat, args)
+    sysb.close()
+    ctx.close()
+    return out
+
+
+def bd_many_cpu_baseline(cfg, kinds, pos, quat, args, steps=3):
+    """The reference's own bdm (CBDmulti: computeMinSepDist, computeForces below the
+    interaction cutoff, makeMove; oracle/ref_bdm_harness.cpp, `fast` build) on the same
+    start, one single-threaded process per host core, each with its own drand48 seed,
+    all concurrently: steps/s = processes x (steps - 1) / the longest time of the steps
+    after the first (the first builds the solver state).  Inputs from the host-side
+    preparation (oracle/pbsam_prep.cpp)."""
+    import tempfile
+    exe = os.path.join(REPO, "oracle", "_ref", "p%d_fast" % cfg["poles"], "bdm_harness")
+    if not os.path.exists(exe):
+        return {"value": None, "note": "reference bdm harness not built"}
+    ncores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as wd:
+        files, _ = reference_inputs_cpu(cfg, args.selfpol_rounds_p10, wd)
+        procs = []
+        for c in range(ncores):
+            spec = os.path.join(wd, "bdm%d.txt" % c)
+            with open(spec, "w") as fh:
+                fh.write("salt %r\nidiel %r\n" % (cfg["salt"], cfg["idiel"]))
+                for fl in files:
+                    fh.write("moltype %s %s %s %s\n" % fl)
+                fh.write("frame\n")
+                for k, p, q in zip(kinds, pos, quat):
+                    fh.write("mol %d %s %s\n" % (k, " ".join("%.17g" % v for v in p),
+                                                 " ".join("%.17g" % v for v in q)))
+                fh.write("bd 1 %d %d 0\nbox %r\n" % (steps, 31 + c, cfg["box"]))
+            procs.append((spec, subprocess.Popen([exe, spec, spec + ".out"], env=dict(os.environ, OMP_NUM_THREADS="1"),
+                                                 stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)))
+        t0 = time.time()
+        per = []
+        for spec, p in procs:
+            try:
+                p.wait(timeout=max(1.0, 4 * args.cpu_limit - (time.time() - t0)))
+            except subprocess.TimeoutExpired:
+                p.kill()
+                p.wait()
+                continue
+            if p.returncode != 0 or not os.path.exists(spec + ".out"):
+                continue
+            for ln in open(spec + ".out"):
+                t = ln.split()
+                if t and t[0] == "TIME" and int(t[2]) > 0:
+                    per.append((float(t[1]), int(t[2])))
+    if not per:
+        return {"value": None, "note": "no reference process finished"}
+    T = max(x[0] for x in per)
+    return {"value": len(per) * per[0][1] / T, "unit": "BD steps/s", "cores": ncores, "kind": "reference",
+            "sample": "%d single-threaded processes of the reference's bdm (CBDmulti, p=%d `fast` build), each %d "
+                      "steps from the same start with its own seed, run concurrently; steps after the first timed "
+                      "(slowest process %.2f s for %d steps)" % (len(per), cfg["poles"], steps, T, per[0][1])}
+
+
 def reference_bd_step_seconds(cfg, files, pos, quat, limit_s, workdir, steps=3, variant="fast", seed=1):
     """The reference's own bdnam step (CBDnam: computeForces while the pair is inside
     f_DIST, then makeMove; oracle/ref_bd_harness.cpp) from each given pose, one
@@ -865,6 +1021,10 @@ def main():
     ap.add_argument("--bd-steps", type=int, default=20, help="timed BD steps")
     ap.add_argument("--bd-uneven", type=int, default=1,
                     help="also time BD of molecules with uneven sphere counts (groups of handles)")
+    ap.add_argument("--bd-many", type=int, default=1,
+                    help="also time many-body bdm dynamics (64 molecules x 30 spheres, periodic 300 A cube)")
+    ap.add_argument("--bd-many-systems", type=int, default=148, help="many-body systems per GPU")
+    ap.add_argument("--bd-many-steps", type=int, default=6, help="timed many-body BD steps")
     ap.add_argument("--exact-tol", type=float, default=1e-10,
                     help="exact BD leg: pbsam_params.exact_tol (the leg reports the force error against 1e-14)")
     ap.add_argument("--exact-relax", type=float, default=1.0, help="exact BD leg: pbsam_params.exact_relax")

@@ -14,8 +14,9 @@
 //
 // spec: salt, idiel, two moltype lines, one frame of mol lines (types 0 then 1),
 //       bd <mode (1)> <n steps> <seed> <unused>
-// output: BDSTEP <steps> 0 <force evaluations> <time>, then POSE lines; exit
-// status 4 when computeForces reports overlapping spheres (where bdm exits).
+// output: BDSTEP <steps> 0 <force evaluations> <time>, then POSE lines, and TIME <wall
+// seconds of the steps after the first> <their count> at the end; exit status 4 when
+// computeForces reports overlapping spheres (where bdm exits).
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -94,8 +95,9 @@ int main(int argc, char **argv)
   FILE *out = fopen(argv[2], "w");
   if (!out) return 2;
   int fevals = 0;
-  double time = 0.0;
+  double time = 0.0, t_start = 0.0;
   for (int k = 0; k < nsteps; k++) {
+    if (k == 1) t_start = read_timer();
     const REAL minDist = bd.computeMinSepDist();
     if (minDist < CMolecule::m_interactRcutoff) fevals++;
     std::cout.rdbuf(sink.rdbuf());               // propagate's failure path prints and exits
@@ -111,6 +113,7 @@ int main(int argc, char **argv)
     }
     fflush(out);
   }
+  if (nsteps > 1) fprintf(out, "TIME %.6e %d\n", read_timer() - t_start, nsteps - 1);
   fclose(out);
   return 0;
 }

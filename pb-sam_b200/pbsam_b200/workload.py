@@ -36,12 +36,56 @@ BD_P10 = dict(n_sph=35, r=(3.0, 6.0), n_q=1200, q_amp=0.6, nets=(2.0, -2.0), pol
               dt_gap=30.0, viscosity=0.89e-3, temperature=298.15, min_gap=1.0)
 
 
-# Brownian dynamics of molecules with uneven sphere counts (SURVEY config 3's 10..60
-# spheres per molecule, charges as config 0): n_types "A" molecules (net +2) and
+# Brownian dynamics of molecules with uneven sphere counts (10..60 spheres per
+# molecule, 300 charges U(-0.6, 0.6) per molecule): n_types "A" molecules (net +2) and
 # n_types "B" molecules (net -2), every A-B pair a handle of per_pair trajectories.
 BD_UNEVEN = dict(n_types=8, sizes=(10, 60), r=(3.0, 6.0), n_q=300, q_amp=0.6, nets=(2.0, -2.0), poles=10, salt=0.05,
                  idiel=4.0, seed=4100, pose_seed=4200, start=50.0, escape=150.0, dt_min=0.02, dt_max=2.0,
                  dt_gap=30.0, viscosity=0.89e-3, temperature=298.15, min_gap=1.0, per_pair=16)
+
+
+# Many-body Brownian dynamics at p = 10 (bdm): 64 molecules of 30 spheres (radii
+# U(3,6) A, 900 charges U(-0.6, 0.6)), 32 copies of molecule A (net +2) followed by
+# 32 of molecule B (net -2), as CBDmulti holds its species, at random places and
+# orientations in a periodic cube of 300 A with at least min_gap between any two
+# molecules' spheres (minimum image); the reference bdm's own diffusion constants
+# (D 0.015 A^2/ps, Dr 4.5e-5 and 4e-5 rad^2/ps, src/BDmulti.cpp:204-205) and time
+# steps (pbsam_bd_params_default for the multi-molecule mode).
+BD_MANY = dict(n_sph=30, r=(3.0, 6.0), n_q=900, q_amp=0.6, nets=(2.0, -2.0), poles=10, salt=0.05, idiel=4.0,
+               seeds=(5101, 5102), pose_seed=5103, n_copies=32, box=300.0, min_gap=2.0,
+               dtr=0.015, drot=(4.5e-5, 4e-5))
+
+
+def many_start(cfg, mols, rank=0):
+    """Species list, [n_mol, 3] positions and [n_mol, 4] quaternions of the many-body
+    start: molecules placed one at a time at uniform random places (rejected while
+    closer than min_gap to one already placed, minimum image)."""
+    rng = np.random.default_rng(cfg["pose_seed"] + 7919 * rank)
+    L = cfg["box"]
+    shapes = [(m.centres, m.radii) for m in mols]
+    ext = [m.extent() for m in mols]
+    kinds = [0] * cfg["n_copies"] + [1] * cfg["n_copies"]
+    pos, quat = [], []
+    for k in kinds:
+        for _ in range(10000):
+            p = rng.uniform(-L / 2, L / 2, 3)
+            q = synth.random_quat(rng)
+            ok = True
+            for j, (pj, qj) in enumerate(zip(pos, quat)):
+                d = p - pj
+                d -= L * np.round(d / L)
+                if np.linalg.norm(d) > ext[k] + ext[kinds[j]] + cfg["min_gap"]:
+                    continue
+                if synth.min_gap(shapes[kinds[j]], np.zeros(3), qj, shapes[k], d, q) < cfg["min_gap"]:
+                    ok = False
+                    break
+            if ok:
+                break
+        else:
+            raise RuntimeError("no free place for molecule %d" % len(pos))
+        pos.append(p)
+        quat.append(q)
+    return kinds, np.array(pos), np.array(quat)
 
 
 def uneven_molecules(cfg):
