@@ -297,6 +297,16 @@ def run_ours(args):
             if out is not None:
                 out["bd_many"] = bdm
                 out["gpu_launches"] += bdm["gpu_launches"]
+            if args.bd_many_exact:
+                try:
+                    bdmx = run_bd_many(args, local, rank, world, dist, exact=True)
+                    if "value" in bdm and "value" in bdmx:
+                        bdmx["vs_plain_bd"] = bdmx["value"] / bdm["value"]
+                except Exception as e:
+                    bdmx = {"error": "%s: %s" % (type(e).__name__, e), "gpu_launches": 0}
+                if out is not None:
+                    out["bd_many_exact"] = bdmx
+                    out["gpu_launches"] += bdmx["gpu_launches"]
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -604,19 +614,21 @@ def run_bd_uneven(args, local, rank, world, dist):
 BD_MANY_METRIC = "BD steps/s (bdm: 64 molecules x 30 spheres in a periodic 300 A cube, p=10)"
 
 
-def run_bd_many(args, local, rank, world, dist):
+def run_bd_many(args, local, rank, world, dist, exact=False):
     """BD steps per second of independent many-body systems: 64 molecules of 30
     spheres (32 of each species) in a periodic 300 A cube, the reference bdm's
     multi-molecule dynamics (forces of every molecule whenever two are inside the
-    interaction cutoff, then every molecule moved in turn), plain FP64 drop-in.  Every
-    system starts from the same configuration with its own noise stream; every step of
-    every system counts as one unit."""
+    interaction cutoff, then every molecule moved in turn), plain FP64 drop-in or
+    (exact) the exact form with adjoint forces.  Every system starts from the same
+    configuration with its own noise stream; every step of every system counts as one
+    unit."""
     import torch
     from pbsam_b200 import replicas, workload
     cfg = dict(workload.BD_MANY)
     t0 = time.time()
     specs, prep_t, _ = workload.prepare(cfg, device=local, selfpol_rounds=args.selfpol_rounds_p10)
-    ctx, types = workload.open_context(cfg, specs, device=local, box_length=cfg["box"])
+    xkw = {"exact": 1, "exact_tol": args.exact_tol} if exact else {}
+    ctx, types = workload.open_context(cfg, specs, device=local, box_length=cfg["box"], **xkw)
     mols = workload.molecules(cfg)
     kinds, pos, quat = workload.many_start(cfg, mols, rank=rank)
     B = args.bd_many_systems
@@ -685,7 +697,13 @@ def run_bd_many(args, local, rank, world, dist):
            "gpu_launches": 3 * steps, "clocks": clocks, "prep": prep_t,
            "mean_phase_ms": {k: round(float(v), 2) for k, v in zip(names, ph[:, :8].mean(axis=0))},
            "mean_sweeps": float(st_last[:, 0].mean()), "mean_inner_solves": float(st_last[:, 2].mean())}
-    if rank == 0 and args.cpu_baseline:
+    if exact:
+        out["metric"] = BD_MANY_METRIC + ", exact form with adjoint forces"
+        out["config"]["workload"] = out["config"]["workload"].replace("plain FP64 form", "exact form, exact_tol %g" %
+                                                                      args.exact_tol)
+        out["mean_phase_ms"].update({k: round(float(v), 2) for k, v in zip(
+            ["backward_energy", "backward_sweeps", "backward_first_round"], ph[:, 12:15].mean(axis=0))})
+    if rank == 0 and args.cpu_baseline and not exact:
         out["cpu_baseline"] = bd_many_cpu_baseline(cfg, kinds, pos, quat, args)
     sysb.close()
     ctx.close()
@@ -1025,6 +1043,8 @@ def main():
                     help="also time many-body bdm dynamics (64 molecules x 30 spheres, periodic 300 A cube)")
     ap.add_argument("--bd-many-systems", type=int, default=148, help="many-body systems per GPU")
     ap.add_argument("--bd-many-steps", type=int, default=6, help="timed many-body BD steps")
+    ap.add_argument("--bd-many-exact", type=int, default=0,
+                    help="also time the many-body leg in the exact form (about a minute per step at 148 systems)")
     ap.add_argument("--exact-tol", type=float, default=1e-10,
                     help="exact BD leg: pbsam_params.exact_tol (the leg reports the force error against 1e-14)")
     ap.add_argument("--exact-relax", type=float, default=1.0, help="exact BD leg: pbsam_params.exact_relax")
