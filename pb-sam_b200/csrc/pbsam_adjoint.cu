@@ -206,18 +206,12 @@ __device__ void solve_direct_T(const Team &tm, const Tab &T, const TypeView &tv,
   double *x = sc.xs, *y = sc.sol;
   for (int k = tm.rank; k < NP2; k += tm.size) { x[k] = gF[k]; x[NP2 + k] = gH[k]; }
   tm.sync();
-  // a thread per column, eight rows in flight
-  for (int j = tm.rank; j < n2; j += tm.size) {
-    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int r = 0;
-    for (; r + 7 < n2; r += 8) {
-#pragma unroll
-      for (int u = 0; u < 8; u++) a[u] += G[(size_t)(r + u) * n2 + j] * x[r + u];
-    }
-    for (; r < n2; r++) a[0] += G[(size_t)r * n2 + j] * x[r];
-    y[j] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+  {
+    const double *Ms[1] = {G}, *xs[1] = {x};
+    const int nr[1] = {n2};
+    cols_apply<1>(tm, Ms, nr, nr, n2, xs, sc.tile, (int)(dyn_region_bytes(NP) / sizeof(double)),
+                  [&](int, int j, double v) { y[j] = v; });
   }
-  tm.sync();
   for (int k = tm.rank; k < NP2; k += tm.size) {
     const int n = deg_of(k);
     gLF[k] = cst[CST_LF1 * NP + n] * y[k] + cst[CST_LF2 * NP + n] * y[NP2 + k];
@@ -574,8 +568,8 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
         if (slot >= 0 && c.tv.nkind[slot] == (analytic ? 0 : 1)) {
           // the precomputed operators of the forward map v -> u, transposed
           const double *NF = c.tv.Nmat + (size_t)slot * 2 * NP2 * NP2;
-          num_apply_T(tm, NF, pF, analytic ? pF : NP, muF(u), nF, NP2);
-          num_apply_T(tm, NF + (size_t)NP2 * NP2, pH, analytic ? pH : NP, muH(u), nH, NP2);
+          num_apply2_T(tm, NF, NF + (size_t)NP2 * NP2, pF, pH, analytic ? pF : NP, analytic ? pH : NP, muF(u),
+                       muH(u), nF, nH, NP2, sc.tile, (int)(dyn_region_bytes(NP) / sizeof(double)));
         } else if (analytic) {
           // analytic: T(u <- v)^T = W T(v <- u) W^-1, from the intra table of target v
           double *wF = t4, *wH = t5;

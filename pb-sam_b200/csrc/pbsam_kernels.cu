@@ -1413,6 +1413,173 @@ __device__ void reexpand_LS(const Team &tm, const Sys &y, int s, bool fromSelf)
   pc.stop(tm, PH_LS);
 }
 
+// ------------------------------------------------------------------ small operator products
+// Row products of NM (1 or 2) small row-major operators of the exact form (the direct
+// inner solve, the near-field operators), row stride ld: for operator m the rows
+// r < rows[m] give sum_{j < cols[m]} M[m][r][j] x[m][j], the rows rows[m] <= r < nout
+// give 0, and emit(m, r, v) receives each result on one lane.  A warp takes R rows of
+// every operator at a time and issues all their loads of a 128-column block together
+// (4 R NM per lane).  Per row, a lane's sums are those of a warp per row (four accumulators over
+// the full 128-column blocks, the ragged block added to the first in column order) and
+// the warp adds them in a fixed butterfly, so a result does not depend on how the rows
+// are dealt to the warps.
+template <int NM, int R, class Emit>
+__device__ __forceinline__ void rows_apply(const Team &tm, const double *const *M, const int *rows, const int *cols,
+                                           int ld, const double *const *x, int nout, Emit emit)
+{
+  const int lane = tm.rank & 31, w = tm.rank >> 5, nw = tm.size >> 5;
+  int cmax = 0;
+#pragma unroll
+  for (int m = 0; m < NM; m++) cmax = cols[m] > cmax ? cols[m] : cmax;
+  for (int r0 = R * w; r0 < nout; r0 += R * nw) {
+    double a[NM][R][4];
+#pragma unroll
+    for (int m = 0; m < NM; m++)
+#pragma unroll
+      for (int q = 0; q < R; q++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) a[m][q][b] = 0.0;
+    for (int j = lane; j < cmax; j += 128) {
+      double v[NM][R][4], u[NM][4];
+#pragma unroll
+      for (int m = 0; m < NM; m++) {
+#pragma unroll
+        for (int b = 0; b < 4; b++) u[m][b] = (j + 32 * b < cols[m]) ? x[m][j + 32 * b] : 0.0;
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+          const double *row = M[m] + (size_t)(r0 + q) * ld;
+          const bool ok = r0 + q < rows[m];
+#pragma unroll
+          for (int b = 0; b < 4; b++) v[m][q][b] = (ok && j + 32 * b < cols[m]) ? row[j + 32 * b] : 0.0;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < NM; m++) {
+        if (j + 96 < cols[m]) {
+#pragma unroll
+          for (int q = 0; q < R; q++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) a[m][q][b] += v[m][q][b] * u[m][b];
+        } else if (j < cols[m]) {
+#pragma unroll
+          for (int q = 0; q < R; q++)
+#pragma unroll
+            for (int b = 0; b < 3; b++)
+              if (j + 32 * b < cols[m]) a[m][q][0] += v[m][q][b] * u[m][b];
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < NM; m++)
+#pragma unroll
+      for (int q = 0; q < R; q++) {
+        double acc = (a[m][q][0] + a[m][q][1]) + (a[m][q][2] + a[m][q][3]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        const int r = r0 + q;
+        if (lane == R * m + q && r < nout) emit(m, r, r < rows[m] ? acc : 0.0);
+      }
+  }
+}
+
+// Column products (the transposes) of NM (1 or 2) small row-major operators: for
+// operator m the columns j < cols[m] give sum_{k < rows[m]} M[m][k][j] y[m][k], passed
+// to emit(m, j, v).  A column's sum has eight accumulators (row k to accumulator k mod 8
+// over the full blocks of eight rows, the ragged end to the first, in row order),
+// combined as ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7)).  With G = 2, 4 or 8
+// groups of threads per column (as many as the columns of both operators leave room
+// for), group g holds accumulators [g 8/G, (g + 1) 8/G) and adds them as its subtree of
+// that sum; the subtree sums meet in shared memory (part, G x columns doubles) and are
+// combined in the same tree, so the result does not depend on G.  Every lane keeps up
+// to sixteen loads in flight.
+template <int NM, int G, class Emit>
+__device__ __forceinline__ void cols_apply_g(const Team &tm, const double *const *M, const int *rows, const int *cols,
+                                             int ld, const double *const *y, double *part, Emit emit)
+{
+  constexpr int A = 8 / G, UB = 16 / A;
+  const int C = cols[0] + (NM > 1 ? cols[NM - 1] : 0);
+  if (tm.rank < G * C) {
+    const int g = tm.rank / C, c = tm.rank - g * C;
+    const int m = (NM > 1 && c >= cols[0]) ? 1 : 0, j = m ? c - cols[0] : c;
+    const double *Mm = M[m], *ym = y[m];
+    const int nb = rows[m] >> 3;
+    double a[A];
+#pragma unroll
+    for (int u = 0; u < A; u++) a[u] = 0.0;
+    for (int i = 0; i < nb; i += UB) {
+      double v[UB][A], w[UB][A];
+#pragma unroll
+      for (int t = 0; t < UB; t++)
+#pragma unroll
+        for (int u = 0; u < A; u++) {
+          const int k = 8 * (i + t) + g * A + u;
+          const bool ok = i + t < nb;
+          v[t][u] = ok ? Mm[(size_t)k * ld + j] : 0.0;
+          w[t][u] = ok ? ym[k] : 0.0;
+        }
+#pragma unroll
+      for (int t = 0; t < UB; t++)
+        if (i + t < nb)
+#pragma unroll
+          for (int u = 0; u < A; u++) a[u] += v[t][u] * w[t][u];
+    }
+    if (g == 0)
+      for (int k = 8 * nb; k < rows[m]; k++) a[0] += Mm[(size_t)k * ld + j] * ym[k];
+    double s;
+    if constexpr (A == 8) s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+    else if constexpr (A == 4) s = (a[0] + a[1]) + (a[2] + a[3]);
+    else if constexpr (A == 2) s = a[0] + a[1];
+    else s = a[0];
+    if (G == 1) emit(m, j, s);
+    else part[g * C + c] = s;
+  }
+  if (G > 1) {
+    tm.sync();
+    for (int c = tm.rank; c < C; c += tm.size) {
+      const int m = (NM > 1 && c >= cols[0]) ? 1 : 0, j = m ? c - cols[0] : c;
+      const double *p = part + c;
+      double s;
+      if constexpr (G == 2) s = p[0] + p[C];
+      else if constexpr (G == 4) s = (p[0] + p[C]) + (p[2 * C] + p[3 * C]);
+      else s = ((p[0] + p[C]) + (p[2 * C] + p[3 * C])) + ((p[4 * C] + p[5 * C]) + (p[6 * C] + p[7 * C]));
+      emit(m, j, s);
+    }
+  }
+  tm.sync();
+}
+
+// cols_apply_g with the largest group count that the team and the shared-memory region
+// part (cap doubles) allow
+template <int NM, class Emit>
+__device__ __forceinline__ void cols_apply(const Team &tm, const double *const *M, const int *rows, const int *cols,
+                                           int ld, const double *const *y, double *part, int cap, Emit emit)
+{
+  const int C = cols[0] + (NM > 1 ? cols[NM - 1] : 0);
+  const int lim = tm.size < cap ? tm.size : cap;
+  if (C > 0 && 8 * C <= lim) cols_apply_g<NM, 8>(tm, M, rows, cols, ld, y, part, emit);
+  else if (C > 0 && 4 * C <= lim) cols_apply_g<NM, 4>(tm, M, rows, cols, ld, y, part, emit);
+  else if (C > 0 && 2 * C <= lim) cols_apply_g<NM, 2>(tm, M, rows, cols, ld, y, part, emit);
+  else {
+    // one thread per column (more columns than threads: stride over them)
+    for (int c0 = 0; c0 < C; c0 += tm.size) {
+      const int c = c0 + tm.rank;
+      if (c < C) {
+        const int m = (NM > 1 && c >= cols[0]) ? 1 : 0, j = m ? c - cols[0] : c;
+        const double *Mm = M[m], *ym = y[m];
+        double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int k = 0;
+        for (; k + 7 < rows[m]; k += 8) {
+#pragma unroll
+          for (int u = 0; u < 8; u++) a[u] += Mm[(size_t)(k + u) * ld + j] * ym[k + u];
+        }
+        for (; k < rows[m]; k++) a[0] += Mm[(size_t)k * ld + j] * ym[k];
+        emit(m, j, ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7])));
+      }
+    }
+    tm.sync();
+  }
+}
+
 // The inner F/H fixed point of one sphere solved directly (the exact form): with
 // fb = Vfix + cLH1 LH + cLF1 LF and hb = Dfix + cLH2 LH + cLF2 LF, (F, H) = G (fb, hb),
 // G (2 NP2 x 2 NP2, row-major, one warp per row) the solution operator of the fixed
@@ -1437,27 +1604,14 @@ __device__ __noinline__ double solve_direct(const Team &tm, const Tab &T, const 
     Fold[k] = F[k];
   }
   tm.sync();
-  const int lane = tm.rank & 31, w = tm.rank >> 5, nw = tm.size >> 5;
-  for (int r = w; r < n2; r += nw) {
-    const double *g = G + (size_t)r * n2;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    int j = lane;
-    for (; j + 96 < n2; j += 128) {   // four loads in flight per lane
-      const double g0 = g[j], g1 = g[j + 32], g2 = g[j + 64], g3 = g[j + 96];
-      a0 += g0 * x[j];
-      a1 += g1 * x[j + 32];
-      a2 += g2 * x[j + 64];
-      a3 += g3 * x[j + 96];
-    }
-    for (; j < n2; j += 32) a0 += g[j] * x[j];
-    double acc = (a0 + a1) + (a2 + a3);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) {
+  {
+    const double *Ms[1] = {G}, *xs[1] = {x};
+    const int nr[1] = {n2};
+    rows_apply<1, 4>(tm, Ms, nr, nr, n2, xs, n2, [&](int, int r, double acc) {
       // omega != 1: the sweep's update over-relaxed (the fixed point is the same)
       if (r < NP2) F[r] = omega == 1.0 ? acc : Fold[r] + omega * (acc - Fold[r]);
       else H[r - NP2] = omega == 1.0 ? acc : Hold[r - NP2] + omega * (acc - Hold[r - NP2]);
-    }
+    });
   }
   tm.sync();
   double pd = 0.0, ps = 0.0;
@@ -1526,50 +1680,27 @@ __device__ double recompute_from_self(const Team &tm, const Sys &y, int s)   // 
   return solve_surface(tm, y, s, true);
 }
 
-// out = (rows of degree < p of N) x, zero beyond (N: NP2 x NP2 row-major), reading the
-// columns of degree < pin; a warp per row, four loads in flight per lane
-__device__ void num_apply(const Team &tm, const double *N, int p, int pin, const double *x, double *out, int NP2)
+// (a, b) = (rows of degree < pF of NF) xF, (rows of degree < pH of NH) xH, zero beyond
+// (NF, NH: NP2 x NP2 row-major), reading the columns of degree < pinF (pinH)
+__device__ __noinline__ void num_apply2(const Team &tm, const double *NF, const double *NH, int pF, int pH, int pinF,
+                                        int pinH, const double *xF, const double *xH, double *a, double *b, int NP2)
 {
-  const int lane = tm.rank & 31, w = tm.rank >> 5, nw = tm.size >> 5, rows = p * p, cols = pin * pin;
-  for (int r = w; r < NP2; r += nw) {
-    double acc = 0.0;
-    if (r < rows) {
-      const double *row = N + (size_t)r * NP2;
-      int j = lane;
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      for (; j + 96 < cols; j += 128) {
-        const double m0 = row[j], m1 = row[j + 32], m2 = row[j + 64], m3 = row[j + 96];
-        a0 += m0 * x[j];
-        a1 += m1 * x[j + 32];
-        a2 += m2 * x[j + 64];
-        a3 += m3 * x[j + 96];
-      }
-      for (; j < cols; j += 32) a0 += row[j] * x[j];
-      acc = (a0 + a1) + (a2 + a3);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    }
-    if (lane == 0) out[r] = acc;
-  }
+  const double *Ms[2] = {NF, NH}, *xs[2] = {xF, xH};
+  const int rows[2] = {pF * pF, pH * pH}, cols[2] = {pinF * pinF, pinH * pinH};
+  rows_apply<2, 2>(tm, Ms, rows, cols, NP2, xs, NP2, [&](int m, int r, double v) { (m ? b : a)[r] = v; });
   tm.sync();
 }
 
-// out[j] += sum over rows k of degree < p of N[k][j] y[k], for the columns j of degree
-// < pin (the transpose of num_apply); a thread per column, eight rows in flight
-__device__ void num_apply_T(const Team &tm, const double *N, int p, int pin, const double *y, double *out, int NP2)
+// outF[j] += sum over rows k of degree < pF of NF[k][j] yF[k] for the columns j of
+// degree < pinF, and the same for H (the transpose of num_apply2); part: shared memory
+// of cap doubles for the column groups' partial sums
+__device__ __noinline__ void num_apply2_T(const Team &tm, const double *NF, const double *NH, int pF, int pH, int pinF,
+                                          int pinH, const double *yF, const double *yH, double *outF, double *outH,
+                                          int NP2, double *part, int cap)
 {
-  const int rows = p * p, cols = pin * pin;
-  for (int j = tm.rank; j < cols; j += tm.size) {
-    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int k = 0;
-    for (; k + 7 < rows; k += 8) {
-#pragma unroll
-      for (int u = 0; u < 8; u++) a[u] += N[(size_t)(k + u) * NP2 + j] * y[k + u];
-    }
-    for (; k < rows; k++) a[0] += N[(size_t)k * NP2 + j] * y[k];
-    out[j] += ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
-  }
-  tm.sync();
+  const double *Ms[2] = {NF, NH}, *ys[2] = {yF, yH};
+  const int rows[2] = {pF * pF, pH * pH}, cols[2] = {pinF * pinF, pinH * pinH};
+  cols_apply<2>(tm, Ms, rows, cols, NP2, ys, part, cap, [&](int m, int j, double v) { (m ? outH : outF)[j] += v; });
 }
 
 // intra near re-expansion with the latest values (src/molecule.cpp:1413-1473).
@@ -1619,8 +1750,8 @@ __device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s, int par
       // s2: an analytic transform at order p is the block of degrees < p of its
       // full-order operator, a numeric one the rows of degree < p
       const double *NF = y.c->tv.Nmat + (size_t)slot * 2 * y.NP2 * y.NP2;
-      num_apply(tm, NF, pF, analytic ? pF : y.NP, y.F(s2), a, y.NP2);
-      num_apply(tm, NF + (size_t)y.NP2 * y.NP2, pH, analytic ? pH : y.NP, y.H(s2), bq, y.NP2);
+      num_apply2(tm, NF, NF + (size_t)y.NP2 * y.NP2, pF, pH, analytic ? pF : y.NP, analytic ? pH : y.NP, y.F(s2),
+                 y.H(s2), a, bq, y.NP2);
       pc.stop(tm, analytic ? PH_INTRA : PH_NUMERIC);
     } else if (analytic) {
       PairXf X;
