@@ -611,8 +611,10 @@ __device__ __noinline__ bool backward_body(const Team &tm, const Sys &y)
         ld += a * a + bb * bb;
         ln += nF[k] * nF[k] + nH[k] * nH[k];
       }
-      dn += team_sum(tm, ld, y.red);
-      nn += team_sum(tm, ln, y.red);
+      double sd, sn;
+      team_sum2(tm, ld, ln, y.red, sd, sn);
+      dn += sd;
+      nn += sn;
       const double om = c.prm.exact_relax;   // over-relaxed as the forward sweeps
       for (int k = tm.rank; k < NP2; k += tm.size) {
         lamF(v)[k] += om * (nF[k] - lamF(v)[k]);

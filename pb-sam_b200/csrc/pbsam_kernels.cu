@@ -238,6 +238,24 @@ __device__ double team_sum(const Team &tm, double v, double *red)
   return r;
 }
 
+// two team sums at once (each the same as team_sum's; red holds 2 x warps doubles)
+__device__ void team_sum2(const Team &tm, double a, double b, double *red, double &ra, double &rb)
+{
+  const int lane = tm.rank & 31, warp = tm.rank >> 5, nw = tm.size >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if (lane == 0) { red[warp] = a; red[nw + warp] = b; }
+  tm.sync();
+  double x = 0.0, z = 0.0;
+  for (int w = 0; w < nw; w++) { x += red[w]; z += red[nw + w]; }
+  tm.sync();
+  ra = x;
+  rb = z;
+}
+
 // per-pair truncation order (src/xforms.cpp:401-414), MAX_ERROR 1e-6
 __device__ __forceinline__ int compute_order(int NP, double rho, double TQ, double scale)
 {
@@ -1624,7 +1642,8 @@ __device__ __noinline__ double solve_direct(const Team &tm, const Tab &T, const 
     pd += wt * (df * df);
     ps += wt * (a * a + b * b);
   }
-  const double td = team_sum(tm, pd, red), tsm = team_sum(tm, ps, red);
+  double td, tsm;
+  team_sum2(tm, pd, ps, red, td, tsm);
   if (tm.rank == 0 && stats) { stats[1] += 1; stats[2] += 1; }
   return tsm > 0.0 ? td / (4 * tsm) : 0.0;
 }
@@ -1680,14 +1699,14 @@ __device__ double recompute_from_self(const Team &tm, const Sys &y, int s)   // 
   return solve_surface(tm, y, s, true);
 }
 
-// (a, b) = (rows of degree < pF of NF) xF, (rows of degree < pH of NH) xH, zero beyond
-// (NF, NH: NP2 x NP2 row-major), reading the columns of degree < pinF (pinH)
+// (a, b) += (rows of degree < pF of NF) xF, (rows of degree < pH of NH) xH, nothing
+// beyond (NF, NH: NP2 x NP2 row-major), reading the columns of degree < pinF (pinH)
 __device__ __noinline__ void num_apply2(const Team &tm, const double *NF, const double *NH, int pF, int pH, int pinF,
                                         int pinH, const double *xF, const double *xH, double *a, double *b, int NP2)
 {
   const double *Ms[2] = {NF, NH}, *xs[2] = {xF, xH};
   const int rows[2] = {pF * pF, pH * pH}, cols[2] = {pinF * pinF, pinH * pinH};
-  rows_apply<2, 2>(tm, Ms, rows, cols, NP2, xs, NP2, [&](int m, int r, double v) { (m ? b : a)[r] = v; });
+  rows_apply<2, 2>(tm, Ms, rows, cols, NP2, xs, NP2, [&](int m, int r, double v) { (m ? b : a)[r] += v; });
   tm.sync();
 }
 
@@ -1748,11 +1767,14 @@ __device__ void reexpand_intra_near(const Team &tm, const Sys &y, int s, int par
     if (slot >= 0 && y.c->tv.nkind[slot] == (analytic ? 0 : 1)) {
       // the exact form's precomputed operators of the pair, the same maps of F and H of
       // s2: an analytic transform at order p is the block of degrees < p of its
-      // full-order operator, a numeric one the rows of degree < p
+      // full-order operator, a numeric one the rows of degree < p.  The pair's terms
+      // are added into LF and LH as they are formed (each entry by the one lane that
+      // sums it: the same additions as through a and bq below)
       const double *NF = y.c->tv.Nmat + (size_t)slot * 2 * y.NP2 * y.NP2;
       num_apply2(tm, NF, NF + (size_t)y.NP2 * y.NP2, pF, pH, analytic ? pF : y.NP, analytic ? pH : y.NP, y.F(s2),
-                 y.H(s2), a, bq, y.NP2);
+                 y.H(s2), LF, LH, y.NP2);
       pc.stop(tm, analytic ? PH_INTRA : PH_NUMERIC);
+      continue;
     } else if (analytic) {
       PairXf X;
       table_pair(tm, T, y.c->tv, y.sc, intra_pair(y.c->tv, ts, s - mo, kj), pH, pF, rj, y.rad(s), X);
