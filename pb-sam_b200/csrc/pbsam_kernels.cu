@@ -1437,10 +1437,10 @@ __device__ void reexpand_LS(const Team &tm, const Sys &y, int s, bool fromSelf)
 // r < rows[m] give sum_{j < cols[m]} M[m][r][j] x[m][j], the rows rows[m] <= r < nout
 // give 0, and emit(m, r, v) receives each result on one lane.  A warp takes R rows of
 // every operator at a time and issues all their loads of a 128-column block together
-// (4 R NM per lane).  Per row, a lane's sums are those of a warp per row (four accumulators over
-// the full 128-column blocks, the ragged block added to the first in column order) and
-// the warp adds them in a fixed butterfly, so a result does not depend on how the rows
-// are dealt to the warps.
+// (4 R NM per lane).  Per row, a lane's sums are those of a warp per row (four
+// accumulators over the full 128-column blocks, the ragged block added to the first in
+// column order) and the warp adds them in a fixed butterfly, so a result does not
+// depend on how the rows are dealt to the warps.
 template <int NM, int R, class Emit>
 __device__ __forceinline__ void rows_apply(const Team &tm, const double *const *M, const int *rows, const int *cols,
                                            int ld, const double *const *x, int nout, Emit emit)
