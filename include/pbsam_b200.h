@@ -93,8 +93,10 @@ typedef struct pbsam_params {
                              full-order p^2 x p^2 operators when they fit in 4 GB (else those of
                              the numeric pairs alone when they fit; p = 10: about 150 MB per
                              35-sphere type) and applied as products in the sweeps and in the
-                             backward pass; 0: transformed as the plain drop-in does.  The two
-                             agree to rounding. */
+                             backward pass, and the angles of every exposed surface point are
+                             tabulated (32 bytes a point) for the surface charges of each
+                             solve; 0: transformed and evaluated as the plain drop-in does.
+                             The two agree to rounding. */
   double exact_tol;       /* exact form only: the sweeps, and the backward pass's transposed
                              sweeps, stop once the root-mean-square relative change of the
                              polarized spheres' H (their adjoint) is below it.  Default 1e-14;

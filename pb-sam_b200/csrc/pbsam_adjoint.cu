@@ -37,6 +37,23 @@
 namespace pbsam {
 
 // ------------------------------------------------------------------ direct inner operator
+// The exact form's point angles: (cos t, sin t, cos phi, sin phi) of every exposed
+// point (relative to its sphere's centre), as surface_q2 computes them per call.
+__global__ void pbsam_spang_kernel(TypeView tv, int TP, double *out)
+{
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= TP) return;
+  const double *pt = tv.spx + 3 * (size_t)h;
+  const Sph s = cart2sph(pt[0], pt[1], pt[2]);
+  double st, ct, sf, cf;
+  sincos(s.theta, &st, &ct);
+  sincos(s.phi, &sf, &cf);
+  out[4 * (size_t)h] = ct;
+  out[4 * (size_t)h + 1] = st;
+  out[4 * (size_t)h + 2] = cf;
+  out[4 * (size_t)h + 3] = sf;
+}
+
 // One CTA per type sphere ts0 + blockIdx.x: [A | Bd] (n x 2n, n = 2 NP2) reduced to
 // [I | G] by Gauss-Jordan elimination with partial pivoting in the CTA's work block;
 // G is copied to tv.Gdir.  Fixed point (src/expcenter.cpp:1079-1135):

@@ -766,6 +766,16 @@ static int finalize_types(pbsam_context *c)
     if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("exact-form operators: ") + cudaGetErrorString(e));
     if (herr) return fail(PBSAM_E_BADARG, "a sphere's inner fixed point is singular; the exact form cannot be used");
     if (c->prm.exact_tables) TRY(build_numeric_operators(B, c, tv, cx, NP, type_off, near_off, near, spx_off, cen, rad));
+    // the exposed points' angles (32 bytes a point), read by the surface charges
+    if (c->prm.exact_tables && TP > 0) {
+      double *A = nullptr;
+      TRY(dalloc(B, &A, (size_t)TP * 4));
+      pbsam_spang_kernel<<<(TP + 255) / 256, 256>>>(tv, TP, A);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaDeviceSynchronize();
+      if (e != cudaSuccess) return fail(PBSAM_E_CUDA, std::string("surface point angles: ") + cudaGetErrorString(e));
+      tv.spang = A;
+    }
   }
   c->finalized = true;
   return PBSAM_OK;

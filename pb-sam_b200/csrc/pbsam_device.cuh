@@ -167,6 +167,49 @@ __device__ __forceinline__ void sh_column(const Tab &T, double cost, double sint
   }
 }
 
+// sh_column with the column's (cos m phi, sin m phi) = (cp, sp) and sint^m = sq given
+// by the caller (the same recurrence and normalisation)
+template <class Fn>
+__device__ __forceinline__ void sh_column_cs(const Tab &T, double cost, double cp, double sp, double sq, int m, int P,
+                                             Fn f)
+{
+  if (m >= P) return;
+  if (m == 0) {
+    double p0 = T.C6[0];
+    f(0, p0 * T.c3(0, 0), 0.0);
+    if (P > 1) {
+      double p1 = cost * p0;
+      f(1, p1 * T.c3(1, 0), 0.0);
+      double pm2 = p0, pm1 = p1;
+      for (int n = 2; n < P; n++) {
+        double pn = cost * T.c1(n, 0) * pm1 - T.c2(n, 0) * pm2;
+        f(n, pn * T.c3(n, 0), 0.0);
+        pm2 = pm1; pm1 = pn;
+      }
+    }
+    return;
+  }
+  const double neg = (m & 1) ? -1.0 : 1.0;
+  const double s = (m & 1) ? -1.0 : 1.0;
+  double pmm = neg * T.C6[m] * sq;
+  {
+    double sc = s * T.c3(m, m);
+    f(m, pmm * (sc * cp), pmm * (sc * sp));
+  }
+  if (m + 1 < P) {
+    double p1 = cost * (2 * m + 1) * pmm;
+    double sc = s * T.c3(m + 1, m);
+    f(m + 1, p1 * (sc * cp), p1 * (sc * sp));
+    double pm2 = pmm, pm1 = p1;
+    for (int n = m + 2; n < P; n++) {
+      double pn = cost * T.c1(n, m) * pm1 - T.c2(n, m) * pm2;
+      double sc2 = s * T.c3(n, m);
+      f(n, pn * (sc2 * cp), pn * (sc2 * sp));
+      pm2 = pm1; pm1 = pn;
+    }
+  }
+}
+
 // team: full SH expansion of P degrees at (theta, phi) into out[P*P]
 template <class TM>
 __device__ void sh_full(const TM &tm, const Tab &T, double theta, double phi, int P, double *out)

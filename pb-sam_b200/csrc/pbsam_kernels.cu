@@ -857,6 +857,57 @@ __device__ __noinline__ void surface_q2(const Team &tm, const Tab &T, const Scr 
   }
 }
 
+// surface_q2 with one expansion per set and both sets, for the exact form: each point's
+// (cos t, sin t, cos phi, sin phi) is read from the type's table (ang, four per point)
+// instead of computed from its coordinates, each column's (cos m phi, sin m phi) comes
+// from the previous column's by angle addition instead of a sincos per column, and
+// sin^m t by one product per column.  The same harmonics to rounding (the exact form's
+// results are set by its fixed point, not by the reference's order of operations).
+__device__ __noinline__ void surface_q2_ang(const Team &tm, const Tab &T, const Scr &sc, const double *ang, int N,
+                                            double dA, const double *E1, const double *c1, double *q1,
+                                            const double *E2, const double *c2, double *q2, double *tot1,
+                                            double *tot2, double *red)
+{
+  const int NP = T.NP, NP2 = NP * NP;
+  double *W = sc.tile;
+  for (int u = tm.rank; u < 2 * NP2; u += tm.size) {
+    const int set = u / NP2, c = u - set * NP2;
+    int n = (int)sqrt((double)c);
+    while (n * n > c) n--;
+    while ((n + 1) * (n + 1) <= c) n++;
+    const double *E = set ? E2 : E1;
+    const double *cd = set ? c2 : c1;
+    W[u] = ((c - n * n > 0) ? 2.0 : 1.0) * (cd[n] * E[c]);
+  }
+  tm.sync();
+  double ta1 = 0.0, ta2 = 0.0;
+  for (int h = tm.rank; h < N; h += tm.size) {
+    const double4 a = ((const double4 *)ang)[h];
+    const double ct = a.x, st = a.y, cf = a.z, sf = a.w;
+    double a1 = 0.0, a2 = 0.0, cp = 1.0, sp = 0.0, sq = 1.0;
+    for (int m = 0; m < NP; m++) {
+      if (m > 0) {
+        const double c0 = cp;
+        cp = c0 * cf - sp * sf;
+        sp = sp * cf + c0 * sf;
+        sq *= st;
+      }
+      sh_column_cs(T, ct, cp, sp, sq, m, NP, [&](int n, double re, double im) {
+        const int i0 = IDX(n) + (m ? 2 * m - 1 : 0);
+        const double *w = W + i0, *w2 = W + NP2 + i0;
+        a1 += (m ? w[0] * re + w[1] * im : w[0] * re);
+        a2 += (m ? w2[0] * re + w2[1] * im : w2[0] * re);
+      });
+    }
+    const double v1 = a1 * dA, v2 = a2 * dA;
+    q1[h] = v1;
+    q2[h] = v2;
+    ta1 += fabs(v1);
+    ta2 += fabs(v2);
+  }
+  team_sum2(tm, ta1, ta2, red, *tot1, *tot2);
+}
+
 // ------------------------------------------------------------------ IMat product
 // Y[d*NP2 + i] = scale[n(i)] * sum_k IMT[i][k] x[d*ld + k] for d < D (applyMMat,
 // src/lautil.cpp:57-72, followed by revertF / revertH).  IMT is the IMat stored
@@ -1669,8 +1720,12 @@ __device__ double solve_surface(const Team &tm, const Sys &y, int s, bool rotH)
   const double *cst = y.c->tv.cst + (size_t)ts * CST_N * y.NP;
   const double dA = 4 * PB_PI / double(y.c->tv.nspx[ts]);
   double totF[1], tot[1];
-  crew_surface_q2<1>(tm, y.cw, T, y.sc, y.red, y.spx(s), y.npts(s), dA, y.F(s), T.CONST2, y.qF(s), totF, y.H(s),
-                     cst + CST_CHGH * y.NP, y.qH(s), tot);
+  if (y.c->prm.exact && y.c->tv.spang && y.cw.size == 1)
+    surface_q2_ang(tm, T, y.sc, y.c->tv.spang + 4 * (size_t)y.c->tv.spx_off[ts], y.npts(s), dA, y.F(s), T.CONST2,
+                   y.qF(s), y.H(s), cst + CST_CHGH * y.NP, y.qH(s), totF, tot, y.red);
+  else
+    crew_surface_q2<1>(tm, y.cw, T, y.sc, y.red, y.spx(s), y.npts(s), dA, y.F(s), T.CONST2, y.qF(s), totF, y.H(s),
+                       cst + CST_CHGH * y.NP, y.qH(s), tot);
   double tF = totF[0];
   pc.stop(tm, PH_SURF);
   if (tm.rank == 0) {

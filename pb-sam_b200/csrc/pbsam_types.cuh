@@ -72,6 +72,8 @@ struct TypeView {
   const int *nkind;        // [slots] 0: analytic pair (rotation + translation), 1: numeric
   const double *Nmat;      // [slots][2][NP2][NP2] row-major or null: the near-field operators
                            // N_F, N_H of the intra near pairs (exact form, pbsam_nummat_kernel)
+  const double *spang;     // [TP][4] or null: cos t, sin t, cos phi, sin phi of every exposed
+                           // point (exact form, pbsam_spang_kernel)
 };
 
 // Batch of B independent systems with the same list of molecules.

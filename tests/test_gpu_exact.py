@@ -135,9 +135,10 @@ def test_exact_backward_vs_oracle_and_central_differences(case, pose, tmp_path):
 
 @pytest.mark.parametrize("case", ["tiny", "cfg0"])
 def test_exact_operators_agree_with_plain_transforms(case):
-    """The intra near-field operators prepared once per type (exact_tables = 1) against
-    the plain transforms at every use (0): every pose of the case, forces and torques
-    (the backward pass) and the lab-frame energy to 1e-11 relative."""
+    """The intra near-field operators and the exposed points' angles prepared once per
+    type (exact_tables = 1) against the plain transforms and the per-call angles at
+    every use (0): every pose of the case, forces and torques (the backward pass) and
+    the lab-frame energy to 1e-11 relative."""
     res = []
     for tables in (1, 0):
         ctx, types, P = exact_ctx(case, exact_tables=tables)
